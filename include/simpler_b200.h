@@ -1,0 +1,285 @@
+/*
+ * simpler_b200.h -- C ABI of libsimpler_b200.so, the B200 (sm_100a) photon march of
+ * simplEr's refractive radiative transfer renderer.
+ *
+ * Everything crossing this boundary is plain C: POD descriptors of doubles/ints, host
+ * pointers and sizes, no C++ or torch types. Every entry point returns SMP_OK (0) or a
+ * negative smp_status; the text of the last error of the calling thread is returned by
+ * smp_last_error(). No entry point exits, asserts or prints.
+ *
+ * Units are the reference's: metres, Hz, m/s, radians.
+ *
+ * Reference interfaces replaced (paths relative to the simplEr project root):
+ *   smp_render / smp_plan_render   <- cuda::CudaRenderer::renderImage      renderer/include/cuda_renderer.h:28-40
+ *                                   <- photon::Renderer::renderImage        renderer/include/photon.h:82-84,
+ *                                                                           renderer/src/photon.cpp:267-340
+ *   smp_plan_create                <- cuda::CudaRenderer::setup             renderer/src/cuda_renderer.cu:745-786
+ *   smp_plan_destroy               <- cuda::CudaRenderer::cleanup           renderer/src/cuda_renderer.cu:788-793
+ *   smp_trace_photons              <- the per-photon body of renderImage    renderer/src/photon.cpp:302-335
+ *                                     (directTracing :41-87, scatter :91-136) with the uniform stream
+ *                                     injected instead of smp::Sampler (renderer/include/sampler.h:19-20)
+ *   smp_field_eval                 <- US::RIF / US::dRIF                    renderer/include/cuda_scene.cuh:463-481
+ *   smp_texture_cdf                <- area_textured_source texture CDF      renderer/src/area_textured_source.cpp:41-45
+ *   smp_render_batch               <- the serial per-configuration loops    renderer/pybindFiles/tests/FUS_configurations.ipynb
+ *                                     (one renderImage per configuration)   (cells at lines 591-603, 713-725)
+ */
+#ifndef SIMPLER_B200_H_
+#define SIMPLER_B200_H_
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SMP_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------------------------- */
+typedef enum smp_status {
+    SMP_OK              =  0,
+    SMP_ERR_BAD_ARG     = -1,   /* invalid descriptor / size / pointer                      */
+    SMP_ERR_CUDA        = -2,   /* a CUDA runtime call failed (text in smp_last_error)       */
+    SMP_ERR_STEP_CAP    = -3,   /* at least one photon hit the per-photon ER-step cap         */
+    SMP_ERR_NAN         = -4,   /* a non-finite position / direction was produced             */
+    SMP_ERR_STREAM      = -5,   /* an injected uniform stream ran out for some photon         */
+    SMP_ERR_NO_DEVICE   = -6,   /* no CUDA device, or not an sm_100 device                    */
+    SMP_ERR_OOM         = -7,   /* device allocation failed                                   */
+    SMP_ERR_UNSUPPORTED = -8    /* option combination not built                               */
+} smp_status;
+
+/* ---- refractive-index field ---------------------------------------------------------------- */
+typedef enum smp_field_type {
+    SMP_FIELD_BESSEL    = 0,  /* rif_analytical: n_o + n_max*s*J_m(k r) cos(m phi)   scene.cpp:205-257   */
+    SMP_FIELD_SOURCES   = 1,  /* rif_sources: spherical point sources on two arcs    scene.cpp:139-195   */
+    SMP_FIELD_PLANEWAVE = 2,  /* n_o + sum_i a_i sin(k_i.x - tau + phase_i) (not in the reference)        */
+    SMP_FIELD_SPLINE    = 3   /* rif_interpolated: tricubic B-spline              spline.h:308-448    */
+} smp_field_type;
+
+#define SMP_MAX_WAVES 8
+
+typedef struct smp_field_desc {
+    int32_t type;                 /* smp_field_type */
+    int32_t precision;            /* refinement levels of traceTillBlock (rif_base.h:28)            */
+    /* common (rif_base.h:10-32, recompute_derived_ :144-154) */
+    double  f_u;                  /* ultrasound frequency (Hz)                                      */
+    double  speed_u;              /* ultrasound speed (m/s); k = 2*pi*f_u/speed_u                   */
+    double  n_o;                  /* baseline refractive index                                      */
+    double  er_stepsize;          /* ER step (m)                                                    */
+    double  egap_end_x;           /* field is n_o, grad 0 for x > egap_end_x   (rif_base.h:134-137) */
+    double  sgap_begin_x;         /*                      or  x < sgap_begin_x                      */
+    double  direct_tol;           /* carried for the settings round trip; unused on the path        */
+    double  rr_weight;            /* carried; unused on the path                                    */
+    int32_t use_initialization_hack; /* carried; unused on the path                                 */
+    /* Bessel (rif_analytical.h:168-175) */
+    int32_t mode;                 /* Bessel order m >= 0                                            */
+    double  n_max, n_clip, phi_min, phi_max;
+    /* FUS point sources (rif_sources.h:18-45) */
+    int32_t n_coeff;              /* triangle-wave harmonics                                        */
+    int32_t theta_sources, trans_z_sources;
+    int32_t active1, active2;
+    int32_t _pad0;
+    double  n_scaling, radius, chordlength, phase1, phase2;
+    double  center1[3], center2[3];
+    /* plane waves (new field type): n = n_o + sum_i a_i sin(k_i . x - tau + phase_i),
+       tau = phi_min + (phi_max - phi_min) * u is the per-photon temporal phase drawn where the
+       reference draws its Bessel 'scaling' (photon.cpp:324) */
+    int32_t n_waves;
+    int32_t _pad1;
+    double  wave_amp[SMP_MAX_WAVES];
+    double  wave_k[SMP_MAX_WAVES][3];
+    double  wave_phase[SMP_MAX_WAVES];
+    /* tricubic B-spline over a regular grid (spline.h); coefficients are already prefiltered
+       (smp_spline_prefilter), x fastest: c[x + Nx*(y + Ny*z)]; host pointer, float */
+    int32_t grid_n[3];
+    int32_t _pad2;
+    double  grid_min[3], grid_max[3];
+    const float *grid_coeff;
+} smp_field_desc;
+
+/* ---- scene: medium box, textured collimated source, sensor --------------------------------- */
+typedef struct smp_scene_desc {
+    double  ior;                  /* medium ior for the boundary BSDF and entry Fresnel (scene.h:47)*/
+    double  medium_l[3], medium_r[3];
+    /* source (area_textured_source.h:20-30) */
+    double  light_origin[3], light_dir[3];
+    double  half_theta_limit;
+    double  light_plane[2];
+    double  Li;
+    int32_t tex_x, tex_y;         /* texture resolution                                             */
+    const double *texture;        /* tex_x*tex_y texels, index y*tex_x + x, rows as stored after the
+                                     PFM bottom-to-top flip (image.h:183-245); host pointer         */
+    double  emitter_lens_origin[3];
+    double  emitter_lens_aperture, emitter_lens_focal_length;
+    int32_t emitter_lens_active;
+    /* camera (camera.cpp:11-29) */
+    int32_t use_bounce_decomposition;
+    double  view_origin[3], view_dir[3], view_horizontal[3];
+    double  view_plane[2];
+    double  pathlength_range[2];  /* (-1,-1) = no binning                                           */
+    double  sensor_lens_origin[3];
+    double  sensor_lens_aperture, sensor_lens_focal_length;
+    int32_t sensor_lens_active;
+    /* film (image.h Image3 x_res, y_res, z_res) */
+    int32_t x_res, y_res, z_res;
+    int32_t _pad0;
+} smp_scene_desc;
+
+/* ---- medium (medium.h:24-38) + Henyey-Greenstein g (phase.cpp) ----------------------------- */
+typedef struct smp_medium_desc {
+    double sigma_t, albedo, g;
+} smp_medium_desc;
+
+/* ---- renderer options (photon.h:27-32 plus the B200 choices) ------------------------------- */
+typedef enum smp_rng {
+    SMP_RNG_SFMT   = 0,   /* SFMT-19937 seeded per photon with (seed + photon index), as
+                             photon.cpp:313: the reference CPU's own stream                      */
+    SMP_RNG_PHILOX = 1,   /* Philox-4x32-10 keyed by (seed, photon index): no state in memory     */
+    SMP_RNG_STREAM = 2    /* injected per-photon uniforms (smp_trace_photons only)                */
+} smp_rng;
+
+typedef enum smp_precision {
+    SMP_PREC_FP32  = 0,   /* FP32 march, FP32 path length, FP32 image atomics (the reference GPU)  */
+    SMP_PREC_MIXED = 1    /* FP32 march, FP64 path-length accumulator, FP64 image atomics         */
+} smp_precision;
+
+typedef struct smp_render_opts {
+    int32_t  max_depth;           /* -1 = unlimited (photon.h:111)                                  */
+    int32_t  use_direct;          /* photon.h:113                                                   */
+    int32_t  use_angular_sampling;/* photon.h:114                                                   */
+    int32_t  rng;                 /* smp_rng                                                        */
+    int32_t  precision;           /* smp_precision                                                  */
+    int32_t  device;              /* CUDA ordinal                                                   */
+    double   max_pathlength;      /* -1 = unlimited (photon.h:112)                                  */
+    uint64_t seed;                /* photon i uses stream (seed + i); seed 0 == the reference       */
+    int64_t  step_cap;            /* per-photon ER-step cap (0 = default 1e8); the reference has none */
+    int32_t  block_size;          /* 0 = autotuned / default                                        */
+    int32_t  blocks_per_sm;       /* 0 = default                                                    */
+} smp_render_opts;
+
+typedef struct smp_stats {
+    int64_t photons;              /* photons traced                                                 */
+    int64_t er_steps;             /* accepted + rejected er_step evaluations                        */
+    int64_t splats;               /* addEnergyToImage calls that reached the film                   */
+    int64_t step_cap_hits;        /* photons stopped by step_cap                                    */
+    int64_t nan_photons;          /* photons stopped by a non-finite state                          */
+    int64_t stream_exhausted;     /* photons whose injected stream ran out                          */
+    double  kernel_ms;            /* device time of the march kernel(s)                             */
+} smp_stats;
+
+/* ---- parity records (smp_trace_photons) ---------------------------------------------------- */
+#define SMP_TRACE_MAX_SPLATS 8
+
+typedef enum smp_photon_end {
+    SMP_END_GENRAY_FAIL = 1,      /* source ray missed the emitter lens aperture                    */
+    SMP_END_NO_SCATTER  = 2,      /* first albedo roulette failed (or albedo 0)                     */
+    SMP_END_ESCAPED     = 3,      /* refracted out through a face in movePhoton                     */
+    SMP_END_ABSORBED    = 4,      /* albedo roulette killed the photon at a vertex                  */
+    SMP_END_MAX_DEPTH   = 5,      /* maxDepth / maxPathlength reached                               */
+    SMP_END_STEP_CAP    = 6,
+    SMP_END_NAN         = 7,
+    SMP_END_STREAM      = 8
+} smp_photon_end;
+
+typedef struct smp_splat_record {
+    float   p[3];                 /* position handed to addEnergyToImage (sensor plane)             */
+    int32_t depth;                /* 0 = direct                                                     */
+    double  pathlength;           /* optical path length used for the z bin                         */
+    double  value;                /* totalPhotonValue before the bilinear split                     */
+} smp_splat_record;
+
+typedef struct smp_photon_record {
+    int64_t photon;
+    int32_t end;                  /* smp_photon_end                                                 */
+    int32_t draws;                /* uniforms consumed                                              */
+    int32_t depth;                /* depth when the photon ended                                    */
+    int32_t n_splats;             /* splat events (may exceed SMP_TRACE_MAX_SPLATS)                 */
+    float   pos[3];               /* photon position at termination                                 */
+    float   dir[3];               /* photon optical direction v = n*omega at termination            */
+    double  total_optical;        /* the photon's running optical path length at termination        */
+    int64_t er_steps;
+    smp_splat_record splats[SMP_TRACE_MAX_SPLATS];
+} smp_photon_record;
+
+/* ---- batched sweep (north-star form 2) ----------------------------------------------------- */
+typedef struct smp_instance_desc {
+    smp_field_desc  field;        /* per-instance field (Bessel / plane wave)                       */
+    smp_medium_desc medium;
+    int64_t         n_photons;    /* this instance's budget                                         */
+    uint64_t        seed;
+} smp_instance_desc;
+
+/* ---- opaque plan ---------------------------------------------------------------------------- */
+typedef struct smp_plan smp_plan;
+
+/* library */
+int         smp_version(void);
+const char *smp_last_error(void);
+int         smp_device_count(void);
+/* sizes of the descriptor structs, so foreign-language mirrors can check their layout */
+size_t      smp_sizeof(const char *type_name);
+
+/* One-shot render (the reference's CudaRenderer::renderImage): uploads the scene, traces
+   n_photons, writes the x*y*z image (index z*X*Y + y*X + x) to the caller-owned host buffer
+   image_out (overwritten, as cuda_renderer.cu:732-739 does), frees everything. */
+int smp_render(const smp_scene_desc *scene, const smp_medium_desc *medium,
+               const smp_field_desc *field, const smp_render_opts *opts,
+               int64_t n_photons, double *image_out, smp_stats *stats_out);
+
+/* Plans keep the scene, texture CDF, field data and film resident on the device so repeated
+   renders pay no setup. */
+int smp_plan_create(const smp_scene_desc *scene, const smp_medium_desc *medium,
+                    const smp_field_desc *field, const smp_render_opts *opts, smp_plan **plan_out);
+int smp_plan_destroy(smp_plan *plan);
+/* change per-render scalars, as the pybind setters set_f_u / set_n_max / set_n_scaling /
+   set_phase1 / set_phase2 do (renderer/include/scene.h:179-219) */
+int smp_plan_set_field(smp_plan *plan, const smp_field_desc *field);
+/* Render photons [first_photon, first_photon + n_photons) into the plan's device film
+   (accumulating; the film is zeroed by smp_plan_clear). Asynchronous on 'stream'
+   (a cudaStream_t, NULL = legacy default stream). weight_photons is the N of Li*T/N
+   (photon.h:76-80); pass the total photon count of the render. */
+int smp_plan_clear(smp_plan *plan, void *stream);
+int smp_plan_trace(smp_plan *plan, int64_t first_photon, int64_t n_photons,
+                   int64_t weight_photons, void *stream);
+/* Copy the film out as doubles (host or device destination). Synchronises 'stream'. */
+int smp_plan_read_image(smp_plan *plan, double *dst, int dst_is_device, void *stream);
+/* Device pointer of the film (float or double per smp_render_opts.precision) and its dtype
+   (4 or 8 bytes per pixel), for zero-copy torch views. */
+int smp_plan_film(smp_plan *plan, void **dev_ptr, int32_t *bytes_per_pixel);
+int smp_plan_stats(smp_plan *plan, smp_stats *stats_out);
+/* Whole render through a plan: clear, trace [0,n), read back to host. */
+int smp_plan_render(smp_plan *plan, int64_t n_photons, double *image_out, smp_stats *stats_out);
+
+/* Parity mode: traces n_photons with per-photon injected uniforms
+   (photon i consumes uniforms[offsets[i] .. offsets[i+1]) ), or with the opts->rng stream when
+   uniforms == NULL, and returns one record per photon. Also accumulates the image into image_out
+   (host, may be NULL). weight_photons as in smp_plan_trace. */
+int smp_trace_photons(const smp_scene_desc *scene, const smp_medium_desc *medium,
+                      const smp_field_desc *field, const smp_render_opts *opts,
+                      int64_t first_photon, int64_t n_photons, int64_t weight_photons,
+                      const float *uniforms, const int64_t *offsets,
+                      smp_photon_record *records_out, double *image_out);
+
+/* Field probe: n(p) and grad n(p) at n_points host points (xyz interleaved) for a given
+   temporal scaling, with the kernel's own device code. */
+int smp_field_eval(const smp_field_desc *field, double scaling, int64_t n_points,
+                   const double *points, double *n_out, double *grad_out);
+
+/* Texture CDF exactly as area_textured_source builds it (float accumulate + normalise),
+   tex_x*tex_y+1 entries. */
+int smp_texture_cdf(const double *texture, int32_t tex_x, int32_t tex_y, float *cdf_out);
+
+/* B-spline prefilter (spline.h:686-764, mirror boundary) of samples -> coefficients, float. */
+int smp_spline_prefilter(const float *samples, const int32_t n[3], float *coeff_out);
+
+/* Batched sweep: n_inst instances sharing one scene/film shape, traced in one persistent
+   launch; images_out holds n_inst consecutive films (host). */
+int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *instances,
+                     int32_t n_inst, const smp_render_opts *opts,
+                     double *images_out, smp_stats *stats_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SIMPLER_B200_H_ */
