@@ -152,9 +152,14 @@ typedef struct smp_render_opts {
     int32_t  device;              /* CUDA ordinal                                                   */
     double   max_pathlength;      /* -1 = unlimited (photon.h:112)                                  */
     uint64_t seed;                /* photon i uses stream (seed + i); seed 0 == the reference       */
-    int64_t  step_cap;            /* per-photon ER-step cap (0 = default 1e8); the reference has none */
+    int64_t  step_cap;            /* per-photon ER-step cap (0 = default 1e7); the reference has none */
     int32_t  block_size;          /* 0 = autotuned / default                                        */
     int32_t  blocks_per_sm;       /* 0 = default                                                    */
+    /* Path budget of one sensor march (movePhotonTillSensor's LargeDist, scene.cpp:627, fixed at
+       1e4 m in the reference). > 0: that many metres. 0: min(1e4, 110/sigma_t), beyond which the
+       march's contribution weight*exp(-sigma_t*d) is exactly 0 in FP32, so a photon trapped by
+       total internal reflection stops there instead of marching 1e4 m. */
+    double   sensor_march_max;
 } smp_render_opts;
 
 typedef struct smp_stats {

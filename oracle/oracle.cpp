@@ -114,6 +114,11 @@ template <typename R> struct Field {
     int N[3] = {0, 0, 0};
     R xmin[3], xres[3];
     const float *coeff = nullptr;
+    // Conditioning deviation: the coefficients (~n) are summed as offsets from their mean, as the
+    // B-spline weights sum to 1 and their derivatives to 0. The reference sums the raw values in
+    // Float and loses about four digits of a 1e-3 gradient to cancellation (spline.h:324-356).
+    std::vector<R> delta;
+    R base = 0;
     // fixed axes of rif_base.h:144-154
     V3<R> axis_uz = V3<R>(R(-1), R(0), R(0)), axis_ux = V3<R>(R(0), R(0), R(1)), p_u;
 
@@ -143,6 +148,13 @@ template <typename R> struct Field {
                 xres[i] = R(N[i] - 1) / (R(f.grid_max[i]) - R(f.grid_min[i]));   // spline.h:146
             }
             coeff = f.grid_coeff;
+            size_t n = size_t(N[0]) * N[1] * N[2];
+            double mean = 0.0;
+            for (size_t i = 0; i < n; ++i) mean += coeff[i];
+            mean /= double(n);
+            base = R(float(mean));
+            delta.resize(n);
+            for (size_t i = 0; i < n; ++i) delta[i] = R(double(coeff[i]) - double(float(mean)));
         }
     }
 
@@ -315,10 +327,10 @@ template <typename R> struct Field {
         for (int i1 = int(std::ceil(x[0] - 2)); i1 <= int(std::floor(x[0] + 2)); ++i1)
             for (int i2 = int(std::ceil(x[1] - 2)); i2 <= int(std::floor(x[1] + 2)); ++i2)
                 for (int i3 = int(std::ceil(x[2] - 2)); i3 <= int(std::floor(x[2] + 2)); ++i3) {
-                    R c = R(coeff[wrap(i1, N[0]) + wrap(i2, N[1]) * N[0] + wrap(i3, N[2]) * N[0] * N[1]]);
+                    R c = delta[wrap(i1, N[0]) + wrap(i2, N[1]) * N[0] + wrap(i3, N[2]) * N[0] * N[1]];
                     v += c * k0(x[0] - R(i1)) * k0(x[1] - R(i2)) * k0(x[2] - R(i3));
                 }
-        return v;
+        return base + v;
     }
     // spline.h:324-356 with the mirror rule
     V3<R> spline_gradient(const V3<R> &p) const {
@@ -328,7 +340,7 @@ template <typename R> struct Field {
         for (int i1 = int(std::ceil(x[0] - 2)); i1 <= int(std::floor(x[0] + 2)); ++i1)
             for (int i2 = int(std::ceil(x[1] - 2)); i2 <= int(std::floor(x[1] + 2)); ++i2)
                 for (int i3 = int(std::ceil(x[2] - 2)); i3 <= int(std::floor(x[2] + 2)); ++i3) {
-                    R c = R(coeff[wrap(i1, N[0]) + wrap(i2, N[1]) * N[0] + wrap(i3, N[2]) * N[0] * N[1]]);
+                    R c = delta[wrap(i1, N[0]) + wrap(i2, N[1]) * N[0] + wrap(i3, N[2]) * N[0] * N[1]];
                     R kx = k0(x[0] - R(i1)), ky = k0(x[1] - R(i2)), kz = k0(x[2] - R(i3));
                     v.x += c * k1(x[0] - R(i1)) * ky * kz;
                     v.y += c * kx * k1(x[1] - R(i2)) * kz;
@@ -352,7 +364,7 @@ template <typename R> struct Lens {                          // lens.cpp:20-97
         focal = R(f);
         active = act != 0;
     }
-    bool deflect(const V3<R> &pos, V3<R> &dir, R &total) const {
+    template <typename T> bool deflect(const V3<R> &pos, V3<R> &dir, T &total) const {
         R sq = 0;
         for (int i = 1; i < 3; ++i) sq += pos[i] * pos[i];
         if (sq > sq_aperture) return false;
@@ -360,14 +372,14 @@ template <typename R> struct Lens {                          // lens.cpp:20-97
         dir[0] = -focal;
         dir[1] = dir[1] * invd * focal - pos[1];
         dir[2] = dir[2] * invd * focal - pos[2];
-        total += focal * invd - dir.length();
+        total += T(focal * invd - dir.length());
         dir.normalize();
         return true;
     }
-    bool propagate_till_lens(V3<R> &pos, V3<R> &dir, R &total) const {
+    template <typename T> bool propagate_till_lens(V3<R> &pos, V3<R> &dir, T &total) const {
         R dist = -(pos[0] - origin[0]) / dir[0];
         pos += dist * dir;
-        total += dist;
+        total += T(dist);
         if (active) return deflect(pos, dir, total);
         return true;
     }
@@ -501,7 +513,9 @@ template <typename R> void Scene<R>::init(const smp_scene_desc &s) {
 }
 
 // ---- the photon march ------------------------------------------------------------------------------
-template <typename R> struct Tracer {
+// R: arithmetic of the march; A: the optical path-length accumulator and film (float in the
+// reference; double for the FP32-march / FP64-accumulation form).
+template <typename R, typename A> struct Tracer {
     const Scene<R> *sc;
     const Field<R> *fd;
     R sigma_t, albedo, mfp, g;
@@ -509,6 +523,7 @@ template <typename R> struct Tracer {
     R max_pathlength;
     bool use_direct, use_angular;
     R h0;          // er_stepsize
+    R large_dist;  // LargeDist of movePhotonTillSensor
     long precision0;
     int64_t step_cap;
     R weight;
@@ -518,7 +533,7 @@ template <typename R> struct Tracer {
     bool abort_cap = false, abort_nan = false;
     smp_photon_record *rec = nullptr;
     int n_splats = 0;
-    std::vector<R> *img = nullptr;   // thread-local film
+    std::vector<A> *img = nullptr;   // thread-local film
 
     bool aborted() const { return abort_cap || abort_nan || u->exhausted; }
 
@@ -533,7 +548,7 @@ template <typename R> struct Tracer {
     }
 
     // Scene::traceTillBlock, scene.cpp:385-425
-    R trace_till_block(V3<R> &p, V3<R> &d, R dist, R &total, R s) {
+    R trace_till_block(V3<R> &p, V3<R> &d, R dist, A &total, R s) {
         V3<R> oldp, oldd;
         R distance = 0;
         int64_t maxsteps = to_i64_x86(double(dist / h0 + R(1)));
@@ -554,7 +569,7 @@ template <typename R> struct Tracer {
                 maxsteps = 11;
             } else {
                 distance += cur;
-                total = R(double(total) + double(cur) * fd->RIF(p, s));
+                total = A(double(total) + double(cur) * fd->RIF(p, s));
             }
         }
         return distance;
@@ -589,8 +604,8 @@ template <typename R> struct Tracer {
     }
 
     // Scene::movePhotonTillSensor, scene.cpp:622-703
-    bool move_till_sensor(V3<R> &p, V3<R> &d, R &distToSensor, R &total, R s) {
-        R large = R(10000);
+    bool move_till_sensor(V3<R> &p, V3<R> &d, R &distToSensor, A &total, R s) {
+        R large = large_dist;                       // LargeDist (scene.cpp:627); see smp_render_opts
         distToSensor = trace_till_block(p, d, large, total, s);
         if (aborted()) return false;
         large -= distToSensor;
@@ -611,7 +626,7 @@ template <typename R> struct Tracer {
     }
 
     // Scene::movePhoton, scene.cpp:706-780
-    bool move_photon(V3<R> &p, V3<R> &d, R dist, R &total, R s) {
+    bool move_photon(V3<R> &p, V3<R> &d, R dist, A &total, R s) {
         R disy = trace_till_block(p, d, dist, total, s);
         if (aborted()) return false;
         dist -= disy;
@@ -637,13 +652,13 @@ template <typename R> struct Tracer {
         return true;
     }
 
-    void add_pixel(int x, int y, int z, R val) {              // scene.h:305-312, image.h:320-324
+    void add_pixel(int x, int y, int z, A val) {              // scene.h:305-312, image.h:320-324
         if (img && x >= 0 && x < sc->X && y >= 0 && y < sc->Y && z >= 0 && z < sc->Z)
             (*img)[size_t(z) * sc->X * sc->Y + size_t(y) * sc->X + x] += val;
     }
 
     // Scene::addEnergyToImage, scene.cpp:782-829
-    void add_energy(const V3<R> &p, R pathlength, int depth, R val) {
+    void add_energy(const V3<R> &p, A pathlength, int depth, R val) {
         if (rec) {
             if (n_splats < SMP_TRACE_MAX_SPLATS) {
                 smp_splat_record &sr = rec->splats[n_splats];
@@ -657,7 +672,7 @@ template <typename R> struct Tracer {
         R x = dot(sc->cam_h, p) - sc->cam_origin.y;
         R y = dot(sc->cam_v, p) - sc->cam_origin.z;
         bool nobin = (sc->pl_min == R(-1)) && (sc->pl_max == R(-1));
-        if (nobin || ((pathlength > sc->pl_min) && (pathlength < sc->pl_max))) {
+        if (nobin || ((pathlength > A(sc->pl_min)) && (pathlength < A(sc->pl_max)))) {
             x = (x / sc->cam_plane[0] + K<R>::half()) * R(sc->X);
             y = (y / sc->cam_plane[1] + K<R>::half()) * R(sc->Y);
             int ix = int(std::floor(x)), iy = int(std::floor(y));
@@ -665,16 +680,16 @@ template <typename R> struct Tracer {
             if (sc->bounce) iz = depth;
             else if (nobin) iz = 0;
             else {
-                R z = pathlength - sc->pl_min;
-                R range = sc->pl_max - sc->pl_min;
-                z = (z / range) * R(sc->Z);
+                A z = pathlength - A(sc->pl_min);
+                A range = A(sc->pl_max) - A(sc->pl_min);
+                z = (z / range) * A(sc->Z);
                 iz = int(std::floor(z));
             }
             R fx = x - std::floor(x), fy = y - std::floor(y);
-            add_pixel(ix, iy, iz, val * (R(1) - fx) * (R(1) - fy));
-            add_pixel(ix + 1, iy, iz, val * fx * (R(1) - fy));
-            add_pixel(ix, iy + 1, iz, val * (R(1) - fx) * fy);
-            add_pixel(ix + 1, iy + 1, iz, val * fx * fy);
+            add_pixel(ix, iy, iz, A(val * (R(1) - fx) * (R(1) - fy)));
+            add_pixel(ix + 1, iy, iz, A(val * fx * (R(1) - fy)));
+            add_pixel(ix, iy + 1, iz, A(val * (R(1) - fx) * fy));
+            add_pixel(ix + 1, iy + 1, iz, A(val * fx * fy));
         }
     }
 
@@ -720,7 +735,7 @@ template <typename R> struct Tracer {
     }
 
     // Scene::addEnergyInParticle, scene.cpp:866-946
-    void add_energy_in_particle(const V3<R> &p, const V3<R> &d, R distTravelled, int depth, R val, R s) {
+    void add_energy_in_particle(const V3<R> &p, const V3<R> &d, A distTravelled, int depth, R val, R s) {
         V3<R> p1 = p;
         if ((p.x - sc->cam_origin.x) < R(1e-4)) return;
         V3<R> dirToSensor = sample_random_direction();
@@ -737,17 +752,17 @@ template <typename R> struct Tracer {
             fw = (R(1) - fresnel(dirToSensor.x, refr.x, R(1) / ior)) / ior / ior;
         }
         R foreshortening = dot(refr, sc->cam_dir) / dot(dirToSensor, sc->cam_dir);
-        R tot = distTravelled;
+        A tot = distTravelled;
         R dts = 0;
         if (!propagate_till_sensor(p1, refr, dts)) return;
-        tot += dts;
+        tot += A(dts);
         R value = val * R(2.0 * double(K<R>::pi())) * std::exp(-sigma_t * distToSensor) *
                   hg_f(d / d.length(), dirToSensor) * foreshortening * fw;
         add_energy(p1, tot, depth, value);
     }
 
     // Renderer::directTracing, photon.cpp:41-87 (total is the photon's own, by reference)
-    void direct_tracing(const V3<R> &p, const V3<R> &d, R s, R &total) {
+    void direct_tracing(const V3<R> &p, const V3<R> &d, R s, A &total) {
         V3<R> p1 = p, d1 = d;
         R distToSensor;
         if (!move_till_sensor(p1, d1, distToSensor, total, s)) return;
@@ -762,7 +777,7 @@ template <typename R> struct Tracer {
         }
         R dts = 0;
         if (!propagate_till_sensor(p1, refr, dts)) return;
-        total += dts;
+        total += A(dts);
         R value = weight * std::exp(-sigma_t * distToSensor) * fw;
         add_energy(p1, total, 0, value);
     }
@@ -774,7 +789,7 @@ template <typename R> struct Tracer {
     }
 
     // Renderer::scatterOnce, photon.cpp:20-38
-    bool scatter_once(V3<R> &p, V3<R> &d, R &dist, R &total, R s, int &end) {
+    bool scatter_once(V3<R> &p, V3<R> &d, R &dist, A &total, R s, int &end) {
         if (roulette()) {
             R mag = d.length();
             V3<R> d1;
@@ -791,7 +806,7 @@ template <typename R> struct Tracer {
     }
 
     // Renderer::scatter, photon.cpp:91-136
-    void scatter(V3<R> &pos, V3<R> &dir, R s, R &total, int &depth_out, int &end) {
+    void scatter(V3<R> &pos, V3<R> &dir, R s, A &total, int &depth_out, int &end) {
         depth_out = 0;
         if (!roulette()) { end = SMP_END_NO_SCATTER; return; }
         R dist = move_step();
@@ -811,7 +826,7 @@ template <typename R> struct Tracer {
     }
 
     // area_textured_source::sample_ray, scene.cpp:107-137
-    bool gen_ray(V3<R> &pos, V3<R> &dir, R &total) {
+    bool gen_ray(V3<R> &pos, V3<R> &dir, A &total) {
         pos = sc->src_origin;
         int pixel = sample_cdf(sc->cdf, (*u)());
         int py = pixel / sc->tex_x;
@@ -832,7 +847,7 @@ template <typename R> struct Tracer {
         abort_cap = abort_nan = false;
         n_splats = 0;
         V3<R> pos, dir;
-        R total = 0;
+        A total = 0;
         int end = SMP_END_GENRAY_FAIL, depth = 0;
         if (gen_ray(pos, dir, total)) {
             R uu = (*u)();
@@ -866,7 +881,7 @@ template <typename R> struct Tracer {
     }
 };
 
-template <typename R>
+template <typename R, typename A>
 static int render_impl(const smp_scene_desc *sd, const smp_medium_desc *md, const smp_field_desc *fdesc,
                        const smp_render_opts *opts, int threads, int64_t first, int64_t n,
                        int64_t weight_photons, const float *uniforms, const int64_t *offsets,
@@ -881,12 +896,12 @@ static int render_impl(const smp_scene_desc *sd, const smp_medium_desc *md, cons
     R weight = sc.Li * sc.fresnel_trans / R(weight_photons);   // photon.h:76-80
     const size_t npix = size_t(sc.X) * sc.Y * sc.Z;
     int nt = threads > 0 ? threads : omp_get_max_threads();
-    std::vector<std::vector<R>> imgs(nt, std::vector<R>(image_out ? npix : 0, R(0)));
-    int64_t cap = opts->step_cap > 0 ? opts->step_cap : int64_t(100000000);
+    std::vector<std::vector<A>> imgs(nt, std::vector<A>(image_out ? npix : 0, A(0)));
+    int64_t cap = opts->step_cap > 0 ? opts->step_cap : int64_t(10000000);
 #pragma omp parallel num_threads(nt)
     {
         int tid = omp_get_thread_num();
-        Tracer<R> tr;
+        Tracer<R, A> tr;
         tr.sc = &sc;
         tr.fd = &fd;
         tr.sigma_t = sigma_t;
@@ -898,6 +913,12 @@ static int render_impl(const smp_scene_desc *sd, const smp_medium_desc *md, cons
         tr.use_direct = opts->use_direct != 0;
         tr.use_angular = opts->use_angular_sampling != 0;
         tr.h0 = R(fdesc->er_stepsize);
+        {
+            float st = float(sigma_t);
+            float d = opts->sensor_march_max > 0.0 ? float(opts->sensor_march_max) : 10000.0f;
+            if (!(opts->sensor_march_max > 0.0) && st > 0.0f) d = std::min(d, 110.0f / st);
+            tr.large_dist = R(d);
+        }
         tr.precision0 = fdesc->precision;
         tr.step_cap = cap;
         tr.weight = weight;
@@ -928,7 +949,7 @@ static int render_impl(const smp_scene_desc *sd, const smp_medium_desc *md, cons
     }
     if (image_out) {
         for (size_t j = 0; j < npix; ++j) {
-            R v = 0;
+            A v = 0;
             for (int t = 0; t < nt; ++t) v += imgs[t][j];
             image_out[j] = double(v);
         }
@@ -990,10 +1011,13 @@ int orc_render(const smp_scene_desc *scene, const smp_medium_desc *medium, const
     if (!scene || !medium || !field || !opts || n < 0 || weight_photons <= 0) return SMP_ERR_BAD_ARG;
     if (uniforms && !offsets) return SMP_ERR_BAD_ARG;
     if (real_bits == 64)
-        return orc::render_impl<double>(scene, medium, field, opts, threads, first, n, weight_photons,
-                                        uniforms, offsets, records, image_out);
-    return orc::render_impl<float>(scene, medium, field, opts, threads, first, n, weight_photons,
-                                   uniforms, offsets, records, image_out);
+        return orc::render_impl<double, double>(scene, medium, field, opts, threads, first, n, weight_photons,
+                                                uniforms, offsets, records, image_out);
+    if (opts->precision == SMP_PREC_MIXED)      // FP32 march, FP64 path length and film
+        return orc::render_impl<float, double>(scene, medium, field, opts, threads, first, n, weight_photons,
+                                               uniforms, offsets, records, image_out);
+    return orc::render_impl<float, float>(scene, medium, field, opts, threads, first, n, weight_photons,
+                                          uniforms, offsets, records, image_out);
 }
 
 int orc_sfmt_floats(uint64_t seed, int n, float *out) {

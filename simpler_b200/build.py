@@ -1,0 +1,87 @@
+"""Build the native parts of simpler_b200 in-tree.
+
+* ``libsimpler_b200.so`` -- the CUDA kernels and the C ABI (``include/simpler_b200.h``),
+  compiled for sm_100a only.
+* the CPU oracle (``oracle/liboracle*.so``) and, when the reference checkout is present, the
+  reference's own primitives (``oracle/_ref``) -- test infrastructure, built here so the GPU box
+  receives them prebuilt.
+
+Usage: ``python -m simpler_b200.build [--verbose]``.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libsimpler_b200.so")
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-lineinfo", "-O3", "-std=c++17",
+    "-Xcompiler", "-fPIC", "-shared",
+    "--expt-relaxed-constexpr",
+]
+
+CU_SOURCES = ["capi.cu"]
+HEADERS = ["kparams.h", "dev_math.cuh", "dev_field.cuh", "march.cuh"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build_library(verbose: bool = False, force: bool = False) -> str:
+    deps = [os.path.join(CSRC, f) for f in CU_SOURCES + HEADERS]
+    deps.append(os.path.join(ROOT, "include", "simpler_b200.h"))
+    if not force and not _stale(LIB, deps):
+        return LIB
+    cmd = [_nvcc(), *NVCC_FLAGS]
+    if verbose:
+        cmd += ["-Xptxas", "-v"]
+    cmd += [os.path.join(CSRC, f) for f in CU_SOURCES] + ["-o", LIB + ".tmp"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"nvcc failed:\n{res.stdout}\n{res.stderr}")
+    if verbose:
+        sys.stderr.write(res.stderr)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+def build_oracle() -> None:
+    """Test infrastructure: the CPU checker and the reference primitives used to pin it."""
+    odir = os.path.join(ROOT, "oracle")
+    env = dict(os.environ)
+    env.pop("CXX", None)
+    res = subprocess.run(["make", "-s", "-C", odir, "all"], capture_output=True, text=True, env=env)
+    if res.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{res.stdout}\n{res.stderr}")
+    ref = os.path.join(odir, "ref", "build_ref.sh")
+    if os.path.isdir("/root/reference") and os.path.exists(ref):
+        res = subprocess.run(["sh", ref], capture_output=True, text=True, env=env)
+        if res.returncode != 0:
+            raise RuntimeError(f"reference primitives build failed:\n{res.stdout}\n{res.stderr}")
+
+
+def build_all(verbose: bool = False, force: bool = False) -> None:
+    build_library(verbose=verbose, force=force)
+    build_oracle()
+
+
+if __name__ == "__main__":
+    build_all(verbose="--verbose" in sys.argv, force="--force" in sys.argv)

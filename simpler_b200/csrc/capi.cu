@@ -1,0 +1,781 @@
+// capi.cu -- the extern "C" boundary of libsimpler_b200.so (declared in include/simpler_b200.h).
+//
+// The reference's GPU seam, cuda::CudaRenderer::renderImage (renderer/src/cuda_renderer.cu:710-742),
+// deep-copies the scene with ~30 small cudaMalloc/cudaMemcpy calls per render, runs one thread per
+// photon, and copies a float film back. Here a plan uploads the scene once (texture CDF, source
+// table, spline coefficients, film) and each render is one persistent launch over all SMs on the
+// caller's stream, so renders can be batched and captured in CUDA graphs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kparams.h"
+#include "march.cuh"
+
+using namespace smp;
+
+// ---- errors ------------------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+static int set_error(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define SMP_CUDA(call)                                                                     \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return set_error(e_ == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, \
+                             "%s failed: %s", #call, cudaGetErrorString(e_));              \
+    } while (0)
+
+// ---- host helpers shared with the CLI / pybind layers ------------------------------------------
+
+// DiscreteDistribution append + normalize (renderer/include/pmf.h:41-99), in float
+static void texture_cdf(const double *tex, int n, std::vector<float> &cdf) {
+    cdf.assign(size_t(n) + 1, 0.0f);
+    for (int i = 0; i < n; ++i) cdf[i + 1] = cdf[i] + static_cast<float>(tex[i]);
+    float sum = cdf[n];
+    if (sum > 0.0f) {
+        float norm = 1.0f / sum;
+        for (int i = 1; i <= n; ++i) cdf[i] *= norm;
+        cdf[n] = 1.0f;
+    }
+}
+
+// Spline<3>::build1d (renderer/include/spline.h:686-714): causal + anticausal recursive filter,
+// pole z1 = sqrt(3) - 2, mirror boundary.
+static void prefilter_1d(const float *data, long off, long stride, int size, float *out) {
+    const float z1 = -2.0f + std::sqrt(3.0f);
+    std::vector<float> cp(size), cn(size);
+    float c0 = 0.0f;
+    for (int i = 0; i < size; ++i) c0 += data[off + i * stride] * float(std::pow(double(z1), i));
+    for (int i = size - 2; i > 0; --i) c0 += data[off + i * stride] * float(std::pow(double(z1), 2 * size - 2 - i));
+    c0 /= float(1.0 - std::pow(double(z1), 2 * size - 2));
+    cp[0] = c0;
+    for (int i = 1; i < size; ++i) cp[i] = data[off + i * stride] + z1 * cp[i - 1];
+    cn[size - 1] = z1 / (z1 * z1 - 1.0f) * (cp[size - 1] + z1 * cp[size - 2]);
+    for (int i = size - 2; i >= 0; --i) cn[i] = z1 * (cn[i + 1] - cp[i]);
+    for (int i = 0; i < size; ++i) out[i] = 6.0f * cn[i];
+}
+
+// Spline<3>::build3d (spline.h:739-764): y, then x, then z passes
+static void prefilter_3d(const float *samples, const int N[3], float *coeff) {
+    const long s01 = long(N[0]) * N[1];
+    std::vector<float> tmp(std::max(std::max(N[0], N[1]), N[2]));
+    for (int k = 0; k < N[2]; ++k)
+        for (int i = 0; i < N[0]; ++i) {
+            prefilter_1d(samples, k * s01 + i, N[0], N[1], tmp.data());
+            for (int t = 0; t < N[1]; ++t) coeff[i + t * N[0] + k * s01] = tmp[t];
+        }
+    for (int k = 0; k < N[2]; ++k)
+        for (int j = 0; j < N[1]; ++j) {
+            prefilter_1d(coeff, k * s01 + long(j) * N[0], 1, N[0], tmp.data());
+            for (int t = 0; t < N[0]; ++t) coeff[t + j * N[0] + k * s01] = tmp[t];
+        }
+    for (int i = 0; i < N[0]; ++i)
+        for (int j = 0; j < N[1]; ++j) {
+            prefilter_1d(coeff, long(j) * N[0] + i, s01, N[2], tmp.data());
+            for (int t = 0; t < N[2]; ++t) coeff[i + j * N[0] + t * s01] = tmp[t];
+        }
+}
+
+// rif_sources::recompute_derived_ (renderer/include/rif_sources.h:156-198): centres of the
+// point sources on the two arcs, arc 1 block then arc 2 block.
+static void source_centres(const smp_field_desc &f, std::vector<float4> &out) {
+    const float radius = float(f.radius), chord = float(f.chordlength);
+    const float tmin = -std::asin(chord / (2.0f * radius)), tmax = std::asin(chord / (2.0f * radius));
+    const float zmin = -chord / 2.0f, zmax = chord / 2.0f;
+    const int nt = f.theta_sources, nz = f.trans_z_sources, ns = nt * nz;
+    const float tdiff = (tmax - tmin) / float(nt - 1), zdiff = (zmax - zmin) / float(nz - 1);
+    out.assign(size_t(2) * ns, make_float4(0, 0, 0, 0));
+    for (int i = 0; i < nt; ++i) {
+        float th = tmin + tdiff * float(i);
+        float xv = radius * (1.0f - std::cos(th)), yv = radius * std::sin(th);
+        for (int j = 0; j < nz; ++j) {
+            int k = i + j * nt;
+            float zx = zmin + zdiff * float(j);
+            out[k] = make_float4(zx + float(f.center1[0]), yv + float(f.center1[1]), xv + float(f.center1[2]), 0.0f);
+            out[ns + k] = make_float4(zx + float(f.center2[0]), xv + float(f.center2[1]), yv + float(f.center2[2]), 0.0f);
+        }
+    }
+}
+
+// Spline coefficients as float offsets from their mean (see spline_field in dev_field.cuh).
+static float spline_offsets(const smp_field_desc &f, std::vector<float> &delta) {
+    size_t n = size_t(f.grid_n[0]) * f.grid_n[1] * f.grid_n[2];
+    double mean = 0.0;
+    for (size_t i = 0; i < n; ++i) mean += f.grid_coeff[i];
+    mean /= double(n);
+    float base = float(mean);
+    delta.resize(n);
+    for (size_t i = 0; i < n; ++i) delta[i] = float(double(f.grid_coeff[i]) - double(base));
+    return base;
+}
+
+// Bessel table for the march: nodes x_i = i*h, entries (J_m, J_m', J_m+1, J_m+1') in double from
+// libstdc++'s std::cyl_bessel_j, rounded to float; J_n' = (J_{n-1} - J_{n+1})/2, J_{-1} = -J_1.
+static const double kBesselH = 1.0 / 16.0;
+static const double kBesselMaxX = 128.0;
+static void bessel_table(int m, double x_max, std::vector<float4> &tab) {
+    x_max = std::min(std::max(x_max, 1.0), kBesselMaxX);
+    const int nodes = int(std::ceil(x_max / kBesselH)) + 2;
+    tab.resize(nodes);
+    auto J = [](int n, double x) -> double {
+        if (n < 0) return (n % 2 ? -1.0 : 1.0) * std::cyl_bessel_j(double(-n), x);
+        return std::cyl_bessel_j(double(n), x);
+    };
+    for (int i = 0; i < nodes; ++i) {
+        double x = i * kBesselH;
+        double jm = J(m, x), jm1 = J(m + 1, x);
+        double djm = 0.5 * (J(m - 1, x) - jm1);
+        double djm1 = 0.5 * (jm - J(m + 2, x));
+        tab[i] = make_float4(float(jm), float(djm), float(jm1), float(djm1));
+    }
+}
+
+// largest k*r the march can meet: the box's extent about the -x axis
+static double box_max_kr(const smp_scene_desc &s, float k_r) {
+    double ry = std::max(std::fabs(s.medium_l[1]), std::fabs(s.medium_r[1]));
+    double rz = std::max(std::fabs(s.medium_l[2]), std::fabs(s.medium_r[2]));
+    return double(k_r) * std::sqrt(ry * ry + rz * rz) * 1.01 + 1.0;
+}
+
+// util.h:42-57 in float, for the entry Fresnel transmission (scene.h:144-164)
+static float fresnel_host(float cosI, float cosT, float eta) {
+    if (std::fabs(eta - 1.0f) < 1.19209290e-07f * std::max(1.0f, std::fabs(eta))) return 0.0f;
+    float Rs = (cosI - eta * cosT) / (cosI + eta * cosT);
+    float Rp = (cosT - eta * cosI) / (cosT + eta * cosI);
+    return 0.5f * (Rs * Rs + Rp * Rp);
+}
+
+static int field_kind(const smp_field_desc &f, int *fk) {
+    switch (f.type) {
+        case SMP_FIELD_BESSEL:
+            if (f.mode < 0 || f.mode > 2)
+                return set_error(SMP_ERR_UNSUPPORTED, "Bessel mode %d: orders 0..2 are built", f.mode);
+            *fk = FK_BESSEL0 + f.mode;
+            return SMP_OK;
+        case SMP_FIELD_PLANEWAVE:
+            if (f.n_waves < 0 || f.n_waves > SMP_MAX_WAVES) return set_error(SMP_ERR_BAD_ARG, "n_waves out of range");
+            *fk = FK_PLANEWAVE;
+            return SMP_OK;
+        case SMP_FIELD_SOURCES:
+            if (f.theta_sources < 2 || f.trans_z_sources < 2 || f.n_coeff < 1)
+                return set_error(SMP_ERR_BAD_ARG, "sources field needs theta_sources, trans_z_sources >= 2 and n_coeff >= 1");
+            *fk = FK_SOURCES;
+            return SMP_OK;
+        case SMP_FIELD_SPLINE:
+            for (int i = 0; i < 3; ++i)
+                if (f.grid_n[i] < 2 || !(f.grid_max[i] > f.grid_min[i]))
+                    return set_error(SMP_ERR_BAD_ARG, "spline grid axis %d invalid", i);
+            if (!f.grid_coeff) return set_error(SMP_ERR_BAD_ARG, "spline grid_coeff is NULL");
+            *fk = FK_SPLINE;
+            return SMP_OK;
+        default:
+            return set_error(SMP_ERR_BAD_ARG, "unknown field type %d", f.type);
+    }
+}
+
+// float field parameters shared by plans and probes (device pointers filled by the caller)
+static void fill_field_params(const smp_field_desc &f, int fk, FieldParams &F) {
+    std::memset(&F, 0, sizeof(F));
+    F.kind = fk;
+    F.mode = f.mode;
+    F.n_o = float(f.n_o);
+    F.egap = float(f.egap_end_x);
+    F.sgap = float(f.sgap_begin_x);
+    // rif_base.h:149-153 in Float: lambda = c/f, k = 2*pi/lambda
+    float lambda = float(f.speed_u) / float(f.f_u);
+    F.k_r = (2.0f * 3.14159265358979f) / lambda;
+    F.amp = float(f.n_max);
+    F.max_scaling = float(f.n_clip) / float(f.n_max);       // rif_analytical.h:222
+    F.phi_min = float(f.phi_min);
+    F.phi_range = float(f.phi_max) - float(f.phi_min);
+    F.n_waves = f.n_waves;
+    for (int i = 0; i < SMP_MAX_WAVES && i < f.n_waves; ++i) {
+        F.wamp[i] = float(f.wave_amp[i]);
+        F.wphase[i] = float(f.wave_phase[i]);
+        for (int j = 0; j < 3; ++j) F.wk[i][j] = float(f.wave_k[i][j]);
+    }
+    F.n_coeff = f.n_coeff;
+    F.nsources = f.theta_sources * f.trans_z_sources;
+    F.active1 = f.active1;
+    F.active2 = f.active2;
+    F.n_scaling = float(f.n_scaling);
+    F.phase1 = float(f.phase1);
+    F.phase2 = float(f.phase2);
+    for (int i = 0; i < 3; ++i) {
+        F.N[i] = f.grid_n[i];
+        F.xmin[i] = float(f.grid_min[i]);
+        F.xres[i] = float(f.grid_n[i] - 1) / (float(f.grid_max[i]) - float(f.grid_min[i]));
+    }
+    F.bh = float(kBesselH);
+    F.binv_h = float(1.0 / kBesselH);
+}
+
+// LargeDist of movePhotonTillSensor (scene.cpp:627): 1e4 m in the reference; by default capped
+// where weight*exp(-sigma_t*d) underflows to 0 in FP32 (sigma_t*d > 110).
+static float sensor_march_budget(const smp_render_opts &o, float sigma_t) {
+    if (o.sensor_march_max > 0.0) return float(o.sensor_march_max);
+    float d = 10000.0f;
+    if (sigma_t > 0.0f) d = std::min(d, 110.0f / sigma_t);
+    return d;
+}
+
+static int check_device(int dev) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return set_error(SMP_ERR_NO_DEVICE, "no CUDA device");
+    if (dev < 0 || dev >= n) return set_error(SMP_ERR_BAD_ARG, "device %d out of range (%d devices)", dev, n);
+    cudaDeviceProp prop;
+    SMP_CUDA(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major != 10) return set_error(SMP_ERR_NO_DEVICE, "device %d is sm_%d%d; this library is built for sm_100a", dev, prop.major, prop.minor);
+    SMP_CUDA(cudaSetDevice(dev));
+    return SMP_OK;
+}
+
+// ---- kernel dispatch ---------------------------------------------------------------------------
+typedef void (*MarchFn)(KParams);
+static MarchFn march_fn(int fk) {
+    switch (fk) {
+        case FK_BESSEL0: return march_kernel<FK_BESSEL0>;
+        case FK_BESSEL1: return march_kernel<FK_BESSEL1>;
+        case FK_BESSEL2: return march_kernel<FK_BESSEL2>;
+        case FK_PLANEWAVE: return march_kernel<FK_PLANEWAVE>;
+        case FK_SOURCES: return march_kernel<FK_SOURCES>;
+        case FK_SPLINE: return march_kernel<FK_SPLINE>;
+        default: return nullptr;
+    }
+}
+
+static const int kBlock = 128;
+
+static int grid_for(int fk, int dev, int blocks_per_sm, size_t smem, int *grid) {
+    MarchFn fn = march_fn(fk);
+    int per_sm = blocks_per_sm;
+    if (per_sm <= 0) {
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, smem);
+        if (e != cudaSuccess) return set_error(SMP_ERR_CUDA, "occupancy query: %s", cudaGetErrorString(e));
+        if (per_sm < 1) per_sm = 1;
+    }
+    int sms = 0;
+    SMP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    *grid = sms * per_sm;
+    return SMP_OK;
+}
+
+// ---- plans -------------------------------------------------------------------------------------
+struct smp_plan {
+    int device = 0;
+    int fk = 0;
+    int grid = 0;
+    smp_scene_desc scene;
+    smp_medium_desc medium;
+    smp_field_desc field;
+    smp_render_opts opts;
+    KParams kp;                 // filled except weight / work range / counters
+    float *d_cdf = nullptr;
+    float4 *d_centers = nullptr;
+    float *d_coeff = nullptr;
+    float4 *d_btab = nullptr;
+    size_t smem_bytes = 0;
+    int event_batch = 8;
+    void *d_film = nullptr;
+    size_t film_elems = 0;
+    unsigned long long *d_counters = nullptr;
+    smp_stats stats;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+static void plan_free(smp_plan *p) {
+    if (!p) return;
+    cudaFree(p->d_cdf);
+    cudaFree(p->d_centers);
+    cudaFree(p->d_coeff);
+    cudaFree(p->d_btab);
+    cudaFree(p->d_film);
+    cudaFree(p->d_counters);
+    if (p->ev0) cudaEventDestroy(p->ev0);
+    if (p->ev1) cudaEventDestroy(p->ev1);
+    delete p;
+}
+
+static int check_descs(const smp_scene_desc *s, const smp_medium_desc *m, const smp_field_desc *f,
+                       const smp_render_opts *o) {
+    if (!s || !m || !f || !o) return set_error(SMP_ERR_BAD_ARG, "NULL descriptor");
+    if (s->x_res <= 0 || s->y_res <= 0 || s->z_res <= 0) return set_error(SMP_ERR_BAD_ARG, "film resolution must be positive");
+    if (s->tex_x <= 0 || s->tex_y <= 0 || !s->texture) return set_error(SMP_ERR_BAD_ARG, "texture missing");
+    if (!(f->er_stepsize > 0.0)) return set_error(SMP_ERR_BAD_ARG, "er_stepsize must be positive");
+    if (!(f->f_u > 0.0) || !(f->speed_u > 0.0)) return set_error(SMP_ERR_BAD_ARG, "f_u and speed_u must be positive");
+    if (o->precision != SMP_PREC_FP32 && o->precision != SMP_PREC_MIXED) return set_error(SMP_ERR_BAD_ARG, "bad precision");
+    if (o->rng != SMP_RNG_PHILOX && o->rng != SMP_RNG_STREAM)
+        return set_error(SMP_ERR_UNSUPPORTED, "rng %d: the march kernel draws from Philox or an injected stream", o->rng);
+    if (m->albedo > 1.0 || m->albedo < 0.0) return set_error(SMP_ERR_BAD_ARG, "albedo outside [0,1]");
+    return SMP_OK;
+}
+
+static int plan_setup_field(smp_plan *p, const smp_field_desc &f) {
+    int rc = field_kind(f, &p->fk);
+    if (rc) return rc;
+    fill_field_params(f, p->fk, p->kp.field);
+    if (p->fk == FK_SOURCES) {
+        std::vector<float4> c;
+        source_centres(f, c);
+        cudaFree(p->d_centers);
+        p->d_centers = nullptr;
+        SMP_CUDA(cudaMalloc(&p->d_centers, c.size() * sizeof(float4)));
+        SMP_CUDA(cudaMemcpy(p->d_centers, c.data(), c.size() * sizeof(float4), cudaMemcpyHostToDevice));
+        p->kp.field.centers = p->d_centers;
+    }
+    if (p->fk == FK_SPLINE) {
+        std::vector<float> delta;
+        p->kp.field.spline_base = spline_offsets(f, delta);
+        cudaFree(p->d_coeff);
+        p->d_coeff = nullptr;
+        SMP_CUDA(cudaMalloc(&p->d_coeff, delta.size() * sizeof(float)));
+        SMP_CUDA(cudaMemcpy(p->d_coeff, delta.data(), delta.size() * sizeof(float), cudaMemcpyHostToDevice));
+        p->kp.field.coeff = p->d_coeff;
+    }
+    p->smem_bytes = 0;
+    if (p->fk <= FK_BESSEL2) {
+        std::vector<float4> tab;
+        bessel_table(f.mode, box_max_kr(p->scene, p->kp.field.k_r), tab);
+        cudaFree(p->d_btab);
+        p->d_btab = nullptr;
+        SMP_CUDA(cudaMalloc(&p->d_btab, tab.size() * sizeof(float4)));
+        SMP_CUDA(cudaMemcpy(p->d_btab, tab.data(), tab.size() * sizeof(float4), cudaMemcpyHostToDevice));
+        p->kp.field.btab = p->d_btab;
+        p->kp.field.bnodes = int(tab.size());
+        p->smem_bytes = tab.size() * sizeof(float4);
+    }
+    p->kp.h0 = float(f.er_stepsize);
+    p->kp.precision = f.precision;
+    p->field = f;
+    return grid_for(p->fk, p->device, p->opts.blocks_per_sm, p->smem_bytes, &p->grid);
+}
+
+extern "C" {
+
+int smp_version(void) { return SMP_ABI_VERSION; }
+const char *smp_last_error(void) { return g_last_error.c_str(); }
+int smp_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+size_t smp_sizeof(const char *t) {
+    if (!t) return 0;
+    if (!std::strcmp(t, "smp_field_desc")) return sizeof(smp_field_desc);
+    if (!std::strcmp(t, "smp_scene_desc")) return sizeof(smp_scene_desc);
+    if (!std::strcmp(t, "smp_medium_desc")) return sizeof(smp_medium_desc);
+    if (!std::strcmp(t, "smp_render_opts")) return sizeof(smp_render_opts);
+    if (!std::strcmp(t, "smp_stats")) return sizeof(smp_stats);
+    if (!std::strcmp(t, "smp_photon_record")) return sizeof(smp_photon_record);
+    if (!std::strcmp(t, "smp_splat_record")) return sizeof(smp_splat_record);
+    if (!std::strcmp(t, "smp_instance_desc")) return sizeof(smp_instance_desc);
+    return 0;
+}
+
+int smp_texture_cdf(const double *texture, int32_t tex_x, int32_t tex_y, float *cdf_out) {
+    if (!texture || !cdf_out || tex_x <= 0 || tex_y <= 0) return set_error(SMP_ERR_BAD_ARG, "bad texture");
+    std::vector<float> cdf;
+    texture_cdf(texture, tex_x * tex_y, cdf);
+    std::memcpy(cdf_out, cdf.data(), cdf.size() * sizeof(float));
+    return SMP_OK;
+}
+
+int smp_spline_prefilter(const float *samples, const int32_t n[3], float *coeff_out) {
+    if (!samples || !n || !coeff_out) return set_error(SMP_ERR_BAD_ARG, "NULL argument");
+    int N[3] = {n[0], n[1], n[2]};
+    for (int i = 0; i < 3; ++i)
+        if (N[i] < 2) return set_error(SMP_ERR_BAD_ARG, "spline axis %d needs >= 2 samples", i);
+    prefilter_3d(samples, N, coeff_out);
+    return SMP_OK;
+}
+
+int smp_plan_create(const smp_scene_desc *scene, const smp_medium_desc *medium, const smp_field_desc *field,
+                    const smp_render_opts *opts, smp_plan **plan_out) {
+    if (!plan_out) return set_error(SMP_ERR_BAD_ARG, "plan_out is NULL");
+    *plan_out = nullptr;
+    int rc = check_descs(scene, medium, field, opts);
+    if (rc) return rc;
+    rc = check_device(opts->device);
+    if (rc) return rc;
+    smp_plan *p = new smp_plan();
+    p->device = opts->device;
+    if (const char *eb = std::getenv("SMP_EVENT_BATCH")) p->event_batch = std::max(1, std::min(32, std::atoi(eb)));
+    p->scene = *scene;
+    p->medium = *medium;
+    p->opts = *opts;
+    std::memset(&p->stats, 0, sizeof(p->stats));
+    KParams &k = p->kp;
+    std::memset(&k, 0, sizeof(k));
+    for (int i = 0; i < 3; ++i) {
+        k.L[i] = float(scene->medium_l[i]);
+        k.R[i] = float(scene->medium_r[i]);
+        k.src_origin[i] = float(scene->light_origin[i]);
+        k.src_lens_origin[i] = float(scene->emitter_lens_origin[i]);
+        k.cam_origin[i] = float(scene->view_origin[i]);
+        k.cam_lens_origin[i] = float(scene->sensor_lens_origin[i]);
+    }
+    k.plane[0] = float(scene->light_plane[0]);
+    k.plane[1] = float(scene->light_plane[1]);
+    k.pixsize[0] = k.plane[0] / float(scene->tex_x);
+    k.pixsize[1] = k.plane[1] / float(scene->tex_y);
+    k.ct = std::cos(float(scene->half_theta_limit));
+    k.tex_x = scene->tex_x;
+    k.n_tex = scene->tex_x * scene->tex_y;
+    k.src_lens_active = scene->emitter_lens_active;
+    k.src_lens_sqap = float(scene->emitter_lens_aperture) * float(scene->emitter_lens_aperture);
+    k.src_lens_focal = float(scene->emitter_lens_focal_length);
+    // camera (camera.cpp:11-29): normalised dir and horizontal, vertical = dir x horizontal
+    float cd[3], ch[3];
+    for (int i = 0; i < 3; ++i) { cd[i] = float(scene->view_dir[i]); ch[i] = float(scene->view_horizontal[i]); }
+    float ld = std::sqrt(cd[0] * cd[0] + cd[1] * cd[1] + cd[2] * cd[2]);
+    float lh = std::sqrt(ch[0] * ch[0] + ch[1] * ch[1] + ch[2] * ch[2]);
+    for (int i = 0; i < 3; ++i) { cd[i] = cd[i] / ld; ch[i] = ch[i] / lh; }
+    for (int i = 0; i < 3; ++i) { k.cam_dir[i] = cd[i]; k.cam_h[i] = ch[i]; }
+    k.cam_v[0] = cd[1] * ch[2] - cd[2] * ch[1];
+    k.cam_v[1] = cd[2] * ch[0] - cd[0] * ch[2];
+    k.cam_v[2] = cd[0] * ch[1] - cd[1] * ch[0];
+    k.cam_plane[0] = float(scene->view_plane[0]);
+    k.cam_plane[1] = float(scene->view_plane[1]);
+    k.pl_min = float(scene->pathlength_range[0]);
+    k.pl_max = float(scene->pathlength_range[1]);
+    k.bounce = scene->use_bounce_decomposition;
+    k.cam_lens_active = scene->sensor_lens_active;
+    k.cam_lens_sqap = float(scene->sensor_lens_aperture) * float(scene->sensor_lens_aperture);
+    k.cam_lens_focal = float(scene->sensor_lens_focal_length);
+    k.ior1 = 1.0f;
+    k.ior2 = float(scene->ior);
+    // medium (medium.h:24-38)
+    k.sigma_t = float(medium->sigma_t);
+    k.albedo = float(medium->albedo);
+    k.mfp = 1.0f / float(medium->sigma_t);
+    if (k.sigma_t <= 1.19209290e-07f) { k.sigma_t = 0.0f; k.mfp = 1.0f; k.albedo = 0.0f; }
+    k.g = float(medium->g);
+    k.max_depth = opts->max_depth;
+    k.max_pathlength = float(opts->max_pathlength);
+    k.use_direct = opts->use_direct;
+    k.use_angular = opts->use_angular_sampling;
+    k.step_cap = opts->step_cap > 0 ? opts->step_cap : 10000000LL;
+    k.large_dist = sensor_march_budget(*opts, k.sigma_t);
+    if (k.step_cap > 2000000000LL) k.step_cap = 2000000000LL;
+    k.X = scene->x_res; k.Y = scene->y_res; k.Z = scene->z_res;
+    k.fp64 = opts->precision == SMP_PREC_MIXED;
+    k.rng = opts->rng;
+    k.seed = opts->seed;
+
+    // texture CDF
+    std::vector<float> cdf;
+    texture_cdf(scene->texture, k.n_tex, cdf);
+    cudaError_t e = cudaMalloc(&p->d_cdf, cdf.size() * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_cdf, cdf.data(), cdf.size() * sizeof(float), cudaMemcpyHostToDevice);
+    p->film_elems = size_t(k.X) * k.Y * k.Z;
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_film, p->film_elems * (k.fp64 ? 8 : 4));
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_counters, CNT_COUNT * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(p->d_film, 0, p->film_elems * (k.fp64 ? 8 : 4));
+    if (e == cudaSuccess) e = cudaEventCreate(&p->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&p->ev1);
+    if (e != cudaSuccess) {
+        plan_free(p);
+        return set_error(e == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "plan allocation: %s", cudaGetErrorString(e));
+    }
+    k.cdf = p->d_cdf;
+    k.film = p->d_film;
+    k.counters = p->d_counters;
+    rc = plan_setup_field(p, *field);
+    if (rc) { plan_free(p); return rc; }
+    *plan_out = p;
+    return SMP_OK;
+}
+
+int smp_plan_destroy(smp_plan *plan) {
+    if (!plan) return SMP_OK;
+    cudaSetDevice(plan->device);
+    plan_free(plan);
+    return SMP_OK;
+}
+
+int smp_plan_set_field(smp_plan *plan, const smp_field_desc *field) {
+    if (!plan || !field) return set_error(SMP_ERR_BAD_ARG, "NULL argument");
+    SMP_CUDA(cudaSetDevice(plan->device));
+    return plan_setup_field(plan, *field);
+}
+
+int smp_plan_clear(smp_plan *plan, void *stream) {
+    if (!plan) return set_error(SMP_ERR_BAD_ARG, "NULL plan");
+    SMP_CUDA(cudaSetDevice(plan->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    SMP_CUDA(cudaMemsetAsync(plan->d_film, 0, plan->film_elems * (plan->kp.fp64 ? 8 : 4), s));
+    std::memset(&plan->stats, 0, sizeof(plan->stats));
+    return SMP_OK;
+}
+
+// weight = Li * T_fresnel / N (photon.h:76-80) with T from scene.h:144-164, in float
+static float photon_weight(const smp_scene_desc &s, int64_t n) {
+    float ior = float(s.ior), T = 1.0f;
+    if (ior > 1.0f) {
+        float refr[3] = {0, 0, 0}, sum = 0.0f;
+        for (int i = 1; i < 3; ++i) { refr[i] = float(s.light_dir[i]) / ior; sum += refr[i] * refr[i]; }
+        refr[0] = std::sqrt(1.0f - sum);
+        if (float(s.light_dir[0]) < 0.0f) refr[0] *= -1.0f;
+        T = ior * ior * (1.0f - fresnel_host(float(s.light_dir[0]), refr[0], ior));
+    }
+    return float(s.Li) * T / float(n);
+}
+
+static int launch(smp_plan *plan, int64_t first, int64_t n, int64_t weight_photons, cudaStream_t s,
+                  const float *d_stream, const long long *d_offsets, smp_photon_record *d_records) {
+    if (n <= 0) return SMP_OK;
+    if (weight_photons <= 0) return set_error(SMP_ERR_BAD_ARG, "weight_photons must be positive");
+    KParams k = plan->kp;
+    k.weight = photon_weight(plan->scene, weight_photons);
+    k.first_photon = first;
+    k.n_photons = n;
+    k.stream = d_stream;
+    k.offsets = d_offsets;
+    k.records = d_records;
+    k.event_batch = plan->event_batch;
+    if (d_stream) k.rng = SMP_RNG_STREAM;
+    else if (k.rng == SMP_RNG_STREAM) return set_error(SMP_ERR_BAD_ARG, "rng STREAM needs uniforms");
+    SMP_CUDA(cudaMemsetAsync(plan->d_counters, 0, CNT_COUNT * sizeof(unsigned long long), s));
+    SMP_CUDA(cudaEventRecord(plan->ev0, s));
+    march_fn(plan->fk)<<<plan->grid, kBlock, plan->smem_bytes, s>>>(k);
+    SMP_CUDA(cudaGetLastError());
+    SMP_CUDA(cudaEventRecord(plan->ev1, s));
+    return SMP_OK;
+}
+
+static int collect_stats(smp_plan *plan, cudaStream_t s) {
+    unsigned long long c[CNT_COUNT];
+    SMP_CUDA(cudaMemcpyAsync(c, plan->d_counters, sizeof(c), cudaMemcpyDeviceToHost, s));
+    SMP_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.0f;
+    SMP_CUDA(cudaEventElapsedTime(&ms, plan->ev0, plan->ev1));
+    plan->stats.photons += (int64_t)c[CNT_PHOTONS];
+    plan->stats.er_steps += (int64_t)c[CNT_STEPS];
+    plan->stats.splats += (int64_t)c[CNT_SPLATS];
+    plan->stats.step_cap_hits += (int64_t)c[CNT_STEP_CAP];
+    plan->stats.nan_photons += (int64_t)c[CNT_NAN];
+    plan->stats.stream_exhausted += (int64_t)c[CNT_STREAM];
+    plan->stats.kernel_ms += ms;
+    if (c[CNT_STAGE_TIMEOUT]) return set_error(SMP_ERR_CUDA, "%llu block(s) timed out staging the field table", c[CNT_STAGE_TIMEOUT]);
+    if (c[CNT_STEP_CAP]) return set_error(SMP_ERR_STEP_CAP, "%llu photon(s) hit the per-photon step cap", c[CNT_STEP_CAP]);
+    if (c[CNT_NAN]) return set_error(SMP_ERR_NAN, "%llu photon(s) produced a non-finite state", c[CNT_NAN]);
+    if (c[CNT_STREAM]) return set_error(SMP_ERR_STREAM, "%llu photon(s) ran out of injected uniforms", c[CNT_STREAM]);
+    return SMP_OK;
+}
+
+int smp_plan_trace(smp_plan *plan, int64_t first_photon, int64_t n_photons, int64_t weight_photons, void *stream) {
+    if (!plan || n_photons < 0 || first_photon < 0) return set_error(SMP_ERR_BAD_ARG, "bad plan / range");
+    SMP_CUDA(cudaSetDevice(plan->device));
+    return launch(plan, first_photon, n_photons, weight_photons, static_cast<cudaStream_t>(stream), nullptr,
+                  nullptr, nullptr);
+}
+
+int smp_plan_stats(smp_plan *plan, smp_stats *stats_out) {
+    if (!plan || !stats_out) return set_error(SMP_ERR_BAD_ARG, "NULL argument");
+    SMP_CUDA(cudaSetDevice(plan->device));
+    int rc = collect_stats(plan, 0);
+    *stats_out = plan->stats;
+    return rc;
+}
+
+__global__ void film_to_double(const float *src, double *dst, size_t n) {
+    size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (; i < n; i += stride) dst[i] = double(src[i]);
+}
+
+int smp_plan_read_image(smp_plan *plan, double *dst, int dst_is_device, void *stream) {
+    if (!plan || !dst) return set_error(SMP_ERR_BAD_ARG, "NULL argument");
+    SMP_CUDA(cudaSetDevice(plan->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t n = plan->film_elems;
+    if (plan->kp.fp64) {
+        SMP_CUDA(cudaMemcpyAsync(dst, plan->d_film, n * 8, dst_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    } else if (dst_is_device) {
+        film_to_double<<<592, 256, 0, s>>>(static_cast<const float *>(plan->d_film), dst, n);
+        SMP_CUDA(cudaGetLastError());
+    } else {
+        std::vector<float> h(n);
+        SMP_CUDA(cudaMemcpyAsync(h.data(), plan->d_film, n * 4, cudaMemcpyDeviceToHost, s));
+        SMP_CUDA(cudaStreamSynchronize(s));
+        for (size_t i = 0; i < n; ++i) dst[i] = double(h[i]);
+    }
+    SMP_CUDA(cudaStreamSynchronize(s));
+    return SMP_OK;
+}
+
+int smp_plan_film(smp_plan *plan, void **dev_ptr, int32_t *bytes_per_pixel) {
+    if (!plan || !dev_ptr || !bytes_per_pixel) return set_error(SMP_ERR_BAD_ARG, "NULL argument");
+    *dev_ptr = plan->d_film;
+    *bytes_per_pixel = plan->kp.fp64 ? 8 : 4;
+    return SMP_OK;
+}
+
+int smp_plan_render(smp_plan *plan, int64_t n_photons, double *image_out, smp_stats *stats_out) {
+    if (!plan || n_photons < 0) return set_error(SMP_ERR_BAD_ARG, "bad plan / photon count");
+    int rc = smp_plan_clear(plan, nullptr);
+    if (rc) return rc;
+    if (n_photons > 0) {
+        rc = smp_plan_trace(plan, 0, n_photons, n_photons, nullptr);
+        if (rc) return rc;
+    }
+    int rs = n_photons > 0 ? collect_stats(plan, 0) : SMP_OK;
+    if (image_out) {
+        rc = smp_plan_read_image(plan, image_out, 0, nullptr);
+        if (rc) return rc;
+    }
+    if (stats_out) *stats_out = plan->stats;
+    return rs;
+}
+
+int smp_render(const smp_scene_desc *scene, const smp_medium_desc *medium, const smp_field_desc *field,
+               const smp_render_opts *opts, int64_t n_photons, double *image_out, smp_stats *stats_out) {
+    smp_plan *p = nullptr;
+    int rc = smp_plan_create(scene, medium, field, opts, &p);
+    if (rc) return rc;
+    rc = smp_plan_render(p, n_photons, image_out, stats_out);
+    std::string err = g_last_error;
+    smp_plan_destroy(p);
+    g_last_error = err;
+    return rc;
+}
+
+int smp_trace_photons(const smp_scene_desc *scene, const smp_medium_desc *medium, const smp_field_desc *field,
+                      const smp_render_opts *opts, int64_t first_photon, int64_t n_photons, int64_t weight_photons,
+                      const float *uniforms, const int64_t *offsets, smp_photon_record *records_out,
+                      double *image_out) {
+    if (n_photons <= 0 || !records_out) return set_error(SMP_ERR_BAD_ARG, "need n_photons > 0 and records_out");
+    if (uniforms && !offsets) return set_error(SMP_ERR_BAD_ARG, "uniforms without offsets");
+    smp_render_opts o = *opts;
+    if (uniforms) o.rng = SMP_RNG_STREAM;
+    else if (o.rng == SMP_RNG_STREAM) return set_error(SMP_ERR_BAD_ARG, "rng STREAM needs uniforms");
+    smp_plan *p = nullptr;
+    int rc = smp_plan_create(scene, medium, field, &o, &p);
+    if (rc) return rc;
+    float *d_u = nullptr;
+    long long *d_off = nullptr;
+    smp_photon_record *d_rec = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (uniforms) {
+        int64_t total = offsets[n_photons];
+        e = cudaMalloc(&d_u, size_t(std::max<int64_t>(total, 1)) * sizeof(float));
+        if (e == cudaSuccess && total > 0) e = cudaMemcpy(d_u, uniforms, size_t(total) * sizeof(float), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMalloc(&d_off, size_t(n_photons + 1) * sizeof(long long));
+        if (e == cudaSuccess) e = cudaMemcpy(d_off, offsets, size_t(n_photons + 1) * sizeof(long long), cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&d_rec, size_t(n_photons) * sizeof(smp_photon_record));
+    if (e == cudaSuccess) e = cudaMemset(d_rec, 0, size_t(n_photons) * sizeof(smp_photon_record));
+    if (e != cudaSuccess) {
+        rc = set_error(SMP_ERR_CUDA, "trace buffers: %s", cudaGetErrorString(e));
+    } else {
+        rc = launch(p, first_photon, n_photons, weight_photons, 0, d_u, d_off, d_rec);
+        int rs = rc ? rc : collect_stats(p, 0);
+        if (!rc) {
+            e = cudaMemcpy(records_out, d_rec, size_t(n_photons) * sizeof(smp_photon_record), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) rc = set_error(SMP_ERR_CUDA, "records copy: %s", cudaGetErrorString(e));
+        }
+        if (!rc && image_out) rc = smp_plan_read_image(p, image_out, 0, nullptr);
+        if (!rc) rc = rs;
+    }
+    std::string err = g_last_error;
+    cudaFree(d_u);
+    cudaFree(d_off);
+    cudaFree(d_rec);
+    smp_plan_destroy(p);
+    g_last_error = err;
+    return rc;
+}
+
+int smp_field_eval(const smp_field_desc *field, double scaling, int64_t n_points, const double *points,
+                   double *n_out, double *grad_out) {
+    if (!field || n_points < 0 || (n_points > 0 && (!points || !n_out || !grad_out)))
+        return set_error(SMP_ERR_BAD_ARG, "bad arguments");
+    int fk;
+    int rc = field_kind(*field, &fk);
+    if (rc) return rc;
+    rc = check_device(0);
+    if (rc) return rc;
+    if (n_points == 0) return SMP_OK;
+    FieldParams F;
+    fill_field_params(*field, fk, F);
+    float4 *d_cen = nullptr;
+    float *d_coeff = nullptr;
+    double *d_pts = nullptr, *d_n = nullptr, *d_g = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (fk == FK_SOURCES) {
+        std::vector<float4> c;
+        source_centres(*field, c);
+        e = cudaMalloc(&d_cen, c.size() * sizeof(float4));
+        if (e == cudaSuccess) e = cudaMemcpy(d_cen, c.data(), c.size() * sizeof(float4), cudaMemcpyHostToDevice);
+        F.centers = d_cen;
+    }
+    if (fk == FK_SPLINE && e == cudaSuccess) {
+        std::vector<float> delta;
+        F.spline_base = spline_offsets(*field, delta);
+        e = cudaMalloc(&d_coeff, delta.size() * sizeof(float));
+        if (e == cudaSuccess) e = cudaMemcpy(d_coeff, delta.data(), delta.size() * sizeof(float), cudaMemcpyHostToDevice);
+        F.coeff = d_coeff;
+    }
+    float4 *d_tab = nullptr;
+    if (fk <= FK_BESSEL2 && e == cudaSuccess) {
+        std::vector<float4> tab;
+        bessel_table(field->mode, kBesselMaxX, tab);
+        e = cudaMalloc(&d_tab, tab.size() * sizeof(float4));
+        if (e == cudaSuccess) e = cudaMemcpy(d_tab, tab.data(), tab.size() * sizeof(float4), cudaMemcpyHostToDevice);
+        F.btab = d_tab;
+        F.bnodes = int(tab.size());
+    }
+    size_t np = size_t(n_points);
+    if (e == cudaSuccess) e = cudaMalloc(&d_pts, np * 3 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_n, np * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_g, np * 3 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpy(d_pts, points, np * 3 * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        int blocks = int((np + 255) / 256);
+        float s = float(scaling);
+        switch (fk) {
+            case FK_BESSEL0: field_probe_kernel<FK_BESSEL0><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
+            case FK_BESSEL1: field_probe_kernel<FK_BESSEL1><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
+            case FK_BESSEL2: field_probe_kernel<FK_BESSEL2><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
+            case FK_PLANEWAVE: field_probe_kernel<FK_PLANEWAVE><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
+            case FK_SOURCES: field_probe_kernel<FK_SOURCES><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
+            default: field_probe_kernel<FK_SPLINE><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
+        }
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(n_out, d_n, np * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(grad_out, d_g, np * 3 * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d_cen);
+    cudaFree(d_coeff);
+    cudaFree(d_tab);
+    cudaFree(d_pts);
+    cudaFree(d_n);
+    cudaFree(d_g);
+    if (e != cudaSuccess) return set_error(SMP_ERR_CUDA, "field probe: %s", cudaGetErrorString(e));
+    return SMP_OK;
+}
+
+int smp_render_batch(const smp_scene_desc *, const smp_instance_desc *, int32_t, const smp_render_opts *,
+                     double *, smp_stats *) {
+    return set_error(SMP_ERR_UNSUPPORTED, "smp_render_batch is not built yet");
+}
+
+}  // extern "C"

@@ -1,0 +1,111 @@
+// kparams.h -- the parameter block every march launch receives by value (__grid_constant__):
+// scene, medium, film, field and work range, already converted to the device's float layout.
+// Shared by the host (capi.cu) and the device code (march.cuh).
+#pragma once
+#include <stdint.h>
+#include "../../include/simpler_b200.h"
+
+namespace smp {
+
+// Field kernels are compiled per kind; the Bessel order is a compile-time constant for m <= 2.
+enum FieldKind : int {
+    FK_BESSEL0 = 0,
+    FK_BESSEL1 = 1,
+    FK_BESSEL2 = 2,
+    FK_BESSELN = 3,
+    FK_PLANEWAVE = 4,
+    FK_SOURCES = 5,
+    FK_SPLINE = 6,
+    FK_COUNT = 7
+};
+
+struct FieldParams {
+    int kind;
+    int mode;               // Bessel order
+    float n_o;
+    float egap, sgap;       // field is n_o outside sgap <= x <= egap
+    float k_r;              // 2*pi*f/c
+    float amp;              // Bessel n_max
+    float max_scaling;      // n_clip / n_max
+    float phi_min, phi_range;
+    // plane waves
+    int n_waves;
+    float wamp[SMP_MAX_WAVES];
+    float wk[SMP_MAX_WAVES][3];
+    float wphase[SMP_MAX_WAVES];
+    // FUS point sources: centres as float4 (xyz, unused), arc 1 then arc 2
+    int n_coeff, nsources, active1, active2;
+    float n_scaling, phase1, phase2;
+    const float4 *centers;  // 2*nsources entries (arc 1 block, arc 2 block)
+    // spline
+    int N[3];
+    float xmin[3], xres[3];
+    float spline_base;      // coefficients are stored as offsets from this value
+    const float *coeff;
+    // Bessel table: node i at x = i*bh holds (J_m, J_m', J_m+1, J_m+1')(x); bnodes nodes
+    const float4 *btab;
+    int bnodes;
+    float bh, binv_h;
+};
+
+struct KParams {
+    // medium box (block.cpp)
+    float L[3], R[3];
+    // textured source (area_textured_source)
+    float src_origin[3];
+    float plane[2], pixsize[2];
+    float ct;
+    int tex_x, n_tex;
+    const float *cdf;       // n_tex + 1 entries
+    int src_lens_active;
+    float src_lens_origin[3], src_lens_sqap, src_lens_focal;
+    // camera
+    float cam_origin[3], cam_dir[3], cam_h[3], cam_v[3];
+    float cam_plane[2];
+    float pl_min, pl_max;
+    int bounce;
+    int cam_lens_active;
+    float cam_lens_origin[3], cam_lens_sqap, cam_lens_focal;
+    // smooth dielectric (ior1 = 1, ior2 = scene ior)
+    float ior1, ior2;
+    // medium
+    float sigma_t, albedo, mfp, g;
+    // renderer
+    int max_depth;
+    float max_pathlength;
+    int use_direct, use_angular;
+    float weight;
+    float h0;
+    float large_dist;       // movePhotonTillSensor path budget (LargeDist)
+    int precision;
+    long long step_cap;
+    // film
+    void *film;
+    int X, Y, Z;
+    int fp64;               // SMP_PREC_MIXED: FP64 path length + FP64 film
+    // uniforms
+    int rng;
+    unsigned long long seed;
+    const float *stream;
+    const long long *offsets;
+    // work: photons [first_photon, first_photon + n_photons)
+    long long first_photon, n_photons;
+    unsigned long long *counters;     // device scratch, see Counter
+    smp_photon_record *records;       // trace mode only (indexed by photon - first_photon)
+    int event_batch;                  // lanes that must finish a march before the warp runs events
+    FieldParams field;
+};
+
+enum Counter : int {
+    CNT_NEXT_PHOTON = 0,   // work distribution (relative to first_photon)
+    CNT_STEPS = 1,
+    CNT_SPLATS = 2,
+    CNT_STEP_CAP = 3,
+    CNT_NAN = 4,
+    CNT_STREAM = 5,
+    CNT_PHOTONS = 6,
+    CNT_STAGE_TIMEOUT = 7,   // a block gave up waiting for its shared-memory staging copy
+    CNT_COUNT = 8
+};
+
+}  // namespace smp

@@ -1,0 +1,128 @@
+"""Python entry points over the C ABI: render, plans, parity traces and field probes."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from .scene import Setup
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def render(setup: Setup, n_photons: int) -> tuple[np.ndarray, L.Stats]:
+    """One-shot render (the reference's Renderer::renderImage). Returns the film as a
+    (z, y, x) float64 array -- index z*X*Y + y*X + x, the reference's Image3 layout -- and stats."""
+    lib = L.load()
+    sc, md, fd, op = setup.descs()
+    img = np.zeros(setup.film_shape(), dtype=np.float64)
+    st = L.Stats()
+    L.check(lib.smp_render(C.byref(sc), C.byref(md), C.byref(fd), C.byref(op), int(n_photons), _ptr(img), C.byref(st)))
+    return img, st
+
+
+class Plan:
+    """Device-resident scene + film; repeated renders pay no setup."""
+
+    def __init__(self, setup: Setup):
+        self.setup = setup
+        self.lib = L.load()
+        self._descs = setup.descs()
+        sc, md, fd, op = self._descs
+        h = C.c_void_p()
+        L.check(self.lib.smp_plan_create(C.byref(sc), C.byref(md), C.byref(fd), C.byref(op), C.byref(h)))
+        self.handle = h
+
+    def clear(self, stream: int = 0) -> None:
+        L.check(self.lib.smp_plan_clear(self.handle, C.c_void_p(stream)))
+
+    def trace(self, first: int, n: int, weight_photons: int, stream: int = 0) -> None:
+        L.check(self.lib.smp_plan_trace(self.handle, int(first), int(n), int(weight_photons), C.c_void_p(stream)))
+
+    def read_image(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.zeros(self.setup.film_shape(), dtype=np.float64)
+        L.check(self.lib.smp_plan_read_image(self.handle, _ptr(out), 0, None))
+        return out
+
+    def read_image_device(self, dev_ptr: int, stream: int = 0) -> None:
+        L.check(self.lib.smp_plan_read_image(self.handle, C.c_void_p(dev_ptr), 1, C.c_void_p(stream)))
+
+    def film(self) -> tuple[int, int]:
+        p = C.c_void_p()
+        b = C.c_int32()
+        L.check(self.lib.smp_plan_film(self.handle, C.byref(p), C.byref(b)))
+        return p.value, b.value
+
+    def stats(self) -> L.Stats:
+        st = L.Stats()
+        L.check(self.lib.smp_plan_stats(self.handle, C.byref(st)))
+        return st
+
+    def render(self, n_photons: int) -> tuple[np.ndarray, L.Stats]:
+        img = np.zeros(self.setup.film_shape(), dtype=np.float64)
+        st = L.Stats()
+        L.check(self.lib.smp_plan_render(self.handle, int(n_photons), _ptr(img), C.byref(st)))
+        return img, st
+
+    def set_field(self, setup: Setup) -> None:
+        fd = setup.field_desc()
+        L.check(self.lib.smp_plan_set_field(self.handle, C.byref(fd)))
+        self._fd_keep = fd
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.smp_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def trace_photons(setup: Setup, first: int, n: int, weight_photons: int,
+                  uniforms: np.ndarray | None = None, offsets: np.ndarray | None = None,
+                  with_image: bool = True):
+    """Parity mode: per-photon records (and the film) for photons [first, first+n)."""
+    lib = L.load()
+    sc, md, fd, op = setup.descs()
+    recs = (L.PhotonRecord * n)()
+    img = np.zeros(setup.film_shape(), dtype=np.float64) if with_image else None
+    u = o = None
+    if uniforms is not None:
+        u = np.ascontiguousarray(uniforms, dtype=np.float32)
+        o = np.ascontiguousarray(offsets, dtype=np.int64)
+    rc = lib.smp_trace_photons(C.byref(sc), C.byref(md), C.byref(fd), C.byref(op), int(first), int(n),
+                               int(weight_photons), _ptr(u) if u is not None else None,
+                               _ptr(o) if o is not None else None, recs, _ptr(img) if img is not None else None)
+    L.check(rc)
+    return recs, img
+
+
+def field_eval(setup: Setup, scaling: float, points: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """n and grad n at points (N,3) with the march kernel's own field code."""
+    lib = L.load()
+    fd = setup.field_desc()
+    pts = np.ascontiguousarray(points, dtype=np.float64)
+    n = np.zeros(len(pts))
+    g = np.zeros((len(pts), 3))
+    L.check(lib.smp_field_eval(C.byref(fd), float(scaling), len(pts), _ptr(pts), _ptr(n), _ptr(g)))
+    return n, g
+
+
+def records_to_arrays(recs) -> dict:
+    """Flatten PhotonRecords into numpy arrays for comparisons."""
+    n = len(recs)
+    raw = np.ctypeslib.as_array(C.cast(recs, C.POINTER(C.c_uint8)), shape=(n * C.sizeof(L.PhotonRecord),))
+    dt = np.dtype([
+        ("photon", "<i8"), ("end", "<i4"), ("draws", "<i4"), ("depth", "<i4"), ("n_splats", "<i4"),
+        ("pos", "<f4", 3), ("dir", "<f4", 3), ("total_optical", "<f8"), ("er_steps", "<i8"),
+        ("splats", [("p", "<f4", 3), ("depth", "<i4"), ("pathlength", "<f8"), ("value", "<f8")], L.SMP_TRACE_MAX_SPLATS),
+    ])
+    assert dt.itemsize == C.sizeof(L.PhotonRecord), (dt.itemsize, C.sizeof(L.PhotonRecord))
+    return raw.view(dt).copy()

@@ -1,0 +1,56 @@
+"""Photon-by-photon comparison of GPU records with oracle records."""
+from __future__ import annotations
+
+import numpy as np
+
+# positions within 1e-4 mm, directions within 1e-5 rad
+POS_TOL_M = 1e-7
+DIR_TOL_RAD = 1e-5
+PATH_TOL_M = 1e-7
+VALUE_RTOL = 1e-4
+
+
+def _angle(a, b):
+    na = np.linalg.norm(a, axis=-1)
+    nb = np.linalg.norm(b, axis=-1)
+    c = np.sum(a * b, axis=-1) / np.maximum(na * nb, 1e-30)
+    return np.arccos(np.clip(c, -1.0, 1.0))
+
+
+def compare_records(gpu, ref) -> dict:
+    """Return per-photon match flags and diagnostics."""
+    n = len(ref)
+    same_events = (gpu["end"] == ref["end"]) & (gpu["draws"] == ref["draws"]) & (gpu["depth"] == ref["depth"]) & (
+        gpu["n_splats"] == ref["n_splats"])
+    pos_err = np.max(np.abs(gpu["pos"].astype(np.float64) - ref["pos"].astype(np.float64)), axis=1)
+    dir_err = _angle(gpu["dir"].astype(np.float64), ref["dir"].astype(np.float64))
+    path_err = np.abs(gpu["total_optical"] - ref["total_optical"])
+    k = np.minimum(ref["n_splats"], gpu["splats"].shape[1])
+    spl_pos = np.zeros(n)
+    spl_path = np.zeros(n)
+    spl_val = np.zeros(n)
+    spl_depth = np.ones(n, dtype=bool)
+    for i in range(gpu["splats"].shape[1]):
+        m = (i < k) & same_events
+        if not m.any():
+            continue
+        gs, rs = gpu["splats"][:, i], ref["splats"][:, i]
+        e = np.max(np.abs(gs["p"].astype(np.float64) - rs["p"].astype(np.float64)), axis=1)
+        spl_pos = np.where(m, np.maximum(spl_pos, e), spl_pos)
+        spl_path = np.where(m, np.maximum(spl_path, np.abs(gs["pathlength"] - rs["pathlength"])), spl_path)
+        rel = np.abs(gs["value"] - rs["value"]) / np.maximum(np.abs(rs["value"]), 1e-30)
+        spl_val = np.where(m, np.maximum(spl_val, rel), spl_val)
+        spl_depth &= ~m | (gs["depth"] == rs["depth"])
+    ok = same_events & (pos_err <= POS_TOL_M) & (dir_err <= DIR_TOL_RAD) & (path_err <= PATH_TOL_M) & (
+        spl_pos <= POS_TOL_M) & (spl_path <= PATH_TOL_M) & (spl_val <= VALUE_RTOL) & spl_depth
+    return {"ok": ok, "same_events": same_events, "pos_err": pos_err, "dir_err": dir_err, "path_err": path_err,
+            "spl_pos": spl_pos, "spl_path": spl_path, "spl_val": spl_val}
+
+
+def summary(c: dict) -> str:
+    n = len(c["ok"])
+    return (f"{c['ok'].sum()}/{n} photons within tolerance; events equal {c['same_events'].sum()}/{n}; "
+            f"max pos {c['pos_err'][c['same_events']].max() if c['same_events'].any() else 0:.3g} m, "
+            f"max dir {c['dir_err'][c['same_events']].max() if c['same_events'].any() else 0:.3g} rad, "
+            f"max path {c['path_err'][c['same_events']].max() if c['same_events'].any() else 0:.3g} m, "
+            f"max splat rel value {c['spl_val'].max():.3g}")
