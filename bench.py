@@ -1,0 +1,313 @@
+#!/usr/bin/env python
+"""bench.py -- photon paths/s of the B200 photon march.
+
+Workload (the precision scale-up configuration): cylindrical Bessel mode 1 field, dn 2e-3 at
+848 kHz, 10 mm cube, sigma_s 1/mm, albedo 0.95, HG g 0.85, 64x64 Bernoulli(0.5) texture (seed 1),
+512x512 px x 128 path-length bins over 0-100 mm, FP32 march with FP64 path length and film.
+One step traces 5e6 photons (1/20 of the 1e8-photon render) into the resident film.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank traces its own photon range (counter-based streams keyed by the global
+photon index, so the render is the same for any GPU count) and the film is reduced to rank 0 over
+NCCL every step. Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import simpler_b200 as sb  # noqa: E402
+from simpler_b200 import _lib as L  # noqa: E402
+from simpler_b200.roofline import flop_per_step_bessel  # noqa: E402
+
+METRIC = "photon paths/s"
+RENDER_PHOTONS = 100_000_000
+PHOTONS_PER_STEP = 5_000_000
+WORKLOAD = "precision scale-up: Bessel mode 1, dn 2e-3, sigma_s 1/mm, albedo 0.95, g 0.85, 1e8-photon render"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--photons-per-step", type=int, default=PHOTONS_PER_STEP)
+    return ap.parse_args()
+
+
+def workload(device: int = 0) -> sb.Setup:
+    return sb.config_precision(device=device)
+
+
+def config_json(args, per_step: int) -> dict:
+    s = workload()
+    return {
+        "workload": WORKLOAD,
+        "photons_per_step_per_gpu": per_step,
+        "render_photons": RENDER_PHOTONS,
+        "field": "bessel", "mode": s.mode, "n_max": s.n_max, "f_u": s.f_u,
+        "medium_mm": 10.0, "sigma_s_per_mm": 1.0, "albedo": s.albedo, "g": s.g,
+        "film": [s.spatial_x, s.spatial_y, s.path_length_bins],
+        "er_stepsize_m": s.er_stepsize, "precision_levels": s.precision,
+        "rng": "philox-4x32-10 keyed by global photon index",
+        "precision": "fp32 march, fp64 path length + fp64 film",
+        "l2": "film 256 MiB (fp64) exceeds the 126 MB L2; no flush needed",
+    }
+
+
+# ---- clocks ---------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---- CPU baseline: the oracle port on the host cores ----------------------------------------------
+def _oracle_lib():
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "liboracle_fast.so"))
+    P = C.POINTER
+    vp = C.c_void_p
+    lib.orc_render.argtypes = [P(L.SceneDesc), P(L.MediumDesc), P(L.FieldDesc), P(L.RenderOpts), C.c_int, C.c_int,
+                               C.c_int64, C.c_int64, C.c_int64, vp, vp, vp, vp]
+    return lib
+
+
+def cpu_trace(n: int, first: int, threads: int) -> float:
+    """Trace n photons of the workload with the CPU restatement; returns seconds (wall)."""
+    lib = _oracle_lib()
+    s = workload()
+    sc, md, fd, op = s.descs()
+    t0 = time.perf_counter()
+    rc = lib.orc_render(C.byref(sc), C.byref(md), C.byref(fd), C.byref(op), 32, threads, first, n, RENDER_PHOTONS,
+                        None, None, None, None)
+    dt = time.perf_counter() - t0
+    assert rc == 0
+    return dt
+
+
+def cpu_baseline(target_s: float = 12.0) -> dict:
+    """Trace batches of the workload on all host threads until about target_s of wall time."""
+    threads = os.cpu_count() or 1
+    batch = max(threads * 16, 64)
+    done, dt, first = 0, 0.0, 0
+    while dt < target_s and done < 2_000_000:
+        dt += cpu_trace(batch, first, threads)
+        done += batch
+        first += batch
+    return {"value": done / dt, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"photons 0..{done} of the same workload ({done} photon paths) in {dt:.1f} s on all "
+                      f"{threads} host threads, CPU restatement built with the reference's -O3 -ffast-math "
+                      f"flags, film accumulation skipped"}
+
+
+# ---- reference arm ---------------------------------------------------------------------------------
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    per_step = max(threads * 4, 32)
+    for i in range(args.warmup):
+        cpu_trace(per_step, i * per_step, threads)
+    times = []
+    for i in range(args.steps):
+        times.append(cpu_trace(per_step, (args.warmup + i) * per_step, threads))
+    tot = sum(times)
+    v = per_step * args.steps / tot
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": config_json(args, per_step),
+        "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
+                         "sample": f"{per_step} photons per step of the same workload on {threads} host threads "
+                                   f"(the reference does not build here; CPU restatement with its -O3 -ffast-math flags)"},
+        "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- our arm -------------------------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
+    per_step = args.photons_per_step
+    setup = workload(local)
+    plan = sb.Plan(setup)
+    stream = torch.cuda.current_stream()
+    h = stream.cuda_stream
+    nz, ny, nx = setup.film_shape()
+    film = torch.zeros((nz, ny, nx), dtype=torch.float64, device=f"cuda:{local}") if world > 1 else None
+
+    def step(i):
+        first = (i * world + rank) * per_step
+        plan.trace(first, per_step, RENDER_PHOTONS, stream=h)
+        if world > 1:
+            plan.read_image_device(film.data_ptr(), stream=h)
+            dist.reduce(film, dst=0)
+
+    plan.clear(h)
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    st0 = plan.stats()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.steps):
+        step(args.warmup + i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    st1 = plan.stats()
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    steps_timed = st1.er_steps - st0.er_steps
+    kernel_ms = st1.kernel_ms - st0.kernel_ms
+    launches = args.steps
+    value = per_step * args.steps * world / (ms / 1e3)
+
+    out = None
+    if rank == 0:
+        peak = C.c_double()
+        L.check(L.load().smp_fp32_peak(local, C.byref(peak)))
+        fps = flop_per_step_bessel(setup.mode)
+        per_launch_s = kernel_ms / launches / 1e3
+        achieved = fps * (steps_timed / launches) / per_launch_s / 1e12
+        roof = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                "frac": achieved / peak.value, "traffic": _profile_traffic(),
+                "flop_per_er_step": fps, "er_steps_per_launch": steps_timed / launches,
+                "peak_source": "FP32 FMA throughput measured live on this GPU (smp_fp32_peak)"}
+        e2e = run_e2e(args, setup, min(args.steps, 3), per_step)
+        out = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32", "data": "synthetic", "config": config_json(args, per_step),
+            "roofline": roof, "cpu_baseline": cpu_baseline() if world == 1 else None, "e2e": e2e,
+            "gpu_launches": launches * 2, "clocks": clk,
+            "er_steps_per_s": steps_timed * world / (ms / 1e3),
+        }
+    plan.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+def _profile_traffic():
+    """DRAM bytes per launch of the march kernel, from the committed ncu summary (if present)."""
+    path = os.path.join(ROOT, "profiles", "march_kernel_precision_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch"):
+                    return float(line.split("=")[1])
+    except OSError:
+        pass
+    return None
+
+
+def run_e2e(args, setup, steps: int, per_step: int) -> dict:
+    """The same metric through the one-shot C-ABI call with a host film (CudaRenderer::renderImage's
+    contract): scene upload, trace, FP64 film read back to host memory, every step."""
+    lib = L.load()
+    sc, md, fd, op = setup.descs()
+    img = np.zeros(setup.film_shape(), dtype=np.float64)
+    stt = L.Stats()
+    t_total = 0.0
+    for i in range(steps + 1):
+        t0 = time.perf_counter()
+        L.check(lib.smp_render(C.byref(sc), C.byref(md), C.byref(fd), C.byref(op), per_step,
+                               C.c_void_p(img.ctypes.data), C.byref(stt)))
+        dt = time.perf_counter() - t0
+        if i > 0:
+            t_total += dt
+    tex = setup.texture.size
+    h2d = (tex + 1) * 4 + 2050 * 16 + 1024          # texture CDF + Bessel table + parameters
+    d2h = img.nbytes + 64
+    return {"value": per_step * steps / t_total, "unit": METRIC, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "steps": steps,
+            "call": "smp_render (one-shot plan, host film) per step, wall clock"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -283,6 +283,11 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
                      int32_t n_inst, const smp_render_opts *opts,
                      double *images_out, smp_stats *stats_out);
 
+/* Measurement utility with no counterpart in the reference: the device's FP32 FMA throughput
+   (TFLOP/s, 2 FLOP per FMA) measured with independent FMA chains on every SM; the roofline
+   denominator for the march, which is bound by the FP32 and issue pipes. */
+int smp_fp32_peak(int device, double *tflops_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,7 +1,8 @@
 """simpler_b200: the refractive radiative transfer photon march of simplEr on B200 (sm_100a).
 
 The compute lives in libsimpler_b200.so (hand-written CUDA behind a C ABI, include/simpler_b200.h);
-this package is the Python host side. Importing it loads the library: there is no CPU fallback.
+this package is the Python host side. Every entry point loads the library on first use and raises
+if it is missing: there is no CPU fallback.
 """
 from . import _lib
 from ._lib import SmpError, check_layout, load
@@ -12,5 +13,3 @@ __all__ = [
     "SmpError", "check_layout", "load", "Plan", "field_eval", "records_to_arrays", "render", "trace_photons",
     "Setup", "bernoulli_texture", "config_planewave", "config_plain_small", "config_precision", "disk_texture",
 ]
-
-load()

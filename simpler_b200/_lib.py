@@ -139,7 +139,7 @@ EXPORTS = [
     "smp_version", "smp_last_error", "smp_device_count", "smp_sizeof", "smp_render",
     "smp_plan_create", "smp_plan_destroy", "smp_plan_set_field", "smp_plan_clear", "smp_plan_trace",
     "smp_plan_read_image", "smp_plan_film", "smp_plan_stats", "smp_plan_render", "smp_trace_photons",
-    "smp_field_eval", "smp_texture_cdf", "smp_spline_prefilter", "smp_render_batch",
+    "smp_field_eval", "smp_texture_cdf", "smp_spline_prefilter", "smp_render_batch", "smp_fp32_peak",
 ]
 
 _lib = None
@@ -182,6 +182,7 @@ def load() -> C.CDLL:
     lib.smp_texture_cdf.argtypes = [vp, C.c_int32, C.c_int32, vp]
     lib.smp_spline_prefilter.argtypes = [vp, vp, vp]
     lib.smp_render_batch.argtypes = [P(SceneDesc), P(InstanceDesc), C.c_int32, P(RenderOpts), vp, P(Stats)]
+    lib.smp_fp32_peak.argtypes = [C.c_int, P(C.c_double)]
     _lib = lib
     return lib
 

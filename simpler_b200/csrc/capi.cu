@@ -201,6 +201,7 @@ static void fill_field_params(const smp_field_desc &f, int fk, FieldParams &F) {
     // rif_base.h:149-153 in Float: lambda = c/f, k = 2*pi/lambda
     float lambda = float(f.speed_u) / float(f.f_u);
     F.k_r = (2.0f * 3.14159265358979f) / lambda;
+    F.inv_k = 1.0f / F.k_r;
     F.amp = float(f.n_max);
     F.max_scaling = float(f.n_clip) / float(f.n_max);       // rif_analytical.h:222
     F.phi_min = float(f.phi_min);
@@ -297,8 +298,16 @@ struct smp_plan {
     size_t film_elems = 0;
     unsigned long long *d_counters = nullptr;
     smp_stats stats;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> launches;   // since the last clear
 };
+
+static void drop_launch_events(smp_plan *p) {
+    for (auto &e : p->launches) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    p->launches.clear();
+}
 
 static void plan_free(smp_plan *p) {
     if (!p) return;
@@ -308,8 +317,7 @@ static void plan_free(smp_plan *p) {
     cudaFree(p->d_btab);
     cudaFree(p->d_film);
     cudaFree(p->d_counters);
-    if (p->ev0) cudaEventDestroy(p->ev0);
-    if (p->ev1) cudaEventDestroy(p->ev1);
+    drop_launch_events(p);
     delete p;
 }
 
@@ -489,8 +497,7 @@ int smp_plan_create(const smp_scene_desc *scene, const smp_medium_desc *medium, 
     if (e == cudaSuccess) e = cudaMalloc(&p->d_film, p->film_elems * (k.fp64 ? 8 : 4));
     if (e == cudaSuccess) e = cudaMalloc(&p->d_counters, CNT_COUNT * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(p->d_film, 0, p->film_elems * (k.fp64 ? 8 : 4));
-    if (e == cudaSuccess) e = cudaEventCreate(&p->ev0);
-    if (e == cudaSuccess) e = cudaEventCreate(&p->ev1);
+    if (e == cudaSuccess) e = cudaMemset(p->d_counters, 0, CNT_COUNT * sizeof(unsigned long long));
     if (e != cudaSuccess) {
         plan_free(p);
         return set_error(e == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "plan allocation: %s", cudaGetErrorString(e));
@@ -522,6 +529,9 @@ int smp_plan_clear(smp_plan *plan, void *stream) {
     SMP_CUDA(cudaSetDevice(plan->device));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     SMP_CUDA(cudaMemsetAsync(plan->d_film, 0, plan->film_elems * (plan->kp.fp64 ? 8 : 4), s));
+    SMP_CUDA(cudaMemsetAsync(plan->d_counters, 0, CNT_COUNT * sizeof(unsigned long long), s));
+    SMP_CUDA(cudaStreamSynchronize(s));
+    drop_launch_events(plan);
     std::memset(&plan->stats, 0, sizeof(plan->stats));
     return SMP_OK;
 }
@@ -553,27 +563,38 @@ static int launch(smp_plan *plan, int64_t first, int64_t n, int64_t weight_photo
     k.event_batch = plan->event_batch;
     if (d_stream) k.rng = SMP_RNG_STREAM;
     else if (k.rng == SMP_RNG_STREAM) return set_error(SMP_ERR_BAD_ARG, "rng STREAM needs uniforms");
-    SMP_CUDA(cudaMemsetAsync(plan->d_counters, 0, CNT_COUNT * sizeof(unsigned long long), s));
-    SMP_CUDA(cudaEventRecord(plan->ev0, s));
+    // the work counter restarts per launch; the statistics accumulate until smp_plan_clear
+    SMP_CUDA(cudaMemsetAsync(plan->d_counters + CNT_NEXT_PHOTON, 0, sizeof(unsigned long long), s));
+    cudaEvent_t e0, e1;
+    SMP_CUDA(cudaEventCreate(&e0));
+    SMP_CUDA(cudaEventCreate(&e1));
+    plan->launches.emplace_back(e0, e1);
+    SMP_CUDA(cudaEventRecord(e0, s));
     march_fn(plan->fk)<<<plan->grid, kBlock, plan->smem_bytes, s>>>(k);
     SMP_CUDA(cudaGetLastError());
-    SMP_CUDA(cudaEventRecord(plan->ev1, s));
+    SMP_CUDA(cudaEventRecord(e1, s));
     return SMP_OK;
 }
 
-static int collect_stats(smp_plan *plan, cudaStream_t s) {
+// Statistics since the last clear: device counters plus the summed launch times. Synchronises the
+// device.
+static int collect_stats(smp_plan *plan) {
     unsigned long long c[CNT_COUNT];
-    SMP_CUDA(cudaMemcpyAsync(c, plan->d_counters, sizeof(c), cudaMemcpyDeviceToHost, s));
-    SMP_CUDA(cudaStreamSynchronize(s));
-    float ms = 0.0f;
-    SMP_CUDA(cudaEventElapsedTime(&ms, plan->ev0, plan->ev1));
-    plan->stats.photons += (int64_t)c[CNT_PHOTONS];
-    plan->stats.er_steps += (int64_t)c[CNT_STEPS];
-    plan->stats.splats += (int64_t)c[CNT_SPLATS];
-    plan->stats.step_cap_hits += (int64_t)c[CNT_STEP_CAP];
-    plan->stats.nan_photons += (int64_t)c[CNT_NAN];
-    plan->stats.stream_exhausted += (int64_t)c[CNT_STREAM];
-    plan->stats.kernel_ms += ms;
+    SMP_CUDA(cudaDeviceSynchronize());
+    SMP_CUDA(cudaMemcpy(c, plan->d_counters, sizeof(c), cudaMemcpyDeviceToHost));
+    double ms_total = 0.0;
+    for (auto &e : plan->launches) {
+        float ms = 0.0f;
+        SMP_CUDA(cudaEventElapsedTime(&ms, e.first, e.second));
+        ms_total += ms;
+    }
+    plan->stats.photons = (int64_t)c[CNT_PHOTONS];
+    plan->stats.er_steps = (int64_t)c[CNT_STEPS];
+    plan->stats.splats = (int64_t)c[CNT_SPLATS];
+    plan->stats.step_cap_hits = (int64_t)c[CNT_STEP_CAP];
+    plan->stats.nan_photons = (int64_t)c[CNT_NAN];
+    plan->stats.stream_exhausted = (int64_t)c[CNT_STREAM];
+    plan->stats.kernel_ms = ms_total;
     if (c[CNT_STAGE_TIMEOUT]) return set_error(SMP_ERR_CUDA, "%llu block(s) timed out staging the field table", c[CNT_STAGE_TIMEOUT]);
     if (c[CNT_STEP_CAP]) return set_error(SMP_ERR_STEP_CAP, "%llu photon(s) hit the per-photon step cap", c[CNT_STEP_CAP]);
     if (c[CNT_NAN]) return set_error(SMP_ERR_NAN, "%llu photon(s) produced a non-finite state", c[CNT_NAN]);
@@ -591,7 +612,7 @@ int smp_plan_trace(smp_plan *plan, int64_t first_photon, int64_t n_photons, int6
 int smp_plan_stats(smp_plan *plan, smp_stats *stats_out) {
     if (!plan || !stats_out) return set_error(SMP_ERR_BAD_ARG, "NULL argument");
     SMP_CUDA(cudaSetDevice(plan->device));
-    int rc = collect_stats(plan, 0);
+    int rc = collect_stats(plan);
     *stats_out = plan->stats;
     return rc;
 }
@@ -637,7 +658,7 @@ int smp_plan_render(smp_plan *plan, int64_t n_photons, double *image_out, smp_st
         rc = smp_plan_trace(plan, 0, n_photons, n_photons, nullptr);
         if (rc) return rc;
     }
-    int rs = n_photons > 0 ? collect_stats(plan, 0) : SMP_OK;
+    int rs = n_photons > 0 ? collect_stats(plan) : SMP_OK;
     if (image_out) {
         rc = smp_plan_read_image(plan, image_out, 0, nullptr);
         if (rc) return rc;
@@ -687,7 +708,7 @@ int smp_trace_photons(const smp_scene_desc *scene, const smp_medium_desc *medium
         rc = set_error(SMP_ERR_CUDA, "trace buffers: %s", cudaGetErrorString(e));
     } else {
         rc = launch(p, first_photon, n_photons, weight_photons, 0, d_u, d_off, d_rec);
-        int rs = rc ? rc : collect_stats(p, 0);
+        int rs = rc ? rc : collect_stats(p);
         if (!rc) {
             e = cudaMemcpy(records_out, d_rec, size_t(n_photons) * sizeof(smp_photon_record), cudaMemcpyDeviceToHost);
             if (e != cudaSuccess) rc = set_error(SMP_ERR_CUDA, "records copy: %s", cudaGetErrorString(e));
@@ -770,6 +791,48 @@ int smp_field_eval(const smp_field_desc *field, double scaling, int64_t n_points
     cudaFree(d_n);
     cudaFree(d_g);
     if (e != cudaSuccess) return set_error(SMP_ERR_CUDA, "field probe: %s", cudaGetErrorString(e));
+    return SMP_OK;
+}
+
+// FP32 FMA throughput probe: every thread runs eight independent FMA chains.
+__global__ void fp32_peak_kernel(float *out, int iters) {
+    float a[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = float(threadIdx.x + j) * 1e-3f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = fmaf(a[j], 0.99990f, 1.0e-4f);
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s += a[j];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+int smp_fp32_peak(int device, double *tflops_out) {
+    if (!tflops_out) return set_error(SMP_ERR_BAD_ARG, "NULL argument");
+    int rc = check_device(device);
+    if (rc) return rc;
+    int sms = 0;
+    SMP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int blocks = sms * 8, threads = 256, iters = 1 << 16;
+    float *d = nullptr;
+    SMP_CUDA(cudaMalloc(&d, size_t(blocks) * threads * sizeof(float)));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    fp32_peak_kernel<<<blocks, threads>>>(d, 1024);
+    cudaEventRecord(a);
+    fp32_peak_kernel<<<blocks, threads>>>(d, iters);
+    cudaEventRecord(b);
+    cudaError_t e = cudaEventSynchronize(b);
+    float ms = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(d);
+    if (e != cudaSuccess) return set_error(SMP_ERR_CUDA, "fp32 probe: %s", cudaGetErrorString(e));
+    *tflops_out = 2.0 * 8.0 * double(iters) * blocks * threads / (double(ms) * 1e-3) / 1e12;
     return SMP_OK;
 }
 

@@ -29,33 +29,30 @@ __device__ __forceinline__ void bessel_field(const FieldParams &F, const float4 
         g = f3(0.0f, 0.0f, 0.0f);
         return;
     }
-    const float y = p.y, z = p.z;
+    float y = p.y, z = p.z;
     const float r2 = fmaf(y, y, z * z);
-    const float r = sqrtf(r2);
-    float jm, jm1;
-    bessel_pair_table<M>(tab, F.bnodes, F.binv_h, F.bh, F.k_r * r, jm, jm1);
+    float rs = rsqrt_fast(r2);                 // +inf at r2 = 0
+    float r = r2 > 0.0f ? r2 * rs : 0.0f;
+    // cos(m phi), sin(m phi) = (z/r + i y/r)^m; at r = 0, phi = atan2(0, 0) = 0
     float cm = 1.0f, sm = 0.0f;
-    if (M > 0) {
-        if (r2 > 0.0f) {
-            float ir = 1.0f / r;
-            float c = z * ir, sn = y * ir;
-            if (M == 1) { cm = c; sm = sn; }
-            else { cm = fmaf(c, c, -sn * sn); sm = 2.0f * c * sn; }
-        }
+    if (M > 0 && r2 > 0.0f) {
+        const float c = z * rs, sn = y * rs;
+        if (M == 1) { cm = c; sm = sn; }
+        else { cm = fmaf(c, c, -sn * sn); sm = 2.0f * c * sn; }
     }
     const float A = F.amp * s;
+    float jm, jm1;
+    bessel_pair_table<M>(tab, F.bnodes, F.binv_h, F.bh, F.k_r * r, jm, jm1);
     n = fmaf(A * jm, cm, F.n_o);
-    float gy = y, gz = z, gr = r;
-    if (r < kEps) {
-        gy = kEps; gz = kEps; gr = kEps;
+    if (!(r >= kEps)) {                        // the gradient's near-axis substitution (scene.cpp:229-234)
+        y = kEps; z = kEps; r = kEps; rs = 1.0f / kEps;
         bessel_pair_table<M>(tab, F.bnodes, F.binv_h, F.bh, F.k_r * kEps, jm, jm1);
     }
-    const float kr = F.k_r * gr;
-    const float djm = (M == 0) ? -jm1 : fmaf(float(M) / kr, jm, -jm1);
-    const float invr = 1.0f / gr;
-    const float a1 = A * djm * F.k_r * invr * cm;            // radial part / r
-    const float a2 = (M == 0) ? 0.0f : A * jm * float(M) * sm * invr * invr;
-    g = f3(0.0f, fmaf(a1, gy, -a2 * gz), fmaf(a1, gz, a2 * gy));
+    // J_m'(kr) = (m/kr) J_m - J_{m+1}, with 1/(kr) = rs/k
+    const float djm = (M == 0) ? -jm1 : fmaf(float(M) * F.inv_k * rs, jm, -jm1);
+    const float a1 = A * djm * F.k_r * rs * cm;            // radial part / r
+    const float a2 = (M == 0) ? 0.0f : A * jm * float(M) * sm * rs * rs;
+    g = f3(0.0f, fmaf(a1, y, -a2 * z), fmaf(a1, z, a2 * y));
 }
 
 // Plane waves (not in the reference): n = n_o + sum_i a_i sin(k_i.p - tau + phase_i)

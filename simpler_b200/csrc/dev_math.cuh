@@ -40,6 +40,29 @@ __device__ __forceinline__ float3 normalized(float3 a) {
 __device__ __forceinline__ bool finite3(float3 a) {
     return isfinite(a.x) && isfinite(a.y) && isfinite(a.z);
 }
+// single hardware approximations (PTX rcp.approx.ftz / rsqrt.approx.ftz: <= 1 ulp / 2^-22.9
+// relative error) for the inner march; the discrete logic keeps IEEE division
+__device__ __forceinline__ float rcp_fast(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float rsqrt_fast(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+// floor(t) and t - floor(t) for 0 <= t < 2^22 without integer conversions: adding 2^23 rounds t to
+// an integer held in the low mantissa bits
+__device__ __forceinline__ int floor_frac(float t, float &frac) {
+    const float big = 8388608.0f;
+    float tb = t + big;
+    int i = __float_as_int(tb) - 0x4B000000;
+    float fr = t - (tb - big);
+    if (fr < 0.0f) { fr += 1.0f; i -= 1; }
+    frac = fr;
+    return i;
+}
 __device__ __forceinline__ float comp(float3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
 __device__ __forceinline__ float3 ld3(const float *v) { return f3(v[0], v[1], v[2]); }
 
@@ -161,8 +184,8 @@ __device__ __forceinline__ void bessel_pair_table(const float4 *tab, int nodes, 
                                                   float &jm, float &jm1) {
     const float t = x * inv_h;
     if (t < float(nodes - 1)) {
-        const int i = int(t);
-        const float f = t - float(i);
+        float f;
+        const int i = floor_frac(t, f);
         const float4 a = tab[i], b = tab[i + 1];
         const float g = 1.0f - f;
         const float g2 = g * g, f2 = f * f;

@@ -25,6 +25,7 @@ struct FieldParams {
     float n_o;
     float egap, sgap;       // field is n_o outside sgap <= x <= egap
     float k_r;              // 2*pi*f/c
+    float inv_k;            // 1/k_r
     float amp;              // Bessel n_max
     float max_scaling;      // n_clip / n_max
     float phi_min, phi_range;
@@ -78,7 +79,7 @@ struct KParams {
     float h0;
     float large_dist;       // movePhotonTillSensor path budget (LargeDist)
     int precision;
-    long long step_cap;
+    int step_cap;
     // film
     void *film;
     int X, Y, Z;

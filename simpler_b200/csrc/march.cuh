@@ -20,6 +20,12 @@ namespace smp {
 
 static constexpr unsigned kFull = 0xffffffffu;
 
+// Resident 128-thread blocks per SM the march kernel is compiled for (register budget 65536 /
+// (128 * blocks)).
+#ifndef SMP_MIN_BLOCKS
+#define SMP_MIN_BLOCKS 4
+#endif
+
 enum LaneState : int { ST_FETCH = 0, ST_EVENT = 1, ST_MARCH = 2, ST_DONE = 3 };
 enum Event : int {
     EV_NEW = 0,          // photon fetched: genRay, scaling, direct or scatter
@@ -46,9 +52,10 @@ struct Lane {
     // current march (traceTillBlock) and its caller (movePhoton / movePhotonTillSensor)
     float3 mp, md, mg;        // position, optical direction v, grad n at mp
     float mn;                 // n at mp
-    double mtot;              // optical length accumulated by this march
+    double mtot;              // optical length accumulated by this march (FP64 form)
+    float mtotf;              // the same in the FP32 form
     float dist_acc, dlimit, cur;
-    long long rem_steps;
+    int rem_steps;
     int prec, ctx, first;
     float large, d2s, rem, sampled;
     const float4 *tab;        // Bessel table in this block's shared memory
@@ -90,11 +97,14 @@ __device__ __forceinline__ float draw(Lane &L, const KParams &P) {
 }
 
 // ---- small pieces of the scene -------------------------------------------------------------
-__device__ __forceinline__ long long steps_for(float dlimit, float h0) {
-    // (long)(dist/h + 1) as the reference's x86-64 build converts it (scene.cpp:391)
+__device__ __forceinline__ int steps_for(float dlimit, float h0) {
+    // (long)(dist/h + 1) as the reference's x86-64 build converts it (scene.cpp:391): out-of-range
+    // values become INT64_MIN (no steps). Counts above 2^31 - 1 are clamped: the per-photon step
+    // cap (<= 2e9) ends the photon first.
     float v = dlimit / h0 + 1.0f;
-    if (!(v >= -9.2233720e18f && v < 9.2233720e18f)) return (long long)0x8000000000000000ULL;
-    return (long long)v;
+    if (!(v >= -9.2233720e18f && v < 9.2233720e18f)) return 0;
+    if (v >= 2147483647.0f) return 2147483647;
+    return int(v);
 }
 
 __device__ __forceinline__ bool inside_box(const KParams &P, float3 p) {
@@ -304,6 +314,7 @@ __device__ __forceinline__ void begin_march(Lane &L, const KParams &P, float dli
     L.cur = P.h0;
     L.prec = P.precision;
     L.rem_steps = steps_for(dlimit, P.h0);
+    L.mtotf = float(L.mtot);
 }
 
 // One iteration of the traceTillBlock loop (scene.cpp:395-419). Returns true when the march
@@ -312,14 +323,15 @@ template <int FK>
 __device__ __forceinline__ bool march_step(Lane &L, const KParams &P) {
     const float hh = 0.5f * L.cur;
     float3 d = f3(fmaf(hh, L.mg.x, L.md.x), fmaf(hh, L.mg.y, L.md.y), fmaf(hh, L.mg.z, L.md.z));
-    const float inv = 1.0f / L.mn;
-    float3 p = f3(fmaf(L.cur * d.x, inv, L.mp.x), fmaf(L.cur * d.y, inv, L.mp.y), fmaf(L.cur * d.z, inv, L.mp.z));
+    const float hinv = L.cur * rcp_fast(L.mn);
+    float3 p = f3(fmaf(d.x, hinv, L.mp.x), fmaf(d.y, hinv, L.mp.y), fmaf(d.z, hinv, L.mp.z));
     float n2;
     float3 g2;
     Field<FK>::eval(P.field, L.tab, p, L.s, n2, g2);
     d = f3(fmaf(hh, g2.x, d.x), fmaf(hh, g2.y, d.y), fmaf(hh, g2.z, d.z));
     ++L.steps;
-    if (!finite3(p) || !finite3(d)) { L.end = SMP_END_NAN; return true; }
+    // A non-finite position fails the box test below, so refinement ends the march within
+    // `precision` steps; run_events checks finiteness when the march ends.
     if (L.steps >= P.step_cap) { L.end = SMP_END_STEP_CAP; return true; }
     if (!inside_box(P, p) || (L.dist_acc + L.cur) > L.dlimit) {
         if (--L.prec < 0) {                      // refinement exhausted: keep the failed step
@@ -332,7 +344,7 @@ __device__ __forceinline__ bool march_step(Lane &L, const KParams &P) {
         L.mp = p; L.md = d; L.mn = n2; L.mg = g2;
         L.dist_acc += L.cur;
         if (P.fp64) L.mtot = fma(double(L.cur), double(n2), L.mtot);
-        else L.mtot = double(fmaf(L.cur, n2, float(L.mtot)));
+        else L.mtotf = fmaf(L.cur, n2, L.mtotf);
     }
     return --L.rem_steps <= 0;
 }
@@ -343,6 +355,11 @@ __device__ __forceinline__ bool march_step(Lane &L, const KParams &P) {
 template <int FK>
 __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
     for (;;) {
+        if (ev == EV_MARCH_END) {
+            if (!P.fp64) L.mtot = double(L.mtotf);
+            if (L.end == 0 && !isfinite((L.mp.x + L.mp.y) + (L.mp.z + L.md.x) + (L.md.y + L.md.z) + L.mn))
+                L.end = SMP_END_NAN;
+        }
         if (ev != EV_FINISH && L.end != 0) {                    // aborted (cap, NaN, stream)
             if (ev == EV_MARCH_END) {
                 if (L.ctx == CTX_MOVE_FIRST || L.ctx == CTX_MOVE_VERTEX) { L.pos = L.mp; L.dir = L.md; L.total = L.mtot; }
@@ -613,7 +630,7 @@ __device__ __noinline__ bool stage_to_shared(void *dst, const void *src, unsigne
 }
 
 template <int FK>
-__global__ void __launch_bounds__(128) march_kernel(const __grid_constant__ KParams P) {
+__global__ void __launch_bounds__(128, SMP_MIN_BLOCKS) march_kernel(const __grid_constant__ KParams P) {
     extern __shared__ __align__(16) float4 smem_tab[];
     const int lane = threadIdx.x & 31;
     Lane L;
@@ -661,7 +678,8 @@ __global__ void __launch_bounds__(128) march_kernel(const __grid_constant__ KPar
         // ---- march phase: step until event_batch lanes (scaled by the live lanes) have ended
         const int thr = max(1, (P.event_batch * __popc(alive) + 16) >> 5);
         for (;;) {
-            if (st == ST_MARCH && march_step<FK>(L, P)) {
+            // two steps per vote; a lane whose march ends on the first skips the second
+            if (st == ST_MARCH && (march_step<FK>(L, P) || march_step<FK>(L, P))) {
                 st = ST_EVENT;
                 pending_ev = EV_MARCH_END;
             }
