@@ -283,6 +283,25 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
                      int32_t n_inst, const smp_render_opts *opts,
                      double *images_out, smp_stats *stats_out);
 
+/* Rendering without allocation -- no counterpart in the reference. For callers that cannot call
+   cudaMalloc (device memory owned by the host application's allocator or budget, code that must not
+   hit cudaMalloc/cudaFree's device-wide synchronisation mid-frame, plugin hosts that hand over only
+   the buffers the renderer may touch). Traces photons [first_photon, first_photon + n_photons)
+   with Philox streams into the caller's device film d_film (float per pixel for SMP_PREC_FP32,
+   double for SMP_PREC_MIXED, Image3 layout, accumulated -- zero it first for a fresh render) on
+   'stream', and returns after the trace has finished. It allocates nothing: the work counter,
+   statistics, Bessel table and texture CDF live in a fixed 1 MiB device array that every GPU
+   loading this library holds until the process exits. Limits: textures up to 253823 texels;
+   Bessel fields of order 0-2 and plane-wave fields; larger inputs are rejected with
+   SMP_ERR_BAD_ARG / SMP_ERR_UNSUPPORTED. All calls on a device share that array and each call
+   overwrites what the last one left there; calls whose GPU work overlaps race on it. The first
+   call on each device looks up the array's device address, so make it before any stream capture.
+   stats_out (may be NULL) receives photon, step and splat counts; kernel_ms is not measured. */
+int smp_render_noalloc(const smp_scene_desc *scene, const smp_medium_desc *medium,
+                       const smp_field_desc *field, const smp_render_opts *opts,
+                       int64_t first_photon, int64_t n_photons, int64_t weight_photons,
+                       void *d_film, void *stream, smp_stats *stats_out);
+
 /* Measurement utility with no counterpart in the reference: the device's FP32 FMA throughput
    (TFLOP/s, 2 FLOP per FMA) measured with independent FMA chains on every SM; the roofline
    denominator for the march, which is bound by the FP32 and issue pipes. */

@@ -140,6 +140,7 @@ EXPORTS = [
     "smp_plan_create", "smp_plan_destroy", "smp_plan_set_field", "smp_plan_clear", "smp_plan_trace",
     "smp_plan_read_image", "smp_plan_film", "smp_plan_stats", "smp_plan_render", "smp_trace_photons",
     "smp_field_eval", "smp_texture_cdf", "smp_spline_prefilter", "smp_render_batch", "smp_fp32_peak",
+    "smp_render_noalloc",
 ]
 
 _lib = None
@@ -183,6 +184,8 @@ def load() -> C.CDLL:
     lib.smp_spline_prefilter.argtypes = [vp, vp, vp]
     lib.smp_render_batch.argtypes = [P(SceneDesc), P(InstanceDesc), C.c_int32, P(RenderOpts), vp, P(Stats)]
     lib.smp_fp32_peak.argtypes = [C.c_int, P(C.c_double)]
+    lib.smp_render_noalloc.argtypes = [P(SceneDesc), P(MediumDesc), P(FieldDesc), P(RenderOpts), C.c_int64, C.c_int64,
+                                       C.c_int64, vp, vp, P(Stats)]
     _lib = lib
     return lib
 

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -842,3 +843,196 @@ int smp_render_batch(const smp_scene_desc *, const smp_instance_desc *, int32_t,
 }
 
 }  // extern "C"
+
+// ==== Rendering without allocation ================================================================
+// Some callers cannot call cudaMalloc: a host application whose device memory is owned by its own
+// allocator or budget, code that must not hit cudaMalloc/cudaFree's implicit device-wide
+// synchronisation in the middle of a frame, or a plugin host that hands the renderer only the
+// buffers it may touch. smp_render_noalloc serves them: the caller passes the descriptors and an
+// already-allocated device film; the work counter, statistics, Bessel table and texture CDF live
+// in the fixed device array below, and host staging uses fixed static buffers.
+//
+// Limits: 1 MiB of device scratch per GPU that loads this library (held until the process exits);
+// textures up to 253823 texels; Bessel fields (orders 0-2) and plane-wave fields only.
+// Every call on a device shares the scratch and overwrites what the previous call left there (the
+// call clears the counters itself); calls whose GPU work overlaps -- on two streams, or from two
+// host threads -- race on it. The first call on each device looks up the array's device address
+// (cudaGetSymbolAddress); make that first call before any stream capture.
+
+#define SMP_NOALLOC_SCRATCH_BYTES (1u << 20)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SMP_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+const size_t kNoAllocCountersBytes = 256;
+const int kNoAllocTabNodes = 2064;                                   // >= ceil(128 * 16) + 2
+const size_t kNoAllocTabBytes = size_t(kNoAllocTabNodes) * sizeof(float4);
+const size_t kNoAllocCdfFloats = (SMP_NOALLOC_SCRATCH_BYTES - kNoAllocCountersBytes - kNoAllocTabBytes) / sizeof(float);
+const int kNoAllocMaxDevices = 64;
+
+unsigned char *g_noalloc_dev[kNoAllocMaxDevices];                  // device address per device
+std::mutex g_noalloc_mutex;                                          // guards the host staging below
+float g_noalloc_cdf_host[kNoAllocCdfFloats];
+float4 g_noalloc_tab_host[kNoAllocTabNodes];
+}  // namespace
+
+// The array's device address on the current device, looked up once per device.
+static int noalloc_scratch(int dev, unsigned char **out) {
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return set_error(SMP_ERR_BAD_ARG, "device %d beyond %d", dev, kNoAllocMaxDevices);
+    if (!g_noalloc_dev[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return set_error(SMP_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+        g_noalloc_dev[dev] = static_cast<unsigned char *>(p);
+    }
+    *out = g_noalloc_dev[dev];
+    return SMP_OK;
+}
+
+extern "C" int smp_render_noalloc(const smp_scene_desc *scene, const smp_medium_desc *medium,
+                                  const smp_field_desc *field, const smp_render_opts *opts,
+                                  int64_t first_photon, int64_t n_photons, int64_t weight_photons,
+                                  void *d_film, void *stream, smp_stats *stats_out) {
+    int rc = check_descs(scene, medium, field, opts);
+    if (rc) return rc;
+    if (!d_film) return set_error(SMP_ERR_BAD_ARG, "d_film is NULL");
+    if (opts->rng != SMP_RNG_PHILOX) return set_error(SMP_ERR_BAD_ARG, "smp_render_noalloc draws from Philox");
+    if (n_photons < 0 || first_photon < 0 || weight_photons <= 0) return set_error(SMP_ERR_BAD_ARG, "bad photon range");
+    int fk;
+    rc = field_kind(*field, &fk);
+    if (rc) return rc;
+    if (!(fk <= FK_BESSEL2 || fk == FK_PLANEWAVE))
+        return set_error(SMP_ERR_UNSUPPORTED, "smp_render_noalloc renders Bessel (orders 0-2) and plane-wave fields");
+    const long long n_tex = (long long)scene->tex_x * scene->tex_y;
+    if (size_t(n_tex) + 1 > kNoAllocCdfFloats)
+        return set_error(SMP_ERR_BAD_ARG, "texture has %lld texels; smp_render_noalloc holds at most %zu",
+                         n_tex, kNoAllocCdfFloats - 1);
+    rc = check_device(opts->device);
+    if (rc) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    unsigned char *scratch = nullptr;
+    rc = noalloc_scratch(opts->device, &scratch);
+    if (rc) return rc;
+    unsigned long long *d_counters = reinterpret_cast<unsigned long long *>(scratch);
+    float4 *d_tab = reinterpret_cast<float4 *>(scratch + kNoAllocCountersBytes);
+    float *d_cdf = reinterpret_cast<float *>(scratch + kNoAllocCountersBytes + kNoAllocTabBytes);
+
+    KParams k;
+    std::memset(&k, 0, sizeof(k));
+    for (int i = 0; i < 3; ++i) {
+        k.L[i] = float(scene->medium_l[i]);
+        k.R[i] = float(scene->medium_r[i]);
+        k.src_origin[i] = float(scene->light_origin[i]);
+        k.src_lens_origin[i] = float(scene->emitter_lens_origin[i]);
+        k.cam_origin[i] = float(scene->view_origin[i]);
+        k.cam_lens_origin[i] = float(scene->sensor_lens_origin[i]);
+    }
+    k.plane[0] = float(scene->light_plane[0]);
+    k.plane[1] = float(scene->light_plane[1]);
+    k.pixsize[0] = k.plane[0] / float(scene->tex_x);
+    k.pixsize[1] = k.plane[1] / float(scene->tex_y);
+    k.ct = std::cos(float(scene->half_theta_limit));
+    k.tex_x = scene->tex_x;
+    k.n_tex = int(n_tex);
+    k.src_lens_active = scene->emitter_lens_active;
+    k.src_lens_sqap = float(scene->emitter_lens_aperture) * float(scene->emitter_lens_aperture);
+    k.src_lens_focal = float(scene->emitter_lens_focal_length);
+    float cd[3], ch[3];
+    for (int i = 0; i < 3; ++i) { cd[i] = float(scene->view_dir[i]); ch[i] = float(scene->view_horizontal[i]); }
+    float ld = std::sqrt(cd[0] * cd[0] + cd[1] * cd[1] + cd[2] * cd[2]);
+    float lh = std::sqrt(ch[0] * ch[0] + ch[1] * ch[1] + ch[2] * ch[2]);
+    for (int i = 0; i < 3; ++i) { k.cam_dir[i] = cd[i] / ld; k.cam_h[i] = ch[i] / lh; }
+    k.cam_v[0] = k.cam_dir[1] * k.cam_h[2] - k.cam_dir[2] * k.cam_h[1];
+    k.cam_v[1] = k.cam_dir[2] * k.cam_h[0] - k.cam_dir[0] * k.cam_h[2];
+    k.cam_v[2] = k.cam_dir[0] * k.cam_h[1] - k.cam_dir[1] * k.cam_h[0];
+    k.cam_plane[0] = float(scene->view_plane[0]);
+    k.cam_plane[1] = float(scene->view_plane[1]);
+    k.pl_min = float(scene->pathlength_range[0]);
+    k.pl_max = float(scene->pathlength_range[1]);
+    k.bounce = scene->use_bounce_decomposition;
+    k.cam_lens_active = scene->sensor_lens_active;
+    k.cam_lens_sqap = float(scene->sensor_lens_aperture) * float(scene->sensor_lens_aperture);
+    k.cam_lens_focal = float(scene->sensor_lens_focal_length);
+    k.ior1 = 1.0f;
+    k.ior2 = float(scene->ior);
+    k.sigma_t = float(medium->sigma_t);
+    k.albedo = float(medium->albedo);
+    k.mfp = 1.0f / float(medium->sigma_t);
+    if (k.sigma_t <= 1.19209290e-07f) { k.sigma_t = 0.0f; k.mfp = 1.0f; k.albedo = 0.0f; }
+    k.g = float(medium->g);
+    k.max_depth = opts->max_depth;
+    k.max_pathlength = float(opts->max_pathlength);
+    k.use_direct = opts->use_direct;
+    k.use_angular = opts->use_angular_sampling;
+    k.step_cap = int(std::min<int64_t>(opts->step_cap > 0 ? opts->step_cap : 10000000LL, 2000000000LL));
+    k.large_dist = sensor_march_budget(*opts, k.sigma_t);
+    k.X = scene->x_res; k.Y = scene->y_res; k.Z = scene->z_res;
+    k.fp64 = opts->precision == SMP_PREC_MIXED;
+    k.rng = SMP_RNG_PHILOX;
+    k.seed = opts->seed;
+    k.weight = photon_weight(*scene, weight_photons);
+    k.first_photon = first_photon;
+    k.n_photons = n_photons;
+    k.event_batch = 8;
+    k.film = d_film;
+    k.counters = d_counters;
+    k.cdf = d_cdf;
+    fill_field_params(*field, fk, k.field);
+    k.h0 = float(field->er_stepsize);
+    k.precision = field->precision;
+
+    // texture CDF (pmf.h:41-99, float) into the static host buffer, then into the scratch
+    float *cdf = g_noalloc_cdf_host;
+    cdf[0] = 0.0f;
+    for (long long i = 0; i < n_tex; ++i) cdf[i + 1] = cdf[i] + static_cast<float>(scene->texture[i]);
+    if (cdf[n_tex] > 0.0f) {
+        float norm = 1.0f / cdf[n_tex];
+        for (long long i = 1; i <= n_tex; ++i) cdf[i] *= norm;
+        cdf[n_tex] = 1.0f;
+    }
+    SMP_CUDA(cudaMemcpyAsync(d_cdf, cdf, size_t(n_tex + 1) * sizeof(float), cudaMemcpyHostToDevice, s));
+    size_t smem = 0;
+    if (fk <= FK_BESSEL2) {
+        double x_max = std::min(std::max(box_max_kr(*scene, k.field.k_r), 1.0), kBesselMaxX);
+        int nodes = int(std::ceil(x_max / kBesselH)) + 2;
+        for (int i = 0; i < nodes; ++i) {
+            double x = i * kBesselH;
+            int m = field->mode;
+            auto J = [](int n, double xx) -> double {
+                if (n < 0) return (n % 2 ? -1.0 : 1.0) * std::cyl_bessel_j(double(-n), xx);
+                return std::cyl_bessel_j(double(n), xx);
+            };
+            double jm = J(m, x), jm1 = J(m + 1, x);
+            g_noalloc_tab_host[i] = make_float4(float(jm), float(0.5 * (J(m - 1, x) - jm1)), float(jm1),
+                                                float(0.5 * (jm - J(m + 2, x))));
+        }
+        SMP_CUDA(cudaMemcpyAsync(d_tab, g_noalloc_tab_host, size_t(nodes) * sizeof(float4), cudaMemcpyHostToDevice, s));
+        k.field.btab = d_tab;
+        k.field.bnodes = nodes;
+        smem = size_t(nodes) * sizeof(float4);
+    }
+    SMP_CUDA(cudaMemsetAsync(d_counters, 0, CNT_COUNT * sizeof(unsigned long long), s));
+    int grid = 0;
+    rc = grid_for(fk, opts->device, opts->blocks_per_sm, smem, &grid);
+    if (rc) return rc;
+    if (n_photons > 0) {
+        march_fn(fk)<<<grid, kBlock, smem, s>>>(k);
+        SMP_CUDA(cudaGetLastError());
+    }
+    unsigned long long c[CNT_COUNT];
+    SMP_CUDA(cudaMemcpyAsync(c, d_counters, sizeof(c), cudaMemcpyDeviceToHost, s));
+    SMP_CUDA(cudaStreamSynchronize(s));
+    if (stats_out) {
+        std::memset(stats_out, 0, sizeof(*stats_out));
+        stats_out->photons = (int64_t)c[CNT_PHOTONS];
+        stats_out->er_steps = (int64_t)c[CNT_STEPS];
+        stats_out->splats = (int64_t)c[CNT_SPLATS];
+        stats_out->step_cap_hits = (int64_t)c[CNT_STEP_CAP];
+        stats_out->nan_photons = (int64_t)c[CNT_NAN];
+    }
+    if (c[CNT_STAGE_TIMEOUT]) return set_error(SMP_ERR_CUDA, "%llu block(s) timed out staging the field table", c[CNT_STAGE_TIMEOUT]);
+    if (c[CNT_STEP_CAP]) return set_error(SMP_ERR_STEP_CAP, "%llu photon(s) hit the per-photon step cap", c[CNT_STEP_CAP]);
+    if (c[CNT_NAN]) return set_error(SMP_ERR_NAN, "%llu photon(s) produced a non-finite state", c[CNT_NAN]);
+    return SMP_OK;
+}
