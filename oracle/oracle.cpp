@@ -720,13 +720,17 @@ template <typename R, typename A> struct Tracer {
     // scene.cpp:26-39 + warp.cpp:22-34. The reference evaluates Vec2f(sampler(), sampler())
     // right to left under GCC x86-64: the first draw lands in sample.y (azimuth), the second in
     // sample.x (z).
+    // warp::squareToUniformHemisphere (warp.cpp:22-34): z = sample.x, azimuth 2 pi sample.y
+    static V3<R> uniform_hemisphere(R sx, R sy) {
+        R z = sx;
+        R tmp = std::sqrt(R(1) - z * z);
+        R a = R(2.0 * double(K<R>::pi())) * sy;
+        return V3<R>(std::cos(a) * tmp, std::sin(a) * tmp, z);
+    }
     V3<R> sample_random_direction() {
         R uy = (*u)();
         R ux = (*u)();
-        R z = ux;
-        R tmp = std::sqrt(R(1) - z * z);
-        R a = R(2.0 * double(K<R>::pi())) * uy;
-        V3<R> v(std::cos(a) * tmp, std::sin(a) * tmp, z);
+        V3<R> v = uniform_hemisphere(ux, uy);
         R t = v.x;
         v.x = -v.z;
         v.z = v.y;
@@ -1018,6 +1022,90 @@ int orc_render(const smp_scene_desc *scene, const smp_medium_desc *medium, const
                                                uniforms, offsets, records, image_out);
     return orc::render_impl<float, float>(scene, medium, field, opts, threads, first, n, weight_photons,
                                           uniforms, offsets, records, image_out);
+}
+
+// ---- single primitives (float, the reference's build), for pinning against its compiled code -------
+int orc_hg_sample(float g, const float *in, uint64_t seed, int skip, float *out) {
+    orc::Uniforms un;
+    un.mode = SMP_RNG_SFMT;
+    un.sfmt.seed(seed);
+    for (int i = 0; i < skip; ++i) (void)un();
+    orc::Tracer<float, float> tr;
+    tr.g = g;
+    tr.u = &un;
+    orc::V3<float> o;
+    tr.hg_sample(orc::V3<float>(in[0], in[1], in[2]), o);
+    out[0] = o.x; out[1] = o.y; out[2] = o.z;
+    return 0;
+}
+
+float orc_hg_f(float g, const float *in, const float *out) {
+    orc::Tracer<float, float> tr;
+    tr.g = g;
+    return tr.hg_f(orc::V3<float>(in[0], in[1], in[2]), orc::V3<float>(out[0], out[1], out[2]));
+}
+
+void orc_hemisphere(float sx, float sy, float *out) {
+    orc::V3<float> v = orc::Tracer<float, float>::uniform_hemisphere(sx, sy);
+    out[0] = v.x; out[1] = v.y; out[2] = v.z;
+}
+
+float orc_fresnel(float ci, float ct, float eta) { return orc::fresnel<float>(ci, ct, eta); }
+
+int orc_refract(const float *a, const float *n, float eta, float *b) {
+    orc::V3<float> o;
+    bool ok = orc::refract<float>(orc::V3<float>(a[0], a[1], a[2]), orc::V3<float>(n[0], n[1], n[2]), eta, o);
+    b[0] = o.x; b[1] = o.y; b[2] = o.z;
+    return ok ? 1 : 0;
+}
+
+void orc_coordinate_system(const float *a, float *b, float *c) {
+    orc::V3<float> vb, vc;
+    orc::coordinate_system<float>(orc::V3<float>(a[0], a[1], a[2]), vb, vc);
+    b[0] = vb.x; b[1] = vb.y; b[2] = vb.z;
+    c[0] = vc.x; c[1] = vc.y; c[2] = vc.z;
+}
+
+void orc_bsdf_sample(float ior1, float ior2, const float *in, const float *n, uint64_t seed, int skip, float *out) {
+    orc::Uniforms un;
+    un.mode = SMP_RNG_SFMT;
+    un.sfmt.seed(seed);
+    for (int i = 0; i < skip; ++i) (void)un();
+    orc::Scene<float> sc;
+    sc.ior1 = ior1;
+    sc.ior2 = ior2;
+    orc::Tracer<float, float> tr;
+    tr.sc = &sc;
+    tr.u = &un;
+    orc::V3<float> o;
+    tr.bsdf_sample(orc::V3<float>(in[0], in[1], in[2]), orc::V3<float>(n[0], n[1], n[2]), o);
+    out[0] = o.x; out[1] = o.y; out[2] = o.z;
+}
+
+int orc_lens_propagate(const float *origin, float aperture, float focal, int active, float *pos, float *dir, float *total) {
+    orc::Lens<float> lens;
+    double o[3] = {origin[0], origin[1], origin[2]};
+    lens.init(o, aperture, focal, active);
+    orc::V3<float> p(pos[0], pos[1], pos[2]), d(dir[0], dir[1], dir[2]);
+    float t = *total;
+    bool ok = lens.propagate_till_lens(p, d, t);
+    pos[0] = p.x; pos[1] = p.y; pos[2] = p.z;
+    dir[0] = d.x; dir[1] = d.y; dir[2] = d.z;
+    *total = t;
+    return ok ? 1 : 0;
+}
+
+// cubic B-spline kernels k0, k1, k2 (spline.h:33-62), double
+int orc_bspline_kernel(int d, int n, const double *x, double *out) {
+    for (int i = 0; i < n; ++i) {
+        if (d == 0) out[i] = orc::Field<double>::k0(x[i]);
+        else if (d == 1) out[i] = orc::Field<double>::k1(x[i]);
+        else {
+            double a = std::abs(x[i]);
+            out[i] = a > 2 ? 0.0 : (a > 1 ? 2 - a : 3 * a - 2);
+        }
+    }
+    return 0;
 }
 
 int orc_sfmt_floats(uint64_t seed, int n, float *out) {
