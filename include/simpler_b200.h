@@ -95,6 +95,10 @@ typedef struct smp_field_desc {
     int32_t _pad2;
     double  grid_min[3], grid_max[3];
     const float *grid_coeff;
+    /* FUS source arcs given explicitly, as the Scene constructor takes them (scene.h:78-95):
+       used when theta_max > theta_min, else derived from chordlength as
+       renderer3d_sample.cpp:136-140 does (theta = -+asin(chord/2r), trans_z = -+chord/2) */
+    double  theta_min, theta_max, trans_z_min, trans_z_max;
 } smp_field_desc;
 
 /* ---- scene: medium box, textured collimated source, sensor --------------------------------- */

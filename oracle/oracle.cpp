@@ -170,6 +170,10 @@ template <typename R> struct Field {
         R theta_min = -std::asin(chord / (R(2) * radius));
         R theta_max = std::asin(chord / (R(2) * radius));
         R zmin = -chord / R(2), zmax = chord / R(2);
+        if (f.theta_max > f.theta_min) {      // explicit arcs (scene.h:78-95 constructor form)
+            theta_min = R(f.theta_min); theta_max = R(f.theta_max);
+            zmin = R(f.trans_z_min); zmax = R(f.trans_z_max);
+        }
         int nt = f.theta_sources, nz = f.trans_z_sources;
         nsources = nt * nz;
         R theta_diff = (theta_max - theta_min) / R(nt - 1);

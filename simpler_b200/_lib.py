@@ -57,6 +57,8 @@ class FieldDesc(C.Structure):
         ("grid_n", C.c_int32 * 3), ("_pad2", C.c_int32),
         ("grid_min", D3), ("grid_max", D3),
         ("grid_coeff", C.POINTER(C.c_float)),
+        ("theta_min", C.c_double), ("theta_max", C.c_double),
+        ("trans_z_min", C.c_double), ("trans_z_max", C.c_double),
     ]
 
 

@@ -1,7 +1,9 @@
 """Build the native parts of simpler_b200 in-tree.
 
 * ``libsimpler_b200.so`` -- the CUDA kernels and the C ABI (``include/simpler_b200.h``),
-  compiled for sm_100a only.
+  compiled for sm_100a only, plus the C++ host layer (``csrc/host/smp_host.cpp``: file formats,
+  the reference's key=value and JSON front-ends);
+* ``bin/renderer3d`` and ``bin/simplER`` -- the reference's two command-line front-ends over it;
 * the CPU oracle (``oracle/liboracle*.so``) and, when the reference checkout is present, the
   reference's own primitives (``oracle/_ref``) -- test infrastructure, built here so the GPU box
   receives them prebuilt.
@@ -27,8 +29,10 @@ NVCC_FLAGS = [
     "--expt-relaxed-constexpr",
 ]
 
-CU_SOURCES = ["capi.cu"]
-HEADERS = ["kparams.h", "dev_math.cuh", "dev_field.cuh", "march.cuh"]
+CU_SOURCES = ["capi.cu", "host/smp_host.cpp"]
+HEADERS = ["kparams.h", "dev_math.cuh", "dev_field.cuh", "march.cuh", "host/smp_host.h"]
+BIN = os.path.join(HERE, "bin")
+MAINS = {"renderer3d": "host/renderer3d_main.cpp", "simplER": "host/simpler_main.cpp"}
 
 
 def _nvcc() -> str:
@@ -63,6 +67,23 @@ def build_library(verbose: bool = False, force: bool = False) -> str:
     return LIB
 
 
+def build_frontends(force: bool = False) -> None:
+    """The command-line front-ends, linked against the library with an rpath to it."""
+    os.makedirs(BIN, exist_ok=True)
+    cxx = shutil.which("g++") or "g++"
+    for name, src in MAINS.items():
+        out = os.path.join(BIN, name)
+        deps = [os.path.join(CSRC, src), os.path.join(CSRC, "host", "smp_host.h"), LIB]
+        if not force and not _stale(out, deps):
+            continue
+        cmd = [cxx, "-std=c++17", "-O2", os.path.join(CSRC, src), "-I", os.path.join(CSRC, "host"),
+               "-L", HERE, "-lsimpler_b200", "-Wl,-rpath,$ORIGIN/..", "-o", out + ".tmp"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"front-end build failed:\n{res.stdout}\n{res.stderr}")
+        os.replace(out + ".tmp", out)
+
+
 def build_oracle() -> None:
     """Test infrastructure: the CPU checker and the reference primitives used to pin it."""
     odir = os.path.join(ROOT, "oracle")
@@ -80,6 +101,7 @@ def build_oracle() -> None:
 
 def build_all(verbose: bool = False, force: bool = False) -> None:
     build_library(verbose=verbose, force=force)
+    build_frontends(force=force)
     build_oracle()
 
 

@@ -98,8 +98,12 @@ static void prefilter_3d(const float *samples, const int N[3], float *coeff) {
 // point sources on the two arcs, arc 1 block then arc 2 block.
 static void source_centres(const smp_field_desc &f, std::vector<float4> &out) {
     const float radius = float(f.radius), chord = float(f.chordlength);
-    const float tmin = -std::asin(chord / (2.0f * radius)), tmax = std::asin(chord / (2.0f * radius));
-    const float zmin = -chord / 2.0f, zmax = chord / 2.0f;
+    float tmin = -std::asin(chord / (2.0f * radius)), tmax = std::asin(chord / (2.0f * radius));
+    float zmin = -chord / 2.0f, zmax = chord / 2.0f;
+    if (f.theta_max > f.theta_min) {
+        tmin = float(f.theta_min); tmax = float(f.theta_max);
+        zmin = float(f.trans_z_min); zmax = float(f.trans_z_max);
+    }
     const int nt = f.theta_sources, nz = f.trans_z_sources, ns = nt * nz;
     const float tdiff = (tmax - tmin) / float(nt - 1), zdiff = (zmax - zmin) / float(nz - 1);
     out.assign(size_t(2) * ns, make_float4(0, 0, 0, 0));

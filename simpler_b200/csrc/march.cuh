@@ -77,6 +77,13 @@ __device__ __forceinline__ void philox_block(unsigned &c0, unsigned &c1, unsigne
     }
 }
 
+// one Philox block, kept out of line: draw() is called from many places in the event code
+__device__ __noinline__ uint4 philox_refill(unsigned blk, unsigned ph_lo, unsigned ph_hi, unsigned k0, unsigned k1) {
+    unsigned c0 = blk, c1 = 0u, c2 = ph_lo, c3 = ph_hi;
+    philox_block(c0, c1, c2, c3, k0, k1);
+    return make_uint4(c0, c1, c2, c3);
+}
+
 __device__ __forceinline__ float draw(Lane &L, const KParams &P) {
     ++L.draws;
     if (P.rng == SMP_RNG_STREAM) {
@@ -85,9 +92,8 @@ __device__ __forceinline__ float draw(Lane &L, const KParams &P) {
         return 0.5f;
     }
     if (L.rhave == 0) {
-        unsigned c0 = L.rblk++, c1 = 0u, c2 = unsigned(L.idx), c3 = unsigned(L.idx >> 32);
-        philox_block(c0, c1, c2, c3, unsigned(P.seed), unsigned(P.seed >> 32));
-        L.r0 = c0; L.r1 = c1; L.r2 = c2; L.r3 = c3;
+        uint4 b = philox_refill(L.rblk++, unsigned(L.idx), unsigned(L.idx >> 32), unsigned(P.seed), unsigned(P.seed >> 32));
+        L.r0 = b.x; L.r1 = b.y; L.r2 = b.z; L.r3 = b.w;
         L.rhave = 4;
     }
     unsigned x = L.r0;
@@ -241,7 +247,7 @@ __device__ __forceinline__ float3 hg_sample(Lane &L, const KParams &P, float3 in
     float sinT = sqrtf(fmaxf(0.0f, 1.0f - cosT * cosT));
     float phi = 6.28318548202514648f * sy;
     float sP, cP;
-    sincosf(phi, &sP, &cP);
+    sincos_red(phi, sP, cP);
     float3 ax, ay;
     if (fabsf(in.x) > fabsf(in.y)) {
         float inv = 1.0f / sqrtf(in.x * in.x + in.z * in.z);
@@ -261,7 +267,7 @@ __device__ __forceinline__ float3 random_direction(Lane &L, const KParams &P) {
     float ux = draw(L, P);
     float tmp = sqrtf(1.0f - ux * ux);
     float sP, cP;
-    sincosf(6.28318548202514648f * uy, &sP, &cP);
+    sincos_red(6.28318548202514648f * uy, sP, cP);
     return f3(-ux, cP * tmp, sP * tmp);
 }
 
@@ -291,7 +297,7 @@ __device__ __forceinline__ bool gen_ray(Lane &L, const KParams &P, float3 &pos, 
     float zt = sqrtf(1.0f - z * z);
     float phi = draw(L, P) * 2.0f * 3.14159265358979f;
     float sP, cP;
-    sincosf(phi, &sP, &cP);
+    sincos_red(phi, sP, cP);
     dir = f3(-z, zt * cP, zt * sP);
     // Lens::propagate_till_lens (lens.cpp:20-33)
     float dist = -(pos.x - P.src_lens_origin[0]) / dir.x;
@@ -382,7 +388,11 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
             const FieldParams &F = P.field;
             if (FK == FK_PLANEWAVE) L.s = fmaf(F.phi_range, u, F.phi_min);
             else if (FK == FK_SOURCES) L.s = 0.0f;
-            else L.s = fmaxf(fminf(sinf(F.phi_min + F.phi_range * u), F.max_scaling), -F.max_scaling);
+            else {
+                float sn, cs;
+                sincos_red(F.phi_min + F.phi_range * u, sn, cs);
+                L.s = fmaxf(fminf(sn, F.max_scaling), -F.max_scaling);
+            }
             L.mp = L.pos;
             Field<FK>::eval(F, L.tab, L.mp, L.s, L.mn, L.mg);
             L.dir = mul(L.dir, L.mn);                     // photon.cpp:329

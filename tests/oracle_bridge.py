@@ -89,8 +89,11 @@ def oracle_trace(setup, first: int, n: int, weight_photons: int, uniforms=None, 
 
 
 def oracle_field(setup, scaling: float, points: np.ndarray, real_bits: int = 64):
+    return oracle_field_desc(setup.field_desc(), scaling, points, real_bits)
+
+
+def oracle_field_desc(fd, scaling: float, points: np.ndarray, real_bits: int = 64):
     lib = oracle()
-    fd = setup.field_desc()
     pts = np.ascontiguousarray(points, dtype=np.float64)
     n = np.zeros(len(pts))
     g = np.zeros((len(pts), 3))
