@@ -19,6 +19,7 @@
 
 #include "kparams.h"
 #include "march.cuh"
+#include "wavefront.cuh"
 
 using namespace smp;
 
@@ -269,6 +270,41 @@ static MarchFn march_fn(int fk) {
 
 static const int kBlock = 128;
 
+typedef void (*WaveFn)(KParams, WaveParams, int);
+static WaveFn wf_march_fn(int fk) {
+    switch (fk) {
+        case FK_BESSEL0: return wf_march_kernel<FK_BESSEL0>;
+        case FK_BESSEL1: return wf_march_kernel<FK_BESSEL1>;
+        case FK_BESSEL2: return wf_march_kernel<FK_BESSEL2>;
+        case FK_PLANEWAVE: return wf_march_kernel<FK_PLANEWAVE>;
+        case FK_SOURCES: return wf_march_kernel<FK_SOURCES>;
+        case FK_SPLINE: return wf_march_kernel<FK_SPLINE>;
+        default: return nullptr;
+    }
+}
+static WaveFn wf_finish_fn(int fk) {
+    switch (fk) {
+        case FK_BESSEL0: return wf_finish_kernel<FK_BESSEL0>;
+        case FK_BESSEL1: return wf_finish_kernel<FK_BESSEL1>;
+        case FK_BESSEL2: return wf_finish_kernel<FK_BESSEL2>;
+        case FK_PLANEWAVE: return wf_finish_kernel<FK_PLANEWAVE>;
+        case FK_SOURCES: return wf_finish_kernel<FK_SOURCES>;
+        case FK_SPLINE: return wf_finish_kernel<FK_SPLINE>;
+        default: return nullptr;
+    }
+}
+static WaveFn wf_event_fn(int fk) {
+    switch (fk) {
+        case FK_BESSEL0: return wf_event_kernel<FK_BESSEL0>;
+        case FK_BESSEL1: return wf_event_kernel<FK_BESSEL1>;
+        case FK_BESSEL2: return wf_event_kernel<FK_BESSEL2>;
+        case FK_PLANEWAVE: return wf_event_kernel<FK_PLANEWAVE>;
+        case FK_SOURCES: return wf_event_kernel<FK_SOURCES>;
+        case FK_SPLINE: return wf_event_kernel<FK_SPLINE>;
+        default: return nullptr;
+    }
+}
+
 static int grid_for(int fk, int dev, int blocks_per_sm, size_t smem, int *grid) {
     MarchFn fn = march_fn(fk);
     int per_sm = blocks_per_sm;
@@ -304,6 +340,17 @@ struct smp_plan {
     unsigned long long *d_counters = nullptr;
     smp_stats stats;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> launches;   // since the last clear
+    // the slot pool of the two-kernel march (wavefront.cuh); allocated at the first trace
+    bool persistent = false;    // SMP_KERNEL=persistent: the single-kernel march of march.cuh instead
+    int wave_chunk = 64;
+    int wave_slots_per_lane = 2;
+    int wave_batch = 16;        // march/event launch pairs between live-slot checks
+    void *d_wave = nullptr;
+    size_t wave_bytes = 0;
+    WaveParams wp;
+    int grid_march = 0, grid_event = 0, grid_finish = 0;
+    unsigned *h_live = nullptr; // pinned
+    cudaEvent_t live_ev = nullptr;
 };
 
 static void drop_launch_events(smp_plan *p) {
@@ -322,6 +369,9 @@ static void plan_free(smp_plan *p) {
     cudaFree(p->d_btab);
     cudaFree(p->d_film);
     cudaFree(p->d_counters);
+    cudaFree(p->d_wave);
+    if (p->h_live) cudaFreeHost(p->h_live);
+    if (p->live_ev) cudaEventDestroy(p->live_ev);
     drop_launch_events(p);
     delete p;
 }
@@ -431,6 +481,10 @@ int smp_plan_create(const smp_scene_desc *scene, const smp_medium_desc *medium, 
     smp_plan *p = new smp_plan();
     p->device = opts->device;
     if (const char *eb = std::getenv("SMP_EVENT_BATCH")) p->event_batch = std::max(1, std::min(32, std::atoi(eb)));
+    if (const char *kn = std::getenv("SMP_KERNEL")) p->persistent = std::strcmp(kn, "persistent") == 0;
+    if (const char *c = std::getenv("SMP_WF_CHUNK")) p->wave_chunk = std::max(2, std::min(4096, std::atoi(c)));
+    if (const char *c = std::getenv("SMP_WF_SLOTS")) p->wave_slots_per_lane = std::max(1, std::min(16, std::atoi(c)));
+    if (const char *c = std::getenv("SMP_WF_BATCH")) p->wave_batch = std::max(1, std::min(256, std::atoi(c)));
     p->scene = *scene;
     p->medium = *medium;
     p->opts = *opts;
@@ -554,6 +608,100 @@ static float photon_weight(const smp_scene_desc &s, int64_t n) {
     return float(s.Li) * T / float(n);
 }
 
+// Grid sizes from occupancy for the plan's current field kind, and the slot pool (slots = lanes of
+// the march grid x wave_slots_per_lane), allocated at the first trace and grown if a new field
+// kind needs more.
+static int wave_setup(smp_plan *p) {
+    WaveFn fm = wf_march_fn(p->fk), fe = wf_event_fn(p->fk), ff = wf_finish_fn(p->fk);
+    if (!fm || !fe || !ff) return set_error(SMP_ERR_BAD_ARG, "bad field kind");
+    int sms = 0, pm = 0, pe = 0, pf = 0;
+    SMP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device));
+    SMP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pm, fm, kBlock, p->smem_bytes));
+    SMP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pe, fe, kBlock, 0));
+    SMP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, ff, kBlock, p->smem_bytes));
+    p->grid_march = sms * std::max(pm, 1);
+    p->grid_event = sms * std::max(pe, 1);
+    p->grid_finish = sms * std::max(pf, 1);
+    const size_t n = size_t(p->grid_march) * kBlock * size_t(p->wave_slots_per_lane);
+    p->wp.chunk = p->wave_chunk;
+    if (p->d_wave && size_t(p->wp.n_slots) >= n) return SMP_OK;
+    cudaFree(p->d_wave);
+    p->d_wave = nullptr;
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t b4 = al(n * sizeof(float4)), bi = al(n * sizeof(int4)), bd = al(n * sizeof(double)),
+                 be = al(n * sizeof(EventPart)), bl = al(n * sizeof(int));
+    const size_t bytes = 4 * b4 + bi + bd + be + 4 * bl + 256;
+    cudaError_t e = cudaMalloc(&p->d_wave, bytes);
+    if (e != cudaSuccess) {
+        p->d_wave = nullptr;
+        return set_error(e == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "slot pool (%zu bytes): %s", bytes, cudaGetErrorString(e));
+    }
+    p->wave_bytes = bytes;
+    char *b = static_cast<char *>(p->d_wave);
+    WaveParams &W = p->wp;
+    W.ma = reinterpret_cast<float4 *>(b); b += b4;
+    W.mb = reinterpret_cast<float4 *>(b); b += b4;
+    W.mc = reinterpret_cast<float4 *>(b); b += b4;
+    W.mdd = reinterpret_cast<float4 *>(b); b += b4;
+    W.mi = reinterpret_cast<int4 *>(b); b += bi;
+    W.mt = reinterpret_cast<double *>(b); b += bd;
+    W.ev = reinterpret_cast<EventPart *>(b); b += be;
+    W.list[0] = reinterpret_cast<int *>(b); b += bl;
+    W.list[1] = reinterpret_cast<int *>(b); b += bl;
+    W.queue[0] = reinterpret_cast<int *>(b); b += bl;
+    W.queue[1] = reinterpret_cast<int *>(b); b += bl;
+    W.cnt = reinterpret_cast<unsigned *>(b);
+    W.n_slots = int(n);
+    if (!p->h_live) SMP_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&p->h_live), 2 * sizeof(unsigned), cudaHostAllocDefault));
+    if (!p->live_ev) SMP_CUDA(cudaEventCreateWithFlags(&p->live_ev, cudaEventDisableTiming));
+    return SMP_OK;
+}
+
+// The two-kernel march: fill the slots, then alternate march and event launches in batches of
+// wave_batch pairs until no slot is live. The live count after each batch is read back while the
+// next batch is already queued, so the device does not idle during the check.
+static int wave_run(smp_plan *p, const KParams &k, cudaStream_t s) {
+    int rc = wave_setup(p);
+    if (rc) return rc;
+    WaveFn fm = wf_march_fn(p->fk), fe = wf_event_fn(p->fk), ff = wf_finish_fn(p->fk);
+    WaveParams W = p->wp;
+    // once the live slots fit in one persistent grid, the finisher runs them to the end
+    const unsigned finish_at = unsigned(p->grid_finish) * unsigned(kBlock);
+    SMP_CUDA(cudaMemsetAsync(W.cnt, 0, 4 * sizeof(unsigned), s));
+    fe<<<p->grid_event, kBlock, 0, s>>>(k, W, -1);
+    SMP_CUDA(cudaGetLastError());
+    // every live photon advances at least one ER step per march launch, and no photon takes more
+    // than step_cap steps, so the loop ends; the cap below only guards the host against a defect
+    const long long max_iter = (long long)k.step_cap * 4 + (1LL << 20);
+    long long it = 0;
+    bool pending = false;
+    for (;;) {
+        for (int j = 0; j < p->wave_batch; ++j, ++it) {
+            fm<<<p->grid_march, kBlock, p->smem_bytes, s>>>(k, W, int(it & 0x3fffffff));
+            fe<<<p->grid_event, kBlock, 0, s>>>(k, W, int(it & 0x3fffffff));
+        }
+        SMP_CUDA(cudaGetLastError());
+        if (pending) {                              // the previous batch's count
+            SMP_CUDA(cudaEventSynchronize(p->live_ev));
+            const unsigned live = p->h_live[0];
+            if (live == 0u) break;
+            // Fewer live slots than the slot pool means the photon counter is exhausted, and from
+            // then on the count only falls, so the batch queued since holds at most `live`.
+            if (live <= finish_at && live < unsigned(W.n_slots)) {
+                ff<<<p->grid_finish, kBlock, p->smem_bytes, s>>>(k, W, int(it & 0x3fffffff));
+                SMP_CUDA(cudaGetLastError());
+                break;
+            }
+        }
+        // live slots after this batch = the march list the next march launch reads
+        SMP_CUDA(cudaMemcpyAsync(p->h_live, W.cnt + (it & 1), sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        SMP_CUDA(cudaEventRecord(p->live_ev, s));
+        pending = true;
+        if (it > max_iter) return set_error(SMP_ERR_CUDA, "march loop did not drain after %lld launches", it);
+    }
+    return SMP_OK;
+}
+
 static int launch(smp_plan *plan, int64_t first, int64_t n, int64_t weight_photons, cudaStream_t s,
                   const float *d_stream, const long long *d_offsets, smp_photon_record *d_records) {
     if (n <= 0) return SMP_OK;
@@ -575,8 +723,13 @@ static int launch(smp_plan *plan, int64_t first, int64_t n, int64_t weight_photo
     SMP_CUDA(cudaEventCreate(&e1));
     plan->launches.emplace_back(e0, e1);
     SMP_CUDA(cudaEventRecord(e0, s));
-    march_fn(plan->fk)<<<plan->grid, kBlock, plan->smem_bytes, s>>>(k);
-    SMP_CUDA(cudaGetLastError());
+    if (plan->persistent) {
+        march_fn(plan->fk)<<<plan->grid, kBlock, plan->smem_bytes, s>>>(k);
+        SMP_CUDA(cudaGetLastError());
+    } else {
+        int rc = wave_run(plan, k, s);
+        if (rc) return rc;
+    }
     SMP_CUDA(cudaEventRecord(e1, s));
     return SMP_OK;
 }
@@ -601,6 +754,7 @@ static int collect_stats(smp_plan *plan) {
     plan->stats.stream_exhausted = (int64_t)c[CNT_STREAM];
     plan->stats.kernel_ms = ms_total;
     if (c[CNT_STAGE_TIMEOUT]) return set_error(SMP_ERR_CUDA, "%llu block(s) timed out staging the field table", c[CNT_STAGE_TIMEOUT]);
+    if (c[CNT_LOST]) return set_error(SMP_ERR_CUDA, "internal: %llu live slot(s) had no lane in the tail kernel", c[CNT_LOST]);
     if (c[CNT_STEP_CAP]) return set_error(SMP_ERR_STEP_CAP, "%llu photon(s) hit the per-photon step cap", c[CNT_STEP_CAP]);
     if (c[CNT_NAN]) return set_error(SMP_ERR_NAN, "%llu photon(s) produced a non-finite state", c[CNT_NAN]);
     if (c[CNT_STREAM]) return set_error(SMP_ERR_STREAM, "%llu photon(s) ran out of injected uniforms", c[CNT_STREAM]);

@@ -106,7 +106,8 @@ enum Counter : int {
     CNT_STREAM = 5,
     CNT_PHOTONS = 6,
     CNT_STAGE_TIMEOUT = 7,   // a block gave up waiting for its shared-memory staging copy
-    CNT_COUNT = 8
+    CNT_LOST = 8,            // live slots the tail kernel had no lane for (a host defect)
+    CNT_COUNT = 9
 };
 
 }  // namespace smp

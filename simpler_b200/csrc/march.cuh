@@ -325,8 +325,9 @@ __device__ __forceinline__ void begin_march(Lane &L, const KParams &P, float dli
 
 // One iteration of the traceTillBlock loop (scene.cpp:395-419). Returns true when the march
 // has ended (loop exhausted, refinement exhausted, or the photon aborted).
-template <int FK>
-__device__ __forceinline__ bool march_step(Lane &L, const KParams &P) {
+// S is a Lane or any state with the same march members (the wavefront march kernel's MarchState).
+template <int FK, class S>
+__device__ __forceinline__ bool march_step(S &L, const KParams &P) {
     const float hh = 0.5f * L.cur;
     float3 d = f3(fmaf(hh, L.mg.x, L.md.x), fmaf(hh, L.mg.y, L.md.y), fmaf(hh, L.mg.z, L.md.z));
     const float hinv = L.cur * rcp_fast(L.mn);
@@ -639,25 +640,15 @@ __device__ __noinline__ bool stage_to_shared(void *dst, const void *src, unsigne
     return __syncthreads_and(ok ? 1 : 0) != 0;
 }
 
+// The lane loop of the persistent kernel: event phase (lanes whose march ended, or that need a
+// photon, run their discrete logic together until every live lane marches again; photons come
+// from the global counter, one atomic per warp) alternating with the march phase (two ER steps per
+// vote until event_batch lanes, scaled by the live lanes, wait for events). A lane enters with
+// `st` = ST_FETCH (no photon) or ST_MARCH (a photon loaded mid-march). All 32 lanes call it.
 template <int FK>
-__global__ void __launch_bounds__(128, SMP_MIN_BLOCKS) march_kernel(const __grid_constant__ KParams P) {
-    extern __shared__ __align__(16) float4 smem_tab[];
-    const int lane = threadIdx.x & 31;
-    Lane L;
-    L.end = 0;
-    L.idx = 0;
-    L.tab = P.field.btab;
-    if (FK <= FK_BESSEL2 && P.field.btab != nullptr) {
-        if (!stage_to_shared(smem_tab, P.field.btab, unsigned(P.field.bnodes) * 16u, P.counters + CNT_STAGE_TIMEOUT))
-            return;                                  // whole block: other blocks take the photons
-        L.tab = smem_tab;
-    }
-    LaneStats S;
-    int st = ST_FETCH;
+__device__ __forceinline__ void lane_loop(Lane &L, int st, const KParams &P, LaneStats &S, int lane) {
     int pending_ev = EV_NEW;
     for (;;) {
-        // ---- event phase: lanes whose march ended (or that need a photon) run their discrete
-        // logic together, until every live lane is marching again
         for (;;) {
             unsigned need = __ballot_sync(kFull, st == ST_FETCH);
             if (need) {
@@ -685,7 +676,6 @@ __global__ void __launch_bounds__(128, SMP_MIN_BLOCKS) march_kernel(const __grid
         }
         const unsigned alive = __ballot_sync(kFull, st != ST_DONE);
         if (alive == 0) break;
-        // ---- march phase: step until event_batch lanes (scaled by the live lanes) have ended
         const int thr = max(1, (P.event_batch * __popc(alive) + 16) >> 5);
         for (;;) {
             // two steps per vote; a lane whose march ends on the first skips the second
@@ -697,7 +687,10 @@ __global__ void __launch_bounds__(128, SMP_MIN_BLOCKS) march_kernel(const __grid
             if (__popc(waiting) >= thr || !__any_sync(kFull, st == ST_MARCH)) break;
         }
     }
-    // warp-reduce the statistics, one atomic per warp per counter
+}
+
+// warp-reduces the statistics, one atomic per warp per counter
+__device__ __forceinline__ void flush_stats(LaneStats &S, const KParams &P, int lane) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         S.steps += __shfl_down_sync(kFull, S.steps, o);
@@ -707,7 +700,7 @@ __global__ void __launch_bounds__(128, SMP_MIN_BLOCKS) march_kernel(const __grid
         S.nan += __shfl_down_sync(kFull, S.nan, o);
         S.stream += __shfl_down_sync(kFull, S.stream, o);
     }
-    if (lane == 0) {
+    if (lane == 0 && S.photons) {
         atomicAdd(P.counters + CNT_STEPS, S.steps);
         atomicAdd(P.counters + CNT_SPLATS, S.splats);
         atomicAdd(P.counters + CNT_PHOTONS, S.photons);
@@ -715,6 +708,24 @@ __global__ void __launch_bounds__(128, SMP_MIN_BLOCKS) march_kernel(const __grid
         if (S.nan) atomicAdd(P.counters + CNT_NAN, S.nan);
         if (S.stream) atomicAdd(P.counters + CNT_STREAM, S.stream);
     }
+}
+
+template <int FK>
+__global__ void __launch_bounds__(128, SMP_MIN_BLOCKS) march_kernel(const __grid_constant__ KParams P) {
+    extern __shared__ __align__(16) float4 smem_tab[];
+    const int lane = threadIdx.x & 31;
+    Lane L;
+    L.end = 0;
+    L.idx = 0;
+    L.tab = P.field.btab;
+    if (FK <= FK_BESSEL2 && P.field.btab != nullptr) {
+        if (!stage_to_shared(smem_tab, P.field.btab, unsigned(P.field.bnodes) * 16u, P.counters + CNT_STAGE_TIMEOUT))
+            return;                                  // whole block: other blocks take the photons
+        L.tab = smem_tab;
+    }
+    LaneStats S;
+    lane_loop<FK>(L, ST_FETCH, P, S, lane);
+    flush_stats(S, P, lane);
 }
 
 // n(p), grad n(p) at host-given points with the march's own field code
