@@ -232,6 +232,52 @@ static void fill_field_params(const smp_field_desc &f, int fk, FieldParams &F) {
     }
     F.bh = float(kBesselH);
     F.binv_h = float(1.0 / kBesselH);
+    F.kb = F.k_r * F.binv_h;
+    // |grad n|_1 bounds for the march's checked windows. Bessel: |dn/dr| <= A k |J_m'| <= A k and
+    // |dn/(r dphi)| = A k m |J_m(x)|/x <= A k (J_{m-1} + J_{m+1} = 2m J_m / x), so |grad n|_1 <= 2 A k;
+    // the factor 4 leaves room for the table's interpolation error. Plane waves: sum |a_i| |k_i|_1.
+    F.grad_bound = 0.0f;
+    if (fk <= FK_BESSEL2) F.grad_bound = 4.0f * std::fabs(F.amp) * F.k_r;
+    if (fk == FK_PLANEWAVE) {
+        float G = 0.0f;
+        for (int i = 0; i < F.n_waves; ++i)
+            G += std::fabs(F.wamp[i]) * (std::fabs(F.wk[i][0]) + std::fabs(F.wk[i][1]) + std::fabs(F.wk[i][2]));
+        F.grad_bound = 2.0f * G;
+    }
+}
+
+// The box test of traceTillBlock, p - L > -eps and R - p > -eps in float, as thresholds:
+// near a face p - L is exact (Sterbenz), so the test is p > L - eps in real arithmetic, i.e.
+// p >= the smallest float above L - eps; likewise p <= the largest float below R + eps.
+static float float_above(double x) {
+    float f = float(x);
+    if (double(f) <= x) f = std::nextafter(f, HUGE_VALF);
+    while (double(std::nextafter(f, -HUGE_VALF)) > x) f = std::nextafter(f, -HUGE_VALF);
+    return f;
+}
+static float float_below(double x) {
+    float f = float(x);
+    if (double(f) >= x) f = std::nextafter(f, -HUGE_VALF);
+    while (double(std::nextafter(f, HUGE_VALF)) < x) f = std::nextafter(f, HUGE_VALF);
+    return f;
+}
+// traceTillBlock's step sizes: h0 and each refinement's current_stepsize / 10 in float
+static void set_step_sizes(KParams &k, const smp_field_desc &f) {
+    k.h0 = float(f.er_stepsize);
+    k.precision = std::max(0, std::min(int(f.precision), SMP_MAX_REFINE));
+    k.cur_tab[0] = k.h0;
+    for (int i = 1; i <= SMP_MAX_REFINE; ++i) {
+        volatile float q = k.cur_tab[i - 1] / 10.0f;     // one IEEE float division per level
+        k.cur_tab[i] = q;
+    }
+}
+
+static void set_box_thresholds(KParams &k) {
+    const double eps = double(1.19209290e-07f);
+    for (int i = 0; i < 3; ++i) {
+        k.box_lo[i] = float_above(double(k.L[i]) - eps);
+        k.box_hi[i] = float_below(double(k.R[i]) + eps);
+    }
 }
 
 // LargeDist of movePhotonTillSensor (scene.cpp:627): 1e4 m in the reference; by default capped
@@ -271,14 +317,14 @@ static MarchFn march_fn(int fk) {
 static const int kBlock = 128;
 
 typedef void (*WaveFn)(KParams, WaveParams, int);
-static WaveFn wf_march_fn(int fk) {
+static WaveFn wf_march_fn(int fk, bool fp64) {
     switch (fk) {
-        case FK_BESSEL0: return wf_march_kernel<FK_BESSEL0>;
-        case FK_BESSEL1: return wf_march_kernel<FK_BESSEL1>;
-        case FK_BESSEL2: return wf_march_kernel<FK_BESSEL2>;
-        case FK_PLANEWAVE: return wf_march_kernel<FK_PLANEWAVE>;
-        case FK_SOURCES: return wf_march_kernel<FK_SOURCES>;
-        case FK_SPLINE: return wf_march_kernel<FK_SPLINE>;
+        case FK_BESSEL0: return fp64 ? wf_march_kernel<FK_BESSEL0, 1> : wf_march_kernel<FK_BESSEL0, 0>;
+        case FK_BESSEL1: return fp64 ? wf_march_kernel<FK_BESSEL1, 1> : wf_march_kernel<FK_BESSEL1, 0>;
+        case FK_BESSEL2: return fp64 ? wf_march_kernel<FK_BESSEL2, 1> : wf_march_kernel<FK_BESSEL2, 0>;
+        case FK_PLANEWAVE: return fp64 ? wf_march_kernel<FK_PLANEWAVE, 1> : wf_march_kernel<FK_PLANEWAVE, 0>;
+        case FK_SOURCES: return fp64 ? wf_march_kernel<FK_SOURCES, 1> : wf_march_kernel<FK_SOURCES, 0>;
+        case FK_SPLINE: return fp64 ? wf_march_kernel<FK_SPLINE, 1> : wf_march_kernel<FK_SPLINE, 0>;
         default: return nullptr;
     }
 }
@@ -343,7 +389,7 @@ struct smp_plan {
     // the slot pool of the two-kernel march (wavefront.cuh); allocated at the first trace
     bool persistent = false;    // SMP_KERNEL=persistent: the single-kernel march of march.cuh instead
     int wave_chunk = 64;
-    int wave_slots_per_lane = 2;
+    int wave_slots_per_lane = 4;
     int wave_batch = 16;        // march/event launch pairs between live-slot checks
     void *d_wave = nullptr;
     size_t wave_bytes = 0;
@@ -382,6 +428,8 @@ static int check_descs(const smp_scene_desc *s, const smp_medium_desc *m, const 
     if (s->x_res <= 0 || s->y_res <= 0 || s->z_res <= 0) return set_error(SMP_ERR_BAD_ARG, "film resolution must be positive");
     if (s->tex_x <= 0 || s->tex_y <= 0 || !s->texture) return set_error(SMP_ERR_BAD_ARG, "texture missing");
     if (!(f->er_stepsize > 0.0)) return set_error(SMP_ERR_BAD_ARG, "er_stepsize must be positive");
+    if (f->precision > SMP_MAX_REFINE)
+        return set_error(SMP_ERR_UNSUPPORTED, "precision %d: at most %d refinement levels", f->precision, SMP_MAX_REFINE);
     if (!(f->f_u > 0.0) || !(f->speed_u > 0.0)) return set_error(SMP_ERR_BAD_ARG, "f_u and speed_u must be positive");
     if (o->precision != SMP_PREC_FP32 && o->precision != SMP_PREC_MIXED) return set_error(SMP_ERR_BAD_ARG, "bad precision");
     if (o->rng != SMP_RNG_PHILOX && o->rng != SMP_RNG_STREAM)
@@ -424,8 +472,7 @@ static int plan_setup_field(smp_plan *p, const smp_field_desc &f) {
         p->kp.field.bnodes = int(tab.size());
         p->smem_bytes = tab.size() * sizeof(float4);
     }
-    p->kp.h0 = float(f.er_stepsize);
-    p->kp.precision = f.precision;
+    set_step_sizes(p->kp, f);
     p->field = f;
     return grid_for(p->fk, p->device, p->opts.blocks_per_sm, p->smem_bytes, &p->grid);
 }
@@ -499,6 +546,7 @@ int smp_plan_create(const smp_scene_desc *scene, const smp_medium_desc *medium, 
         k.cam_origin[i] = float(scene->view_origin[i]);
         k.cam_lens_origin[i] = float(scene->sensor_lens_origin[i]);
     }
+    set_box_thresholds(k);
     k.plane[0] = float(scene->light_plane[0]);
     k.plane[1] = float(scene->light_plane[1]);
     k.pixsize[0] = k.plane[0] / float(scene->tex_x);
@@ -612,7 +660,7 @@ static float photon_weight(const smp_scene_desc &s, int64_t n) {
 // the march grid x wave_slots_per_lane), allocated at the first trace and grown if a new field
 // kind needs more.
 static int wave_setup(smp_plan *p) {
-    WaveFn fm = wf_march_fn(p->fk), fe = wf_event_fn(p->fk), ff = wf_finish_fn(p->fk);
+    WaveFn fm = wf_march_fn(p->fk, p->kp.fp64 != 0), fe = wf_event_fn(p->fk), ff = wf_finish_fn(p->fk);
     if (!fm || !fe || !ff) return set_error(SMP_ERR_BAD_ARG, "bad field kind");
     int sms = 0, pm = 0, pe = 0, pf = 0;
     SMP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device));
@@ -663,7 +711,7 @@ static int wave_setup(smp_plan *p) {
 static int wave_run(smp_plan *p, const KParams &k, cudaStream_t s) {
     int rc = wave_setup(p);
     if (rc) return rc;
-    WaveFn fm = wf_march_fn(p->fk), fe = wf_event_fn(p->fk), ff = wf_finish_fn(p->fk);
+    WaveFn fm = wf_march_fn(p->fk, p->kp.fp64 != 0), fe = wf_event_fn(p->fk), ff = wf_finish_fn(p->fk);
     WaveParams W = p->wp;
     // once the live slots fit in one persistent grid, the finisher runs them to the end
     const unsigned finish_at = unsigned(p->grid_finish) * unsigned(kBlock);
@@ -1086,6 +1134,7 @@ extern "C" int smp_render_noalloc(const smp_scene_desc *scene, const smp_medium_
         k.cam_origin[i] = float(scene->view_origin[i]);
         k.cam_lens_origin[i] = float(scene->sensor_lens_origin[i]);
     }
+    set_box_thresholds(k);
     k.plane[0] = float(scene->light_plane[0]);
     k.plane[1] = float(scene->light_plane[1]);
     k.pixsize[0] = k.plane[0] / float(scene->tex_x);
@@ -1137,8 +1186,7 @@ extern "C" int smp_render_noalloc(const smp_scene_desc *scene, const smp_medium_
     k.counters = d_counters;
     k.cdf = d_cdf;
     fill_field_params(*field, fk, k.field);
-    k.h0 = float(field->er_stepsize);
-    k.precision = field->precision;
+    set_step_sizes(k, *field);
 
     // texture CDF (pmf.h:41-99, float) into the static host buffer, then into the scratch
     float *cdf = g_noalloc_cdf_host;

@@ -23,31 +23,51 @@ static constexpr float kEps = 1.19209290e-07f;    // M_EPSILON (constants.h)
 // cos(m phi), sin(m phi) come from (z/r + i y/r)^m instead of atan2 + sincos.
 // Below r = M_EPSILON the gradient uses y = z = r = M_EPSILON as the reference does.
 template <int M>
-__device__ __forceinline__ void bessel_field(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) {
-    if (p.x > F.egap || p.x < F.sgap) {
-        n = F.n_o;
-        g = f3(0.0f, 0.0f, 0.0f);
-        return;
-    }
+__device__ __forceinline__ void bessel_field_ng(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) {
     float y = p.y, z = p.z;
     const float r2 = fmaf(y, y, z * z);
     float rs = rsqrt_fast(r2);                 // +inf at r2 = 0
+    const float A = F.amp * s;
+    float jm, jm1;
+    if (r2 * rs >= kEps) {                     // off the axis (false for r2 = 0: 0 * inf is NaN)
+        const float r = r2 * rs;
+        bessel_pair_table_t<M>(tab, F.bnodes, F.bh, F.kb * r, F.k_r * r, jm, jm1);
+        if (M == 0) {
+            // grad = A k J_0'(kr) (0, y, z)/r = -A k J_1(kr) (0, y, z)/r
+            n = fmaf(A, jm, F.n_o);
+            const float w = -(A * F.k_r) * jm1 * rs;
+            g = f3(0.0f, w * y, w * z);
+        } else if (M == 1) {
+            // n = n_o + A J_1(kr) z/r; with J_1' = J_1/(kr) - J_2 the gradient reduces to
+            // dn/dy = -A k J_2(kr) y z/r^2,  dn/dz = A J_1(kr)/r - A k J_2(kr) z^2/r^2
+            const float aj = A * jm * rs;
+            n = fmaf(aj, z, F.n_o);
+            const float wz = (A * F.k_r) * jm1 * (rs * rs) * z;
+            g = f3(0.0f, -wz * y, fmaf(-wz, z, aj));
+        } else {
+            const float c = z * rs, sn = y * rs;
+            const float cm = fmaf(c, c, -sn * sn), sm = 2.0f * c * sn;
+            n = fmaf(A * jm, cm, F.n_o);
+            const float djm = fmaf(float(M) * F.inv_k * rs, jm, -jm1);
+            const float a1 = A * djm * F.k_r * rs * cm;
+            const float a2 = A * jm * float(M) * sm * rs * rs;
+            g = f3(0.0f, fmaf(a1, y, -a2 * z), fmaf(a1, z, a2 * y));
+        }
+        return;
+    }
+    // on or next to the axis: the value at r, the gradient from y = z = r = M_EPSILON
+    // (scene.cpp:229-234); at r = 0, phi = atan2(0, 0) = 0
     float r = r2 > 0.0f ? r2 * rs : 0.0f;
-    // cos(m phi), sin(m phi) = (z/r + i y/r)^m; at r = 0, phi = atan2(0, 0) = 0
     float cm = 1.0f, sm = 0.0f;
     if (M > 0 && r2 > 0.0f) {
         const float c = z * rs, sn = y * rs;
         if (M == 1) { cm = c; sm = sn; }
         else { cm = fmaf(c, c, -sn * sn); sm = 2.0f * c * sn; }
     }
-    const float A = F.amp * s;
-    float jm, jm1;
     bessel_pair_table<M>(tab, F.bnodes, F.binv_h, F.bh, F.k_r * r, jm, jm1);
     n = fmaf(A * jm, cm, F.n_o);
-    if (!(r >= kEps)) {                        // the gradient's near-axis substitution (scene.cpp:229-234)
-        y = kEps; z = kEps; r = kEps; rs = 1.0f / kEps;
-        bessel_pair_table<M>(tab, F.bnodes, F.binv_h, F.bh, F.k_r * kEps, jm, jm1);
-    }
+    y = kEps; z = kEps; r = kEps; rs = 1.0f / kEps;
+    bessel_pair_table<M>(tab, F.bnodes, F.binv_h, F.bh, F.k_r * kEps, jm, jm1);
     // J_m'(kr) = (m/kr) J_m - J_{m+1}, with 1/(kr) = rs/k
     const float djm = (M == 0) ? -jm1 : fmaf(float(M) * F.inv_k * rs, jm, -jm1);
     const float a1 = A * djm * F.k_r * rs * cm;            // radial part / r
@@ -55,13 +75,18 @@ __device__ __forceinline__ void bessel_field(const FieldParams &F, const float4 
     g = f3(0.0f, fmaf(a1, y, -a2 * z), fmaf(a1, z, a2 * y));
 }
 
+// gap gating (rif_base.h:104-137): n_o and no gradient outside sgap <= x <= egap
+__device__ __forceinline__ bool in_gap(const FieldParams &F, float3 p) { return p.x > F.egap || p.x < F.sgap; }
+
+// In the gaps the amplitude is zeroed instead of branching: n = n_o + 0 and grad n = 0 exactly,
+// and every lane runs the same instructions.
+template <int M>
+__device__ __forceinline__ void bessel_field(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) {
+    bessel_field_ng<M>(F, tab, p, in_gap(F, p) ? 0.0f : s, n, g);
+}
+
 // Plane waves (not in the reference): n = n_o + sum_i a_i sin(k_i.p - tau + phase_i)
-__device__ __forceinline__ void wave_field(const FieldParams &F, float3 p, float tau, float &n, float3 &g) {
-    if (p.x > F.egap || p.x < F.sgap) {
-        n = F.n_o;
-        g = f3(0.0f, 0.0f, 0.0f);
-        return;
-    }
+__device__ __forceinline__ void wave_field_ng(const FieldParams &F, float3 p, float tau, float &n, float3 &g) {
     float acc = 0.0f;
     float3 gg = f3(0.0f, 0.0f, 0.0f);
     for (int i = 0; i < F.n_waves; ++i) {
@@ -76,6 +101,15 @@ __device__ __forceinline__ void wave_field(const FieldParams &F, float3 p, float
     }
     n = F.n_o + acc;
     g = gg;
+}
+
+__device__ __forceinline__ void wave_field(const FieldParams &F, float3 p, float tau, float &n, float3 &g) {
+    if (in_gap(F, p)) {
+        n = F.n_o;
+        g = f3(0.0f, 0.0f, 0.0f);
+        return;
+    }
+    wave_field_ng(F, p, tau, n, g);
 }
 
 // Spherical point sources on two arcs (scene.cpp:139-195, rif_sources.h:156-198):
@@ -192,21 +226,27 @@ __device__ __forceinline__ void spline_field(const FieldParams &F, float3 p, flo
 template <int FK> struct Field;
 template <> struct Field<FK_BESSEL0> {
     static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) { bessel_field<0>(F, tab, p, s, n, g); }
+    static __device__ __forceinline__ void eval_ng(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) { bessel_field_ng<0>(F, tab, p, s, n, g); }
 };
 template <> struct Field<FK_BESSEL1> {
     static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) { bessel_field<1>(F, tab, p, s, n, g); }
+    static __device__ __forceinline__ void eval_ng(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) { bessel_field_ng<1>(F, tab, p, s, n, g); }
 };
 template <> struct Field<FK_BESSEL2> {
     static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) { bessel_field<2>(F, tab, p, s, n, g); }
+    static __device__ __forceinline__ void eval_ng(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) { bessel_field_ng<2>(F, tab, p, s, n, g); }
 };
 template <> struct Field<FK_PLANEWAVE> {
     static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *, float3 p, float s, float &n, float3 &g) { wave_field(F, p, s, n, g); }
+    static __device__ __forceinline__ void eval_ng(const FieldParams &F, const float4 *, float3 p, float s, float &n, float3 &g) { wave_field_ng(F, p, s, n, g); }
 };
 template <> struct Field<FK_SOURCES> {
     static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *, float3 p, float, float &n, float3 &g) { sources_field(F, p, n, g); }
+    static __device__ __forceinline__ void eval_ng(const FieldParams &F, const float4 *, float3 p, float, float &n, float3 &g) { sources_field(F, p, n, g); }
 };
 template <> struct Field<FK_SPLINE> {
     static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *, float3 p, float, float &n, float3 &g) { spline_field(F, p, n, g); }
+    static __device__ __forceinline__ void eval_ng(const FieldParams &F, const float4 *, float3 p, float, float &n, float3 &g) { spline_field(F, p, n, g); }
 };
 
 }  // namespace smp

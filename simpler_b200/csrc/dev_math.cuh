@@ -129,7 +129,7 @@ template <int M> __device__ __forceinline__ float bessel_small(float h, float q)
 
 // J_0 and J_1 for x >= 3 (A&S 9.4.3, 9.4.6)
 __device__ __forceinline__ void bessel01_large(float x, float &j0, float &j1) {
-    float y = 3.0f / x;
+    float y = 3.0f * rcp_fast(x);
     float f0 = 0.00014476f;
     f0 = fmaf(f0, y, -0.00072805f); f0 = fmaf(f0, y, 0.00137237f); f0 = fmaf(f0, y, -0.00009512f);
     f0 = fmaf(f0, y, -0.00552740f); f0 = fmaf(f0, y, -0.00000077f); f0 = fmaf(f0, y, 0.79788456f);
@@ -169,7 +169,7 @@ template <int M> __device__ __forceinline__ void bessel_pair(float x, float &jm,
         float j0, j1;
         bessel01_large(x, j0, j1);
         if (M == 0) { jm = j0; jm1 = j1; return; }
-        float ix = 1.0f / x;
+        float ix = rcp_fast(x);
         float j2 = fmaf(2.0f * ix, j1, -j0);
         if (M == 1) { jm = j1; jm1 = j2; return; }
         float j3 = fmaf(4.0f * ix, j2, -j1);
@@ -186,6 +186,29 @@ __device__ __forceinline__ void bessel_pair_table(const float4 *tab, int nodes, 
     if (t < float(nodes - 1)) {
         float f;
         const int i = floor_frac(t, f);
+        const float4 a = tab[i], b = tab[i + 1];
+        const float g = 1.0f - f;
+        const float g2 = g * g, f2 = f * f;
+        const float h00 = fmaf(2.0f, f, 1.0f) * g2;
+        const float h01 = f2 * fmaf(-2.0f, f, 3.0f);
+        const float h10 = f * g2 * h;
+        const float h11 = -f2 * g * h;
+        jm = fmaf(h00, a.x, fmaf(h10, a.y, fmaf(h01, b.x, h11 * b.y)));
+        jm1 = fmaf(h00, a.z, fmaf(h10, a.w, fmaf(h01, b.z, h11 * b.w)));
+    } else {
+        bessel_pair<M>(x, jm, jm1);
+    }
+}
+
+// The same lookup from t = x / h (x passed for arguments beyond the table): floor(t) by a
+// round-down add of 2^23, which leaves t - floor(t) exact without a correction step.
+template <int M>
+__device__ __forceinline__ void bessel_pair_table_t(const float4 *tab, int nodes, float h, float t, float x,
+                                                    float &jm, float &jm1) {
+    if (t < float(nodes - 1)) {
+        const float tb = __fadd_rd(t, 8388608.0f);
+        const int i = __float_as_int(tb) - 0x4B000000;
+        const float f = t - (tb - 8388608.0f);
         const float4 a = tab[i], b = tab[i + 1];
         const float g = 1.0f - f;
         const float g2 = g * g, f2 = f * f;

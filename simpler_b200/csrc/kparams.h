@@ -47,11 +47,17 @@ struct FieldParams {
     const float4 *btab;
     int bnodes;
     float bh, binv_h;
+    float kb;               // k_r / bh: table coordinate per metre of r
+    float grad_bound;       // bound on |grad n|_1 anywhere (0: unknown)
 };
+
+#define SMP_MAX_REFINE 39
 
 struct KParams {
     // medium box (block.cpp)
     float L[3], R[3];
+    // the same box as exact float thresholds: p - L > -eps  <=>  p >= box_lo, R - p > -eps  <=>  p <= box_hi
+    float box_lo[3], box_hi[3];
     // textured source (area_textured_source)
     float src_origin[3];
     float plane[2], pixsize[2];
@@ -78,7 +84,8 @@ struct KParams {
     float weight;
     float h0;
     float large_dist;       // movePhotonTillSensor path budget (LargeDist)
-    int precision;
+    int precision;          // refinement levels, <= SMP_MAX_REFINE
+    float cur_tab[SMP_MAX_REFINE + 1];   // h0, h0/10, (h0/10)/10, ... as traceTillBlock divides in float
     int step_cap;
     // film
     void *film;

@@ -54,8 +54,9 @@ struct Lane {
     float mn;                 // n at mp
     double mtot;              // optical length accumulated by this march (FP64 form)
     float mtotf;              // the same in the FP32 form
-    float dist_acc, dlimit, cur;
-    int rem_steps;
+    float dist_acc, dlimit, cur, hh;   // hh = cur / 2
+    double cur_d;             // cur in double for the FP64 accumulator
+    int stop;                 // step count at which traceTillBlock's loop count runs out (<= step cap)
     int prec, ctx, first;
     float large, d2s, rem, sampled;
     const float4 *tab;        // Bessel table in this block's shared memory
@@ -113,10 +114,6 @@ __device__ __forceinline__ int steps_for(float dlimit, float h0) {
     return int(v);
 }
 
-__device__ __forceinline__ bool inside_box(const KParams &P, float3 p) {
-    return (p.x - P.L[0] > -kEps) && (P.R[0] - p.x > -kEps) && (p.y - P.L[1] > -kEps) &&
-           (P.R[1] - p.y > -kEps) && (p.z - P.L[2] > -kEps) && (P.R[2] - p.z > -kEps);
-}
 
 // nearest face of the medium box (scene.cpp:655-676 / :736-757)
 __device__ __forceinline__ float3 face_normal(const KParams &P, float3 p) {
@@ -318,42 +315,65 @@ __device__ __forceinline__ void begin_march(Lane &L, const KParams &P, float dli
     L.dist_acc = 0.0f;
     L.dlimit = dlimit;
     L.cur = P.h0;
+    L.hh = 0.5f * P.h0;
+    L.cur_d = double(P.h0);
     L.prec = P.precision;
-    L.rem_steps = steps_for(dlimit, P.h0);
+    L.stop = int(min((long long)L.steps + (long long)steps_for(dlimit, P.h0), (long long)P.step_cap));
     L.mtotf = float(L.mtot);
 }
+// a march with no steps ends at once (traceTillBlock's maxsteps <= 0)
+__device__ __forceinline__ bool march_has_steps(const Lane &L) { return L.stop > L.steps; }
 
-// One iteration of the traceTillBlock loop (scene.cpp:395-419). Returns true when the march
-// has ended (loop exhausted, refinement exhausted, or the photon aborted).
-// S is a Lane or any state with the same march members (the wavefront march kernel's MarchState).
-template <int FK, class S>
+// One iteration of the traceTillBlock loop (scene.cpp:395-419): kick, drift, one fused field
+// evaluation, kick, then the loop's tests. Returns true when the march has ended (loop count or
+// refinement exhausted, or the photon aborted). S is a Lane or any state with the same march
+// members.
+//
+// The tests are arranged for the common case, an accepted step with steps to go: the box test
+// (thresholds box_lo/box_hi, exact) and the distance test (dist_acc + cur <= dlimit) are one
+// minimum compared with 0, and the loop count and the step cap share one counter (`stop` is
+// the loop's end clamped to the cap; the cap is told apart on the rare path).
+template <int FK, int FP = -1, class S>
 __device__ __forceinline__ bool march_step(S &L, const KParams &P) {
-    const float hh = 0.5f * L.cur;
-    float3 d = f3(fmaf(hh, L.mg.x, L.md.x), fmaf(hh, L.mg.y, L.md.y), fmaf(hh, L.mg.z, L.md.z));
+    const bool f64 = FP < 0 ? P.fp64 != 0 : FP != 0;     // FP: the path-length form, if fixed at compile time
+    const float3 d = f3(fmaf(L.hh, L.mg.x, L.md.x), fmaf(L.hh, L.mg.y, L.md.y), fmaf(L.hh, L.mg.z, L.md.z));
     const float hinv = L.cur * rcp_fast(L.mn);
-    float3 p = f3(fmaf(d.x, hinv, L.mp.x), fmaf(d.y, hinv, L.mp.y), fmaf(d.z, hinv, L.mp.z));
+    const float3 p = f3(fmaf(d.x, hinv, L.mp.x), fmaf(d.y, hinv, L.mp.y), fmaf(d.z, hinv, L.mp.z));
     float n2;
     float3 g2;
     Field<FK>::eval(P.field, L.tab, p, L.s, n2, g2);
-    d = f3(fmaf(hh, g2.x, d.x), fmaf(hh, g2.y, d.y), fmaf(hh, g2.z, d.z));
+    const float3 d2 = f3(fmaf(L.hh, g2.x, d.x), fmaf(L.hh, g2.y, d.y), fmaf(L.hh, g2.z, d.z));
     ++L.steps;
-    // A non-finite position fails the box test below, so refinement ends the march within
+    const float sacc = L.dist_acc + L.cur;
+    float m = fminf(fminf(p.x - P.box_lo[0], P.box_hi[0] - p.x), fminf(p.y - P.box_lo[1], P.box_hi[1] - p.y));
+    m = fminf(m, fminf(fminf(p.z - P.box_lo[2], P.box_hi[2] - p.z), L.dlimit - sacc));
+    const bool ok = m >= 0.0f;
+    if (ok && L.steps < L.stop) {
+        L.mp = p; L.md = d2; L.mn = n2; L.mg = g2;
+        L.dist_acc = sacc;
+        if (f64) L.mtot = fma(L.cur_d, double(n2), L.mtot);
+        else L.mtotf = fmaf(L.cur, n2, L.mtotf);
+        return false;
+    }
+    // A non-finite position fails the box test, so refinement ends the march within
     // `precision` steps; run_events checks finiteness when the march ends.
     if (L.steps >= P.step_cap) { L.end = SMP_END_STEP_CAP; return true; }
-    if (!inside_box(P, p) || (L.dist_acc + L.cur) > L.dlimit) {
-        if (--L.prec < 0) {                      // refinement exhausted: keep the failed step
-            L.mp = p; L.md = d; L.mn = n2; L.mg = g2;
-            return true;
-        }
-        L.cur = L.cur / 10.0f;                    // restore (mp, md unchanged) and refine
-        L.rem_steps = 11;
-    } else {
-        L.mp = p; L.md = d; L.mn = n2; L.mg = g2;
-        L.dist_acc += L.cur;
-        if (P.fp64) L.mtot = fma(double(L.cur), double(n2), L.mtot);
+    if (ok) {                                     // accepted, and the loop count is exhausted
+        L.mp = p; L.md = d2; L.mn = n2; L.mg = g2;
+        L.dist_acc = sacc;
+        if (f64) L.mtot = fma(L.cur_d, double(n2), L.mtot);
         else L.mtotf = fmaf(L.cur, n2, L.mtotf);
+        return true;
     }
-    return --L.rem_steps <= 0;
+    if (--L.prec < 0) {                           // refinement exhausted: keep the failed step
+        L.mp = p; L.md = d2; L.mn = n2; L.mg = g2;
+        return true;
+    }
+    L.cur = P.cur_tab[P.precision - L.prec];      // restore (mp, md unchanged) and refine: cur / 10
+    L.hh = 0.5f * L.cur;
+    L.cur_d = double(L.cur);
+    L.stop = min(L.steps + 10, P.step_cap);       // maxsteps = 11 from i = 0: ten more steps
+    return false;
 }
 
 // ---- discrete logic between marches ---------------------------------------------------------
@@ -404,7 +424,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
                 L.first = 1;
                 L.large = P.large_dist;
                 begin_march<FK>(L, P, L.large, false);
-                if (L.rem_steps > 0) return ST_MARCH;
+                if (march_has_steps(L)) return ST_MARCH;
                 ev = EV_MARCH_END;
             } else {
                 ev = EV_SCATTER;
@@ -428,7 +448,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
                         if (dot3(d1, n) < 0.0f) {
                             L.md = d1;
                             begin_march<FK>(L, P, L.large, false);
-                            if (L.rem_steps > 0) return ST_MARCH;
+                            if (march_has_steps(L)) return ST_MARCH;
                             ev = EV_MARCH_END;
                             break;
                         }
@@ -494,7 +514,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
                     if (dot3(d1, n) < 0.0f) {
                         L.md = mul(d1, mag);
                         begin_march<FK>(L, P, L.rem, false);
-                        if (L.rem_steps > 0) return ST_MARCH;
+                        if (march_has_steps(L)) return ST_MARCH;
                         ev = EV_MARCH_END;
                         break;
                     }
@@ -520,7 +540,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
             L.md = L.dir;
             L.mtot = L.total;
             begin_march<FK>(L, P, dist, true);
-            if (L.rem_steps > 0) return ST_MARCH;
+            if (march_has_steps(L)) return ST_MARCH;
             ev = EV_MARCH_END;
             break;
         }
@@ -538,7 +558,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
                 L.first = 1;
                 L.large = P.large_dist;
                 begin_march<FK>(L, P, L.large, false);
-                if (L.rem_steps > 0) return ST_MARCH;
+                if (march_has_steps(L)) return ST_MARCH;
                 ev = EV_MARCH_END;
                 break;
             }
@@ -557,7 +577,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
             L.md = L.dir;
             L.mtot = L.total;
             begin_march<FK>(L, P, dist, true);
-            if (L.rem_steps > 0) return ST_MARCH;
+            if (march_has_steps(L)) return ST_MARCH;
             ev = EV_MARCH_END;
             break;
         }

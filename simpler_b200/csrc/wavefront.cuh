@@ -27,15 +27,15 @@
 namespace smp {
 
 #ifndef SMP_WF_MARCH_MIN_BLOCKS
-#define SMP_WF_MARCH_MIN_BLOCKS 8
+#define SMP_WF_MARCH_MIN_BLOCKS 6
 #endif
 
 // the state march_step reads and writes
 struct MarchState {
     float3 mp, md, mg;
-    float mn, cur, dist_acc, dlimit, s, mtotf;
-    double mtot;
-    int steps, end, prec, rem_steps;
+    float mn, cur, dist_acc, dlimit, s, mtotf, hh;
+    double mtot, cur_d;
+    int steps, end, prec, stop;
     const float4 *tab;
 };
 
@@ -58,7 +58,7 @@ struct WaveParams {
     float4 *mb;        // md.xyz, cur
     float4 *mc;        // mg.xyz, dist_acc
     float4 *mdd;       // dlimit, s, mtotf, -
-    int4 *mi;          // steps, end, prec, rem_steps
+    int4 *mi;          // steps, end, prec, stop
     double *mt;        // mtot (FP64 path-length form only)
     EventPart *ev;
     int *list[2];      // march lists, by iteration parity
@@ -75,7 +75,9 @@ __device__ __forceinline__ void wf_load_march(const WaveParams &W, const KParams
     M.md = f3(b.x, b.y, b.z); M.cur = b.w;
     M.mg = f3(c.x, c.y, c.z); M.dist_acc = c.w;
     M.dlimit = d.x; M.s = d.y; M.mtotf = d.z;
-    M.steps = e.x; M.end = e.y; M.prec = e.z; M.rem_steps = e.w;
+    M.steps = e.x; M.end = e.y; M.prec = e.z; M.stop = e.w;
+    M.hh = 0.5f * M.cur;
+    M.cur_d = double(M.cur);
     M.mtot = P.fp64 ? W.mt[slot] : 0.0;
 }
 
@@ -85,7 +87,7 @@ __device__ __forceinline__ void wf_store_march(const WaveParams &W, const KParam
     W.mb[slot] = make_float4(M.md.x, M.md.y, M.md.z, M.cur);
     W.mc[slot] = make_float4(M.mg.x, M.mg.y, M.mg.z, M.dist_acc);
     W.mdd[slot] = make_float4(M.dlimit, M.s, M.mtotf, 0.0f);
-    W.mi[slot] = make_int4(M.steps, M.end, M.prec, M.rem_steps);
+    W.mi[slot] = make_int4(M.steps, M.end, M.prec, M.stop);
     if (P.fp64) W.mt[slot] = M.mtot;
 }
 
@@ -94,7 +96,8 @@ __device__ __forceinline__ void wf_load_lane(const WaveParams &W, const KParams 
     wf_load_march(W, P, slot, M);
     L.mp = M.mp; L.mn = M.mn; L.md = M.md; L.cur = M.cur; L.mg = M.mg; L.dist_acc = M.dist_acc;
     L.dlimit = M.dlimit; L.s = M.s; L.mtotf = M.mtotf; L.mtot = M.mtot;
-    L.steps = M.steps; L.end = M.end; L.prec = M.prec; L.rem_steps = M.rem_steps;
+    L.steps = M.steps; L.end = M.end; L.prec = M.prec; L.stop = M.stop;
+    L.hh = M.hh; L.cur_d = M.cur_d;
     const EventPart &E = W.ev[slot];
     L.idx = E.idx; L.total = E.total; L.spos = E.spos; L.send = E.send;
     L.pos = E.pos; L.dir = E.dir; L.totalDist = E.totalDist;
@@ -128,19 +131,22 @@ __device__ __forceinline__ void warp_append(int *arr, unsigned *cnt, unsigned ma
 
 // March launch `it`: slots on list[it & 1] advance up to `chunk` ER steps each. When fewer slots
 // are live than the grid has lanes, the chunk grows in proportion (up to 64x) so the last photons
-// are not paced by launch latency.
-template <int FK>
-__global__ void __launch_bounds__(128, FK == FK_SPLINE ? SMP_WF_MARCH_MIN_BLOCKS - 3 : SMP_WF_MARCH_MIN_BLOCKS)
+// are not paced by launch latency. F64: the FP64 path-length form (only its accumulator is
+// loaded, carried and stored).
+template <int FK, int F64>
+__global__ void __launch_bounds__(128, FK == FK_SPLINE ? 4 : SMP_WF_MARCH_MIN_BLOCKS)
 wf_march_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveParams W, int it) {
     extern __shared__ __align__(16) float4 smem_tab[];
     const int lane = threadIdx.x & 31, cur = it & 1, nxt = cur ^ 1;
     const unsigned n = W.cnt[cur];
     if (n == 0u) return;
-    const float4 *tab = P.field.btab;
-    if (FK <= FK_BESSEL2 && P.field.btab != nullptr) {
-        // on a staging timeout (recorded in the counters) the block reads the table from global memory
-        if (stage_to_shared(smem_tab, P.field.btab, unsigned(P.field.bnodes) * 16u, P.counters + CNT_STAGE_TIMEOUT))
-            tab = smem_tab;
+    if (FK <= FK_BESSEL2) {
+        if (!stage_to_shared(smem_tab, P.field.btab, unsigned(P.field.bnodes) * 16u, P.counters + CNT_STAGE_TIMEOUT)) {
+            // timed out (recorded in the counters): copy with plain loads; a late bulk copy
+            // writes the same bytes
+            for (int i = threadIdx.x; i < P.field.bnodes; i += blockDim.x) smem_tab[i] = P.field.btab[i];
+            __syncthreads();
+        }
     }
     const unsigned lanes = gridDim.x * blockDim.x;
     const int chunk = W.chunk * int(min(64u, max(1u, lanes / n)));
@@ -153,12 +159,26 @@ wf_march_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
         if (valid) {
             slot = W.list[cur][i];
             MarchState M;
-            wf_load_march(W, P, slot, M);
-            M.tab = tab;
+            const float4 a = W.ma[slot], b = W.mb[slot], c = W.mc[slot], d = W.mdd[slot];
+            const int4 e = W.mi[slot];
+            M.mp = f3(a.x, a.y, a.z); M.mn = a.w;
+            M.md = f3(b.x, b.y, b.z); M.cur = b.w;
+            M.mg = f3(c.x, c.y, c.z); M.dist_acc = c.w;
+            M.dlimit = d.x; M.s = d.y; M.mtotf = d.z;
+            M.steps = e.x; M.end = 0; M.prec = e.z; M.stop = e.w;   // a marching slot has no end code
+            M.hh = 0.5f * M.cur;
+            M.cur_d = double(M.cur);
+            M.mtot = F64 ? W.mt[slot] : 0.0;
+            M.tab = smem_tab;
             for (int k = 0; k < chunk; k += 2) {
-                if (march_step<FK>(M, P) || march_step<FK>(M, P)) { ended = true; break; }
+                if (march_step<FK, F64>(M, P) || march_step<FK, F64>(M, P)) { ended = true; break; }
             }
-            wf_store_march(W, P, slot, M);
+            W.ma[slot] = make_float4(M.mp.x, M.mp.y, M.mp.z, M.mn);
+            W.mb[slot] = make_float4(M.md.x, M.md.y, M.md.z, M.cur);
+            W.mc[slot] = make_float4(M.mg.x, M.mg.y, M.mg.z, M.dist_acc);
+            if (F64) W.mt[slot] = M.mtot;
+            else W.mdd[slot] = make_float4(M.dlimit, M.s, M.mtotf, 0.0f);
+            W.mi[slot] = make_int4(M.steps, M.end, M.prec, M.stop);
         }
         const unsigned em = __ballot_sync(kFull, valid && ended);
         const unsigned cm = __ballot_sync(kFull, valid && !ended);
