@@ -173,7 +173,11 @@ typedef struct smp_stats {
     int64_t step_cap_hits;        /* photons stopped by step_cap                                    */
     int64_t nan_photons;          /* photons stopped by a non-finite state                          */
     int64_t stream_exhausted;     /* photons whose injected stream ran out                          */
-    double  kernel_ms;            /* device time of the march kernel(s)                             */
+    double  kernel_ms;            /* device time of the trace(s): every kernel, first to last       */
+    double  march_ms;             /* device time inside the ER-march kernel alone                   */
+    int64_t march_steps;          /* er_step evaluations executed by that kernel                    */
+    int64_t launches;             /* kernels launched                                               */
+    int64_t march_launches;       /* of which ER-march kernel launches                              */
 } smp_stats;
 
 /* ---- parity records (smp_trace_photons) ---------------------------------------------------- */

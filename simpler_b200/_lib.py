@@ -107,7 +107,8 @@ class Stats(C.Structure):
     _fields_ = [
         ("photons", C.c_int64), ("er_steps", C.c_int64), ("splats", C.c_int64),
         ("step_cap_hits", C.c_int64), ("nan_photons", C.c_int64), ("stream_exhausted", C.c_int64),
-        ("kernel_ms", C.c_double),
+        ("kernel_ms", C.c_double), ("march_ms", C.c_double), ("march_steps", C.c_int64),
+        ("launches", C.c_int64), ("march_launches", C.c_int64),
     ]
 
 

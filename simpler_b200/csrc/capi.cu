@@ -397,6 +397,9 @@ struct smp_plan {
     int grid_march = 0, grid_event = 0, grid_finish = 0;
     unsigned *h_live = nullptr; // pinned
     cudaEvent_t live_ev = nullptr;
+    std::vector<cudaEvent_t> march_ev;   // event pairs around march-kernel launches (a reused pool)
+    size_t march_ev_used = 0;            // since the last clear
+    long long n_launched = 0;            // kernels launched since the last clear
 };
 
 static void drop_launch_events(smp_plan *p) {
@@ -418,6 +421,7 @@ static void plan_free(smp_plan *p) {
     cudaFree(p->d_wave);
     if (p->h_live) cudaFreeHost(p->h_live);
     if (p->live_ev) cudaEventDestroy(p->live_ev);
+    for (cudaEvent_t e : p->march_ev) cudaEventDestroy(e);
     drop_launch_events(p);
     delete p;
 }
@@ -639,6 +643,8 @@ int smp_plan_clear(smp_plan *plan, void *stream) {
     SMP_CUDA(cudaMemsetAsync(plan->d_counters, 0, CNT_COUNT * sizeof(unsigned long long), s));
     SMP_CUDA(cudaStreamSynchronize(s));
     drop_launch_events(plan);
+    plan->march_ev_used = 0;
+    plan->n_launched = 0;
     std::memset(&plan->stats, 0, sizeof(plan->stats));
     return SMP_OK;
 }
@@ -718,16 +724,26 @@ static int wave_run(smp_plan *p, const KParams &k, cudaStream_t s) {
     SMP_CUDA(cudaMemsetAsync(W.cnt, 0, 4 * sizeof(unsigned), s));
     fe<<<p->grid_event, kBlock, 0, s>>>(k, W, -1);
     SMP_CUDA(cudaGetLastError());
+    p->n_launched += 1;
     // every live photon advances at least one ER step per march launch, and no photon takes more
     // than step_cap steps, so the loop ends; the cap below only guards the host against a defect
     const long long max_iter = (long long)k.step_cap * 4 + (1LL << 20);
     long long it = 0;
     bool pending = false;
     for (;;) {
+        while (p->march_ev.size() < p->march_ev_used + 2 * size_t(p->wave_batch)) {
+            cudaEvent_t e;
+            SMP_CUDA(cudaEventCreate(&e));
+            p->march_ev.push_back(e);
+        }
         for (int j = 0; j < p->wave_batch; ++j, ++it) {
+            SMP_CUDA(cudaEventRecord(p->march_ev[p->march_ev_used], s));
             fm<<<p->grid_march, kBlock, p->smem_bytes, s>>>(k, W, int(it & 0x3fffffff));
+            SMP_CUDA(cudaEventRecord(p->march_ev[p->march_ev_used + 1], s));
+            p->march_ev_used += 2;
             fe<<<p->grid_event, kBlock, 0, s>>>(k, W, int(it & 0x3fffffff));
         }
+        p->n_launched += 2 * p->wave_batch;
         SMP_CUDA(cudaGetLastError());
         if (pending) {                              // the previous batch's count
             SMP_CUDA(cudaEventSynchronize(p->live_ev));
@@ -738,6 +754,7 @@ static int wave_run(smp_plan *p, const KParams &k, cudaStream_t s) {
             if (live <= finish_at && live < unsigned(W.n_slots)) {
                 ff<<<p->grid_finish, kBlock, p->smem_bytes, s>>>(k, W, int(it & 0x3fffffff));
                 SMP_CUDA(cudaGetLastError());
+                p->n_launched += 1;
                 break;
             }
         }
@@ -774,6 +791,7 @@ static int launch(smp_plan *plan, int64_t first, int64_t n, int64_t weight_photo
     if (plan->persistent) {
         march_fn(plan->fk)<<<plan->grid, kBlock, plan->smem_bytes, s>>>(k);
         SMP_CUDA(cudaGetLastError());
+        plan->n_launched += 1;
     } else {
         int rc = wave_run(plan, k, s);
         if (rc) return rc;
@@ -801,6 +819,16 @@ static int collect_stats(smp_plan *plan) {
     plan->stats.nan_photons = (int64_t)c[CNT_NAN];
     plan->stats.stream_exhausted = (int64_t)c[CNT_STREAM];
     plan->stats.kernel_ms = ms_total;
+    double march_ms = 0.0;
+    for (size_t i = 0; i + 1 < plan->march_ev_used; i += 2) {
+        float ms = 0.0f;
+        SMP_CUDA(cudaEventElapsedTime(&ms, plan->march_ev[i], plan->march_ev[i + 1]));
+        march_ms += ms;
+    }
+    plan->stats.march_ms = plan->persistent ? ms_total : march_ms;
+    plan->stats.march_steps = plan->persistent ? (int64_t)c[CNT_STEPS] : (int64_t)c[CNT_MARCH_STEPS];
+    plan->stats.launches = plan->n_launched;
+    plan->stats.march_launches = plan->persistent ? plan->n_launched : (int64_t)(plan->march_ev_used / 2);
     if (c[CNT_STAGE_TIMEOUT]) return set_error(SMP_ERR_CUDA, "%llu block(s) timed out staging the field table", c[CNT_STAGE_TIMEOUT]);
     if (c[CNT_LOST]) return set_error(SMP_ERR_CUDA, "internal: %llu live slot(s) had no lane in the tail kernel", c[CNT_LOST]);
     if (c[CNT_STEP_CAP]) return set_error(SMP_ERR_STEP_CAP, "%llu photon(s) hit the per-photon step cap", c[CNT_STEP_CAP]);
@@ -1236,6 +1264,9 @@ extern "C" int smp_render_noalloc(const smp_scene_desc *scene, const smp_medium_
         stats_out->splats = (int64_t)c[CNT_SPLATS];
         stats_out->step_cap_hits = (int64_t)c[CNT_STEP_CAP];
         stats_out->nan_photons = (int64_t)c[CNT_NAN];
+        stats_out->march_steps = (int64_t)c[CNT_STEPS];
+        stats_out->launches = n_photons > 0 ? 1 : 0;
+        stats_out->march_launches = stats_out->launches;
     }
     if (c[CNT_STAGE_TIMEOUT]) return set_error(SMP_ERR_CUDA, "%llu block(s) timed out staging the field table", c[CNT_STAGE_TIMEOUT]);
     if (c[CNT_STEP_CAP]) return set_error(SMP_ERR_STEP_CAP, "%llu photon(s) hit the per-photon step cap", c[CNT_STEP_CAP]);

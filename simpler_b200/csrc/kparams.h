@@ -114,7 +114,8 @@ enum Counter : int {
     CNT_PHOTONS = 6,
     CNT_STAGE_TIMEOUT = 7,   // a block gave up waiting for its shared-memory staging copy
     CNT_LOST = 8,            // live slots the tail kernel had no lane for (a host defect)
-    CNT_COUNT = 9
+    CNT_MARCH_STEPS = 9,     // ER steps executed by the march kernel of the two-kernel path
+    CNT_COUNT = 10
 };
 
 }  // namespace smp

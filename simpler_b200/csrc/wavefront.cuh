@@ -151,6 +151,7 @@ wf_march_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
     const unsigned lanes = gridDim.x * blockDim.x;
     const int chunk = W.chunk * int(min(64u, max(1u, lanes / n)));
     const unsigned nwarps = lanes >> 5;
+    unsigned done = 0;                               // ER steps this lane executed
     for (unsigned base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; base < n; base += nwarps * 32u) {
         const unsigned i = base + unsigned(lane);
         const bool valid = i < n;
@@ -170,9 +171,11 @@ wf_march_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
             M.cur_d = double(M.cur);
             M.mtot = F64 ? W.mt[slot] : 0.0;
             M.tab = smem_tab;
+            const int steps0 = M.steps;
             for (int k = 0; k < chunk; k += 2) {
                 if (march_step<FK, F64>(M, P) || march_step<FK, F64>(M, P)) { ended = true; break; }
             }
+            done += unsigned(M.steps - steps0);
             W.ma[slot] = make_float4(M.mp.x, M.mp.y, M.mp.z, M.mn);
             W.mb[slot] = make_float4(M.md.x, M.md.y, M.md.z, M.cur);
             W.mc[slot] = make_float4(M.mg.x, M.mg.y, M.mg.z, M.dist_acc);
@@ -185,6 +188,10 @@ wf_march_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
         warp_append(W.queue[cur], W.cnt + 2 + cur, em, slot, lane);
         warp_append(W.list[nxt], W.cnt + nxt, cm, slot, lane);
     }
+    unsigned long long wd = done;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wd += __shfl_down_sync(kFull, wd, o);
+    if (lane == 0 && wd) atomicAdd(P.counters + CNT_MARCH_STEPS, wd);
 }
 
 // Event launch `it` (or the initial fill when it < 0): queued slots run their discrete logic;
