@@ -250,7 +250,7 @@ def run_ours(args):
         achieved = fps * march_steps / (march_ms / 1e3) / 1e12
         roof = {"bound": "fp32", "kernel": "wf_march_kernel<FK_BESSEL1, fp64 path length>",
                 "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-                "frac": achieved / peak.value, "traffic": _profile_traffic(march_steps / n_march),
+                "frac": achieved / peak.value, "traffic": _profile_traffic(),
                 "flop_per_er_step": fps, "er_steps_per_launch": march_steps / n_march,
                 "march_kernel_share_of_step_time": march_ms / ms,
                 "peak_source": "FP32 FMA throughput measured live on this GPU (smp_fp32_peak)"}
@@ -271,16 +271,15 @@ def run_ours(args):
         print(json.dumps(out), flush=True)
 
 
-def _profile_traffic(steps_per_launch: float):
-    """DRAM bytes per march-kernel launch: the committed ncu capture's bytes per ER step (the
-    launch's state loads and stores and any film traffic scale with the steps it executes) times
-    this run's ER steps per launch."""
+def _profile_traffic():
+    """DRAM bytes of one steady-state march-kernel launch (every slot of the pool live, the bench's
+    slot count and chunk), from the committed ncu capture."""
     path = os.path.join(ROOT, "profiles", "wf_march_kernel_precision_traffic.txt")
     try:
         with open(path) as f:
             for line in f:
-                if line.startswith("dram_bytes_per_er_step"):
-                    return float(line.split("=")[1]) * steps_per_launch
+                if line.startswith("dram_bytes_per_launch"):
+                    return float(line.split("=")[1])
     except OSError:
         pass
     return None

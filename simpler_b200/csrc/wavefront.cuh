@@ -39,8 +39,8 @@ struct MarchState {
     const float4 *tab;
 };
 
-// the rest of a Lane, stored per slot as one record
-struct EventPart {
+// the rest of a Lane, stored per slot as one 128-byte record moved with 16-byte accesses
+struct __align__(16) EventPart {
     long long idx;
     double total;
     long long spos, send;
@@ -51,6 +51,20 @@ struct EventPart {
     int rhave, ctx, first;
     float large, d2s, rem, sampled;
 };
+static_assert(sizeof(EventPart) % 16 == 0, "EventPart is moved as float4s");
+
+__device__ __forceinline__ void ev_load(const EventPart *src, EventPart &E) {
+    const float4 *s = reinterpret_cast<const float4 *>(src);
+    float4 *d = reinterpret_cast<float4 *>(&E);
+#pragma unroll
+    for (int i = 0; i < int(sizeof(EventPart) / 16); ++i) d[i] = s[i];
+}
+__device__ __forceinline__ void ev_store(EventPart *dst, const EventPart &E) {
+    float4 *d = reinterpret_cast<float4 *>(dst);
+    const float4 *s = reinterpret_cast<const float4 *>(&E);
+#pragma unroll
+    for (int i = 0; i < int(sizeof(EventPart) / 16); ++i) d[i] = s[i];
+}
 
 struct WaveParams {
     // march state, structure of arrays
@@ -98,7 +112,8 @@ __device__ __forceinline__ void wf_load_lane(const WaveParams &W, const KParams 
     L.dlimit = M.dlimit; L.s = M.s; L.mtotf = M.mtotf; L.mtot = M.mtot;
     L.steps = M.steps; L.end = M.end; L.prec = M.prec; L.stop = M.stop;
     L.hh = M.hh; L.cur_d = M.cur_d;
-    const EventPart &E = W.ev[slot];
+    EventPart E;
+    ev_load(W.ev + slot, E);
     L.idx = E.idx; L.total = E.total; L.spos = E.spos; L.send = E.send;
     L.pos = E.pos; L.dir = E.dir; L.totalDist = E.totalDist;
     L.depth = E.depth; L.nspl = E.nspl; L.draws = E.draws;
@@ -116,7 +131,7 @@ __device__ __forceinline__ void wf_store_lane(const WaveParams &W, const KParams
     E.r0 = L.r0; E.r1 = L.r1; E.r2 = L.r2; E.r3 = L.r3; E.rblk = L.rblk; E.rhave = L.rhave;
     E.ctx = L.ctx; E.first = L.first;
     E.large = L.large; E.d2s = L.d2s; E.rem = L.rem; E.sampled = L.sampled;
-    W.ev[slot] = E;
+    ev_store(W.ev + slot, E);
 }
 
 // Appends `v` of every lane in `mask` to arr[], one atomic per warp. All 32 lanes call it.
