@@ -45,8 +45,12 @@ class Renderer:
         o.device = self.device
         o.seed = self.seed
         st = L.Stats()
-        film = np.zeros_like(img.pixels)
+        film = img.pixels
+        if not (film.flags.c_contiguous and film.dtype == np.float64):
+            film = np.ascontiguousarray(film, dtype=np.float64)
+        # written in place (the library overwrites every pixel); ctypes releases the GIL meanwhile
         L.check(lib.smp_render(C.byref(s), C.byref(m), C.byref(scene.field_desc), C.byref(o), int(numPhotons),
                                C.c_void_p(film.ctypes.data), C.byref(st)))
-        img.pixels[...] = film
+        if film is not img.pixels:
+            img.pixels[...] = film
         self.last_stats = st
