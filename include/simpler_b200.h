@@ -299,7 +299,7 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
    double for SMP_PREC_MIXED, Image3 layout, accumulated -- zero it first for a fresh render) on
    'stream', and returns after the trace has finished. It allocates nothing: the work counter,
    statistics, Bessel table and texture CDF live in a fixed 1 MiB device array that every GPU
-   loading this library holds until the process exits. Limits: textures up to 253823 texels;
+   loading this library holds until the process exits. Limits: texture CDF + Bessel table within the 1 MiB (a 501x501 texture fits);
    Bessel fields of order 0-2 and plane-wave fields; larger inputs are rejected with
    SMP_ERR_BAD_ARG / SMP_ERR_UNSUPPORTED. All calls on a device share that array and each call
    overwrites what the last one left there; calls whose GPU work overlaps race on it. The first

@@ -132,25 +132,41 @@ static float spline_offsets(const smp_field_desc &f, std::vector<float> &delta) 
     return base;
 }
 
-// Bessel table for the march: nodes x_i = i*h, entries (J_m, J_m', J_m+1, J_m+1') in double from
-// libstdc++'s std::cyl_bessel_j, rounded to float; J_n' = (J_{n-1} - J_{n+1})/2, J_{-1} = -J_1.
+// Bessel table for the march: intervals of width h = 1/16 in x = k r up to x_max (<= 128). For
+// each interval, the cubic Hermite interpolant of J_m and of J_m+1 from their values and
+// derivatives at both ends (libstdc++'s std::cyl_bessel_j in double; J_n' = (J_{n-1} - J_{n+1})/2,
+// J_{-1} = -J_1), written in powers of f = x/h - i and rounded to float:
+//   p(f) = J_0 + h J_0' f + (3 (J_1 - J_0) - h (2 J_0' + J_1')) f^2 + (2 (J_0 - J_1) + h (J_0' + J_1')) f^3
 static const double kBesselH = 1.0 / 16.0;
 static const double kBesselMaxX = 128.0;
-static void bessel_table(int m, double x_max, std::vector<float4> &tab) {
+static int bessel_intervals(double x_max) {
     x_max = std::min(std::max(x_max, 1.0), kBesselMaxX);
-    const int nodes = int(std::ceil(x_max / kBesselH)) + 2;
-    tab.resize(nodes);
+    return int(std::ceil(x_max / kBesselH)) + 1;
+}
+static void bessel_table_fill(int m, int intervals, float4 *tab) {
     auto J = [](int n, double x) -> double {
         if (n < 0) return (n % 2 ? -1.0 : 1.0) * std::cyl_bessel_j(double(-n), x);
         return std::cyl_bessel_j(double(n), x);
     };
-    for (int i = 0; i < nodes; ++i) {
-        double x = i * kBesselH;
-        double jm = J(m, x), jm1 = J(m + 1, x);
-        double djm = 0.5 * (J(m - 1, x) - jm1);
-        double djm1 = 0.5 * (jm - J(m + 2, x));
-        tab[i] = make_float4(float(jm), float(djm), float(jm1), float(djm1));
+    auto cubic = [](double j0, double d0, double j1, double d1, double h) {
+        return make_float4(float(j0), float(h * d0), float(3.0 * (j1 - j0) - h * (2.0 * d0 + d1)),
+                           float(2.0 * (j0 - j1) + h * (d0 + d1)));
+    };
+    double a0 = J(m, 0.0), a1 = J(m + 1, 0.0);
+    double da0 = 0.5 * (J(m - 1, 0.0) - a1), da1 = 0.5 * (a0 - J(m + 2, 0.0));
+    for (int i = 0; i < intervals; ++i) {
+        const double x = (i + 1) * kBesselH;
+        const double b0 = J(m, x), b1 = J(m + 1, x);
+        const double db0 = 0.5 * (J(m - 1, x) - b1), db1 = 0.5 * (b0 - J(m + 2, x));
+        tab[2 * i] = cubic(a0, da0, b0, db0, kBesselH);
+        tab[2 * i + 1] = cubic(a1, da1, b1, db1, kBesselH);
+        a0 = b0; a1 = b1; da0 = db0; da1 = db1;
     }
+}
+static void bessel_table(int m, double x_max, std::vector<float4> &tab) {
+    const int intervals = bessel_intervals(x_max);
+    tab.resize(2 * size_t(intervals));
+    bessel_table_fill(m, intervals, tab.data());
 }
 
 // largest k*r the march can meet: the box's extent about the -x axis
@@ -388,7 +404,7 @@ struct smp_plan {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> launches;   // since the last clear
     // the slot pool of the two-kernel march (wavefront.cuh); allocated at the first trace
     bool persistent = false;    // SMP_KERNEL=persistent: the single-kernel march of march.cuh instead
-    int wave_chunk = 64;
+    int wave_chunk = 128;
     int wave_slots_per_lane = 4;
     int wave_batch = 16;        // march/event launch pairs between live-slot checks
     void *d_wave = nullptr;
@@ -474,6 +490,7 @@ static int plan_setup_field(smp_plan *p, const smp_field_desc &f) {
         SMP_CUDA(cudaMemcpy(p->d_btab, tab.data(), tab.size() * sizeof(float4), cudaMemcpyHostToDevice));
         p->kp.field.btab = p->d_btab;
         p->kp.field.bnodes = int(tab.size());
+        p->kp.field.bint = int(tab.size() / 2);
         p->smem_bytes = tab.size() * sizeof(float4);
     }
     set_step_sizes(p->kp, f);
@@ -998,6 +1015,7 @@ int smp_field_eval(const smp_field_desc *field, double scaling, int64_t n_points
         if (e == cudaSuccess) e = cudaMemcpy(d_tab, tab.data(), tab.size() * sizeof(float4), cudaMemcpyHostToDevice);
         F.btab = d_tab;
         F.bnodes = int(tab.size());
+        F.bint = int(tab.size() / 2);
     }
     size_t np = size_t(n_points);
     if (e == cudaSuccess) e = cudaMalloc(&d_pts, np * 3 * sizeof(double));
@@ -1087,7 +1105,9 @@ int smp_render_batch(const smp_scene_desc *, const smp_instance_desc *, int32_t,
 // in the fixed device array below, and host staging uses fixed static buffers.
 //
 // Limits: 1 MiB of device scratch per GPU that loads this library (held until the process exits);
-// textures up to 253823 texels; Bessel fields (orders 0-2) and plane-wave fields only.
+// the texture CDF and the Bessel table share the scratch: 4 (texels + 1) + 32 x (table intervals)
+// <= 1 MiB - 256 bytes (a 501 x 501 texture fits beside any table for k r up to 98; at most 262079
+// texels); Bessel fields (orders 0-2) and plane-wave fields only.
 // Every call on a device shares the scratch and overwrites what the previous call left there (the
 // call clears the counters itself); calls whose GPU work overlaps -- on two streams, or from two
 // host threads -- race on it. The first call on each device looks up the array's device address
@@ -1098,15 +1118,15 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[SMP_NOALLOC_SCR
 
 namespace {
 const size_t kNoAllocCountersBytes = 256;
-const int kNoAllocTabNodes = 2064;                                   // >= ceil(128 * 16) + 2
-const size_t kNoAllocTabBytes = size_t(kNoAllocTabNodes) * sizeof(float4);
-const size_t kNoAllocCdfFloats = (SMP_NOALLOC_SCRATCH_BYTES - kNoAllocCountersBytes - kNoAllocTabBytes) / sizeof(float);
+const size_t kNoAllocShared = SMP_NOALLOC_SCRATCH_BYTES - kNoAllocCountersBytes;   // table, then CDF
+const int kNoAllocTabMax = 2 * 2049;                                 // float4 entries for k r <= 128
+const size_t kNoAllocCdfFloats = kNoAllocShared / sizeof(float);
 const int kNoAllocMaxDevices = 64;
 
 unsigned char *g_noalloc_dev[kNoAllocMaxDevices];                  // device address per device
 std::mutex g_noalloc_mutex;                                          // guards the host staging below
 float g_noalloc_cdf_host[kNoAllocCdfFloats];
-float4 g_noalloc_tab_host[kNoAllocTabNodes];
+float4 g_noalloc_tab_host[kNoAllocTabMax];
 }  // namespace
 
 // The array's device address on the current device, looked up once per device.
@@ -1137,9 +1157,15 @@ extern "C" int smp_render_noalloc(const smp_scene_desc *scene, const smp_medium_
     if (!(fk <= FK_BESSEL2 || fk == FK_PLANEWAVE))
         return set_error(SMP_ERR_UNSUPPORTED, "smp_render_noalloc renders Bessel (orders 0-2) and plane-wave fields");
     const long long n_tex = (long long)scene->tex_x * scene->tex_y;
-    if (size_t(n_tex) + 1 > kNoAllocCdfFloats)
-        return set_error(SMP_ERR_BAD_ARG, "texture has %lld texels; smp_render_noalloc holds at most %zu",
-                         n_tex, kNoAllocCdfFloats - 1);
+    int tab_entries = 0;
+    if (fk <= FK_BESSEL2) {
+        const float k_r = (2.0f * 3.14159265358979f) / (float(field->speed_u) / float(field->f_u));
+        tab_entries = 2 * bessel_intervals(box_max_kr(*scene, k_r));
+    }
+    const size_t tab_bytes = size_t(tab_entries) * sizeof(float4);
+    if (tab_bytes + (size_t(n_tex) + 1) * sizeof(float) > kNoAllocShared)
+        return set_error(SMP_ERR_BAD_ARG, "texture has %lld texels; beside this field's Bessel table "
+                         "smp_render_noalloc holds at most %zu", n_tex, (kNoAllocShared - tab_bytes) / sizeof(float) - 1);
     rc = check_device(opts->device);
     if (rc) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1150,7 +1176,7 @@ extern "C" int smp_render_noalloc(const smp_scene_desc *scene, const smp_medium_
     if (rc) return rc;
     unsigned long long *d_counters = reinterpret_cast<unsigned long long *>(scratch);
     float4 *d_tab = reinterpret_cast<float4 *>(scratch + kNoAllocCountersBytes);
-    float *d_cdf = reinterpret_cast<float *>(scratch + kNoAllocCountersBytes + kNoAllocTabBytes);
+    float *d_cdf = reinterpret_cast<float *>(scratch + kNoAllocCountersBytes + tab_bytes);
 
     KParams k;
     std::memset(&k, 0, sizeof(k));
@@ -1228,23 +1254,12 @@ extern "C" int smp_render_noalloc(const smp_scene_desc *scene, const smp_medium_
     SMP_CUDA(cudaMemcpyAsync(d_cdf, cdf, size_t(n_tex + 1) * sizeof(float), cudaMemcpyHostToDevice, s));
     size_t smem = 0;
     if (fk <= FK_BESSEL2) {
-        double x_max = std::min(std::max(box_max_kr(*scene, k.field.k_r), 1.0), kBesselMaxX);
-        int nodes = int(std::ceil(x_max / kBesselH)) + 2;
-        for (int i = 0; i < nodes; ++i) {
-            double x = i * kBesselH;
-            int m = field->mode;
-            auto J = [](int n, double xx) -> double {
-                if (n < 0) return (n % 2 ? -1.0 : 1.0) * std::cyl_bessel_j(double(-n), xx);
-                return std::cyl_bessel_j(double(n), xx);
-            };
-            double jm = J(m, x), jm1 = J(m + 1, x);
-            g_noalloc_tab_host[i] = make_float4(float(jm), float(0.5 * (J(m - 1, x) - jm1)), float(jm1),
-                                                float(0.5 * (jm - J(m + 2, x))));
-        }
-        SMP_CUDA(cudaMemcpyAsync(d_tab, g_noalloc_tab_host, size_t(nodes) * sizeof(float4), cudaMemcpyHostToDevice, s));
+        bessel_table_fill(field->mode, tab_entries / 2, g_noalloc_tab_host);
+        SMP_CUDA(cudaMemcpyAsync(d_tab, g_noalloc_tab_host, tab_bytes, cudaMemcpyHostToDevice, s));
         k.field.btab = d_tab;
-        k.field.bnodes = nodes;
-        smem = size_t(nodes) * sizeof(float4);
+        k.field.bnodes = tab_entries;
+        k.field.bint = tab_entries / 2;
+        smem = tab_bytes;
     }
     SMP_CUDA(cudaMemsetAsync(d_counters, 0, CNT_COUNT * sizeof(unsigned long long), s));
     int grid = 0;

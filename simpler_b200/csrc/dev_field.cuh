@@ -31,7 +31,7 @@ __device__ __forceinline__ void bessel_field_ng(const FieldParams &F, const floa
     float jm, jm1;
     if (r2 * rs >= kEps) {                     // off the axis (false for r2 = 0: 0 * inf is NaN)
         const float r = r2 * rs;
-        bessel_pair_table_t<M>(tab, F.bnodes, F.bh, F.kb * r, F.k_r * r, jm, jm1);
+        bessel_pair_table_t<M>(tab, F.bint, F.kb * r, F.k_r * r, jm, jm1);
         if (M == 0) {
             // grad = A k J_0'(kr) (0, y, z)/r = -A k J_1(kr) (0, y, z)/r
             n = fmaf(A, jm, F.n_o);
@@ -64,10 +64,10 @@ __device__ __forceinline__ void bessel_field_ng(const FieldParams &F, const floa
         if (M == 1) { cm = c; sm = sn; }
         else { cm = fmaf(c, c, -sn * sn); sm = 2.0f * c * sn; }
     }
-    bessel_pair_table<M>(tab, F.bnodes, F.binv_h, F.bh, F.k_r * r, jm, jm1);
+    bessel_pair_table<M>(tab, F.bint, F.binv_h, F.k_r * r, jm, jm1);
     n = fmaf(A * jm, cm, F.n_o);
     y = kEps; z = kEps; r = kEps; rs = 1.0f / kEps;
-    bessel_pair_table<M>(tab, F.bnodes, F.binv_h, F.bh, F.k_r * kEps, jm, jm1);
+    bessel_pair_table<M>(tab, F.bint, F.binv_h, F.k_r * kEps, jm, jm1);
     // J_m'(kr) = (m/kr) J_m - J_{m+1}, with 1/(kr) = rs/k
     const float djm = (M == 0) ? -jm1 : fmaf(float(M) * F.inv_k * rs, jm, -jm1);
     const float a1 = A * djm * F.k_r * rs * cm;            // radial part / r

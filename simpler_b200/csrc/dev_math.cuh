@@ -9,9 +9,10 @@
 //            degree-6 polynomials in 3/x (|eps| <= 1.6e-8 / 7e-8 / 4e-8 / 9e-8), and the
 //            upward three-term recurrence J_{n+1} = (2n/x) J_n - J_{n-1} for n + 1 <= 3 <= x.
 //   theta_1 is evaluated as theta_0 - pi/2 + (P_1 - P_0), so one sincos serves both orders.
-// The march itself reads (J_m, J_m', J_{m+1}, J_{m+1}') from a per-plan table with cubic
-// Hermite interpolation (bessel_pair_table): branch-free, two 16-byte shared-memory loads and ten
-// FMAs; the formulas above serve arguments beyond the table.
+// The march itself reads J_m and J_{m+1} from a per-plan table (bessel_pair_table): for each
+// interval [i h, (i+1) h) the cubic Hermite interpolant of (J, J') at its two nodes, as power-basis
+// coefficients in f = x/h - i (computed on the host in double); two 16-byte shared-memory loads
+// and six FMAs (Horner); the formulas above serve arguments beyond the table.
 // The reference evaluates J_m with the double-precision libm jn (scene.cpp:214, :238-240);
 // tests bound the absolute error of this code against it.
 #pragma once
@@ -177,50 +178,27 @@ template <int M> __device__ __forceinline__ void bessel_pair(float x, float &jm,
     }
 }
 
-// (J_M, J_{M+1}) from the per-plan cubic Hermite table (nodes every h, entries
-// (J_M, J_M', J_{M+1}, J_{M+1}') computed on the host in double); beyond the table, A&S + recurrence.
+// (J_M, J_{M+1}) at x = t h from the per-plan table: entry 2i = the cubic of J_M on interval i,
+// entry 2i+1 that of J_{M+1} (coefficients of 1, f, f^2, f^3); `intervals` intervals. floor(t) by a
+// round-down add of 2^23, which leaves t - floor(t) exact. Beyond the table, A&S + recurrence.
 template <int M>
-__device__ __forceinline__ void bessel_pair_table(const float4 *tab, int nodes, float inv_h, float h, float x,
-                                                  float &jm, float &jm1) {
-    const float t = x * inv_h;
-    if (t < float(nodes - 1)) {
-        float f;
-        const int i = floor_frac(t, f);
-        const float4 a = tab[i], b = tab[i + 1];
-        const float g = 1.0f - f;
-        const float g2 = g * g, f2 = f * f;
-        const float h00 = fmaf(2.0f, f, 1.0f) * g2;
-        const float h01 = f2 * fmaf(-2.0f, f, 3.0f);
-        const float h10 = f * g2 * h;
-        const float h11 = -f2 * g * h;
-        jm = fmaf(h00, a.x, fmaf(h10, a.y, fmaf(h01, b.x, h11 * b.y)));
-        jm1 = fmaf(h00, a.z, fmaf(h10, a.w, fmaf(h01, b.z, h11 * b.w)));
+__device__ __forceinline__ void bessel_pair_table_t(const float4 *tab, int intervals, float t, float x,
+                                                    float &jm, float &jm1) {
+    if (t < float(intervals)) {
+        const float tb = __fadd_rd(t, 8388608.0f);
+        const int i = __float_as_int(tb) - 0x4B000000;
+        const float f = t - (tb - 8388608.0f);
+        const float4 a = tab[2 * i], b = tab[2 * i + 1];
+        jm = fmaf(fmaf(fmaf(a.w, f, a.z), f, a.y), f, a.x);
+        jm1 = fmaf(fmaf(fmaf(b.w, f, b.z), f, b.y), f, b.x);
     } else {
         bessel_pair<M>(x, jm, jm1);
     }
 }
-
-// The same lookup from t = x / h (x passed for arguments beyond the table): floor(t) by a
-// round-down add of 2^23, which leaves t - floor(t) exact without a correction step.
 template <int M>
-__device__ __forceinline__ void bessel_pair_table_t(const float4 *tab, int nodes, float h, float t, float x,
-                                                    float &jm, float &jm1) {
-    if (t < float(nodes - 1)) {
-        const float tb = __fadd_rd(t, 8388608.0f);
-        const int i = __float_as_int(tb) - 0x4B000000;
-        const float f = t - (tb - 8388608.0f);
-        const float4 a = tab[i], b = tab[i + 1];
-        const float g = 1.0f - f;
-        const float g2 = g * g, f2 = f * f;
-        const float h00 = fmaf(2.0f, f, 1.0f) * g2;
-        const float h01 = f2 * fmaf(-2.0f, f, 3.0f);
-        const float h10 = f * g2 * h;
-        const float h11 = -f2 * g * h;
-        jm = fmaf(h00, a.x, fmaf(h10, a.y, fmaf(h01, b.x, h11 * b.y)));
-        jm1 = fmaf(h00, a.z, fmaf(h10, a.w, fmaf(h01, b.z, h11 * b.w)));
-    } else {
-        bessel_pair<M>(x, jm, jm1);
-    }
+__device__ __forceinline__ void bessel_pair_table(const float4 *tab, int intervals, float inv_h, float x,
+                                                  float &jm, float &jm1) {
+    bessel_pair_table_t<M>(tab, intervals, x * inv_h, x, jm, jm1);
 }
 
 }  // namespace smp

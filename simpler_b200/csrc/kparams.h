@@ -43,9 +43,10 @@ struct FieldParams {
     float xmin[3], xres[3];
     float spline_base;      // coefficients are stored as offsets from this value
     const float *coeff;
-    // Bessel table: node i at x = i*bh holds (J_m, J_m', J_m+1, J_m+1')(x); bnodes nodes
+    // Bessel table: for interval i of width bh, btab[2i] / btab[2i+1] hold the cubics of J_m /
+    // J_m+1 in f = x/bh - i; bint intervals, bnodes = 2 * bint float4 entries
     const float4 *btab;
-    int bnodes;
+    int bnodes, bint;
     float bh, binv_h;
     float kb;               // k_r / bh: table coordinate per metre of r
     float grad_bound;       // bound on |grad n|_1 anywhere (0: unknown)
