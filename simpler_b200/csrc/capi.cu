@@ -404,8 +404,8 @@ struct smp_plan {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> launches;   // since the last clear
     // the slot pool of the two-kernel march (wavefront.cuh); allocated at the first trace
     bool persistent = false;    // SMP_KERNEL=persistent: the single-kernel march of march.cuh instead
-    int wave_chunk = 128;
-    int wave_slots_per_lane = 4;
+    int wave_chunk = 96;
+    int wave_slots_per_lane = 6;
     int wave_batch = 16;        // march/event launch pairs between live-slot checks
     void *d_wave = nullptr;
     size_t wave_bytes = 0;
