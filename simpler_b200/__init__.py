@@ -6,10 +6,12 @@ if it is missing: there is no CPU fallback.
 """
 from . import _lib
 from ._lib import SmpError, check_layout, load
-from .render import Plan, field_eval, records_to_arrays, render, trace_photons
-from .scene import Setup, bernoulli_texture, config_planewave, config_plain_small, config_precision, disk_texture
+from .render import Plan, field_eval, records_to_arrays, render, render_batch, trace_photons
+from .scene import (Setup, bernoulli_texture, config_batch_sweep, config_planewave, config_plain_small,
+                    config_precision, disk_texture)
 
 __all__ = [
-    "SmpError", "check_layout", "load", "Plan", "field_eval", "records_to_arrays", "render", "trace_photons",
+    "SmpError", "check_layout", "load", "Plan", "field_eval", "records_to_arrays", "render", "render_batch",
+    "trace_photons", "config_batch_sweep",
     "Setup", "bernoulli_texture", "config_planewave", "config_plain_small", "config_precision", "disk_texture",
 ]

@@ -27,6 +27,10 @@ NVCC_FLAGS = [
     "-lineinfo", "-O3", "-std=c++17",
     "-Xcompiler", "-fPIC", "-shared",
     "--expt-relaxed-constexpr",
+    # no automatic a*b+c contraction: every kernel (and the CPU oracle) rounds the same expression
+    # the same way, so the single-kernel and two-kernel paths give identical photons; the hot
+    # arithmetic uses explicit fmaf
+    "-fmad=false",
 ]
 
 CU_SOURCES = ["capi.cu", "host/smp_host.cpp"]

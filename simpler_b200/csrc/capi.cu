@@ -326,6 +326,7 @@ static MarchFn march_fn(int fk) {
         case FK_PLANEWAVE: return march_kernel<FK_PLANEWAVE>;
         case FK_SOURCES: return march_kernel<FK_SOURCES>;
         case FK_SPLINE: return march_kernel<FK_SPLINE>;
+        case FK_BATCH: return march_kernel<FK_BATCH>;
         default: return nullptr;
     }
 }
@@ -341,6 +342,7 @@ static WaveFn wf_march_fn(int fk, bool fp64) {
         case FK_PLANEWAVE: return fp64 ? wf_march_kernel<FK_PLANEWAVE, 1> : wf_march_kernel<FK_PLANEWAVE, 0>;
         case FK_SOURCES: return fp64 ? wf_march_kernel<FK_SOURCES, 1> : wf_march_kernel<FK_SOURCES, 0>;
         case FK_SPLINE: return fp64 ? wf_march_kernel<FK_SPLINE, 1> : wf_march_kernel<FK_SPLINE, 0>;
+        case FK_BATCH: return fp64 ? wf_march_kernel<FK_BATCH, 1> : wf_march_kernel<FK_BATCH, 0>;
         default: return nullptr;
     }
 }
@@ -352,6 +354,7 @@ static WaveFn wf_finish_fn(int fk) {
         case FK_PLANEWAVE: return wf_finish_kernel<FK_PLANEWAVE>;
         case FK_SOURCES: return wf_finish_kernel<FK_SOURCES>;
         case FK_SPLINE: return wf_finish_kernel<FK_SPLINE>;
+        case FK_BATCH: return wf_finish_kernel<FK_BATCH>;
         default: return nullptr;
     }
 }
@@ -363,6 +366,7 @@ static WaveFn wf_event_fn(int fk) {
         case FK_PLANEWAVE: return wf_event_kernel<FK_PLANEWAVE>;
         case FK_SOURCES: return wf_event_kernel<FK_SOURCES>;
         case FK_SPLINE: return wf_event_kernel<FK_SPLINE>;
+        case FK_BATCH: return wf_event_kernel<FK_BATCH>;
         default: return nullptr;
     }
 }
@@ -1089,9 +1093,109 @@ int smp_fp32_peak(int device, double *tflops_out) {
     return SMP_OK;
 }
 
-int smp_render_batch(const smp_scene_desc *, const smp_instance_desc *, int32_t, const smp_render_opts *,
-                     double *, smp_stats *) {
-    return set_error(SMP_ERR_UNSUPPORTED, "smp_render_batch is not built yet");
+// The batched sweep: every instance's photons are one index range of a single photon stream, so
+// the slot pool mixes instances as it refills and the whole sweep has one tail. Each instance's
+// field, medium, weight, seed and film travel with its photons (Inst records); the scene and the
+// film shape are shared. Photon j of instance i draws the Philox stream (seed_i, j), so each
+// instance's film is the one a single-instance render with that seed produces.
+int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *instances, int32_t n_inst,
+                     const smp_render_opts *opts, double *images_out, smp_stats *stats_out) {
+    if (!scene || !instances || !opts || n_inst <= 0) return set_error(SMP_ERR_BAD_ARG, "bad batch arguments");
+    if (opts->rng != SMP_RNG_PHILOX) return set_error(SMP_ERR_UNSUPPORTED, "a batched sweep draws from Philox");
+    std::vector<int> fks(n_inst);
+    long long total = 0;
+    for (int i = 0; i < n_inst; ++i) {
+        int rc = check_descs(scene, &instances[i].medium, &instances[i].field, opts);
+        if (rc) return rc;
+        rc = field_kind(instances[i].field, &fks[i]);
+        if (rc) return rc;
+        if (fks[i] > FK_BESSEL2)
+            return set_error(SMP_ERR_UNSUPPORTED, "instance %d: a batched sweep renders Bessel fields of order 0-2", i);
+        if (instances[i].n_photons < 0) return set_error(SMP_ERR_BAD_ARG, "instance %d: negative photon budget", i);
+        total += instances[i].n_photons;
+    }
+    smp_plan *p = nullptr;
+    int rc = smp_plan_create(scene, &instances[0].medium, &instances[0].field, opts, &p);
+    if (rc) return rc;
+    const size_t px = p->film_elems, bpp = p->kp.fp64 ? 8 : 4;
+    // host side of the per-instance records and tables
+    std::vector<Inst> hi(n_inst);
+    std::vector<long long> first(size_t(n_inst) + 1, 0);
+    std::vector<float4> tabs;
+    std::vector<size_t> tab_off(n_inst);
+    for (int i = 0; i < n_inst; ++i) {
+        const smp_instance_desc &d = instances[i];
+        Inst &I = hi[i];
+        std::memset(&I, 0, sizeof(I));
+        fill_field_params(d.field, fks[i], I.field);
+        std::vector<float4> t;
+        bessel_table(d.field.mode, box_max_kr(*scene, I.field.k_r), t);
+        tab_off[i] = tabs.size();
+        tabs.insert(tabs.end(), t.begin(), t.end());
+        I.field.bnodes = int(t.size());
+        I.field.bint = int(t.size() / 2);
+        I.sigma_t = float(d.medium.sigma_t);                      // medium.h:24-38
+        I.albedo = float(d.medium.albedo);
+        I.mfp = 1.0f / float(d.medium.sigma_t);
+        if (I.sigma_t <= 1.19209290e-07f) { I.sigma_t = 0.0f; I.mfp = 1.0f; I.albedo = 0.0f; }
+        I.g = float(d.medium.g);
+        I.weight = d.n_photons > 0 ? photon_weight(*scene, d.n_photons) : 0.0f;
+        I.large_dist = sensor_march_budget(*opts, I.sigma_t);
+        I.seed = d.seed;
+        first[i + 1] = first[i] + d.n_photons;
+    }
+    Inst *d_insts = nullptr;
+    long long *d_first = nullptr;
+    float4 *d_tabs = nullptr;
+    void *d_films = nullptr;
+    cudaError_t e = cudaMalloc(&d_insts, sizeof(Inst) * size_t(n_inst));
+    if (e == cudaSuccess) e = cudaMalloc(&d_first, sizeof(long long) * size_t(n_inst + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&d_tabs, sizeof(float4) * tabs.size());
+    if (e == cudaSuccess) e = cudaMalloc(&d_films, px * bpp * size_t(n_inst));
+    if (e == cudaSuccess) e = cudaMemset(d_films, 0, px * bpp * size_t(n_inst));
+    if (e == cudaSuccess) {
+        for (int i = 0; i < n_inst; ++i) {
+            hi[i].field.btab = d_tabs + tab_off[i];
+            hi[i].film = static_cast<char *>(d_films) + px * bpp * size_t(i);
+        }
+        e = cudaMemcpy(d_insts, hi.data(), sizeof(Inst) * size_t(n_inst), cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(d_first, first.data(), sizeof(long long) * size_t(n_inst + 1), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_tabs, tabs.data(), sizeof(float4) * tabs.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        rc = set_error(e == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "batch buffers: %s", cudaGetErrorString(e));
+    } else {
+        p->kp.insts = d_insts;
+        p->kp.inst_first = d_first;
+        p->kp.n_inst = n_inst;
+        p->fk = FK_BATCH;
+        p->smem_bytes = 0;
+        rc = grid_for(FK_BATCH, p->device, p->opts.blocks_per_sm, 0, &p->grid);
+        if (!rc) rc = smp_plan_clear(p, nullptr);
+        // the weight argument is unused: each instance carries its own Li T / N
+        if (!rc && total > 0) rc = launch(p, 0, total, 1, nullptr, nullptr, nullptr, nullptr);
+        int rs = rc ? rc : collect_stats(p);
+        if (!rc && images_out) {
+            if (p->kp.fp64) {
+                e = cudaMemcpy(images_out, d_films, px * 8 * size_t(n_inst), cudaMemcpyDeviceToHost);
+            } else {
+                std::vector<float> h(px * size_t(n_inst));
+                e = cudaMemcpy(h.data(), d_films, h.size() * 4, cudaMemcpyDeviceToHost);
+                for (size_t j = 0; j < h.size(); ++j) images_out[j] = double(h[j]);
+            }
+            if (e != cudaSuccess) rc = set_error(SMP_ERR_CUDA, "batch films: %s", cudaGetErrorString(e));
+        }
+        if (stats_out) *stats_out = p->stats;
+        if (!rc) rc = rs;
+    }
+    std::string err = g_last_error;
+    cudaFree(d_insts);
+    cudaFree(d_first);
+    cudaFree(d_tabs);
+    cudaFree(d_films);
+    smp_plan_destroy(p);
+    g_last_error = err;
+    return rc;
 }
 
 }  // extern "C"

@@ -236,6 +236,19 @@ template <> struct Field<FK_BESSEL2> {
     static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) { bessel_field<2>(F, tab, p, s, n, g); }
     static __device__ __forceinline__ void eval_ng(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) { bessel_field_ng<2>(F, tab, p, s, n, g); }
 };
+// batched sweep: the instance's Bessel field, its order chosen per photon
+template <> struct Field<FK_BATCH> {
+    static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) {
+        if (F.mode == 0) bessel_field<0>(F, tab, p, s, n, g);
+        else if (F.mode == 1) bessel_field<1>(F, tab, p, s, n, g);
+        else bessel_field<2>(F, tab, p, s, n, g);
+    }
+    static __device__ __forceinline__ void eval_ng(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) {
+        if (F.mode == 0) bessel_field_ng<0>(F, tab, p, s, n, g);
+        else if (F.mode == 1) bessel_field_ng<1>(F, tab, p, s, n, g);
+        else bessel_field_ng<2>(F, tab, p, s, n, g);
+    }
+};
 template <> struct Field<FK_PLANEWAVE> {
     static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *, float3 p, float s, float &n, float3 &g) { wave_field(F, p, s, n, g); }
     static __device__ __forceinline__ void eval_ng(const FieldParams &F, const float4 *, float3 p, float s, float &n, float3 &g) { wave_field_ng(F, p, s, n, g); }

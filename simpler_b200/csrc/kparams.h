@@ -16,7 +16,8 @@ enum FieldKind : int {
     FK_PLANEWAVE = 4,
     FK_SOURCES = 5,
     FK_SPLINE = 6,
-    FK_COUNT = 7
+    FK_BATCH = 7,           // Bessel modes 0-2 with per-instance parameters (batched sweep)
+    FK_COUNT = 8
 };
 
 struct FieldParams {
@@ -50,6 +51,17 @@ struct FieldParams {
     float bh, binv_h;
     float kb;               // k_r / bh: table coordinate per metre of r
     float grad_bound;       // bound on |grad n|_1 anywhere (0: unknown)
+};
+
+// One instance of a batched sweep: its field, medium, photon weight, film and seed. The scene
+// (box, source, camera, film shape) is shared by all instances.
+struct Inst {
+    FieldParams field;
+    float sigma_t, albedo, mfp, g;
+    float weight;           // Li T / N of this instance
+    float large_dist;       // movePhotonTillSensor budget for this sigma_t
+    void *film;             // this instance's film (X*Y*Z, float or double)
+    unsigned long long seed;
 };
 
 #define SMP_MAX_REFINE 39
@@ -103,6 +115,11 @@ struct KParams {
     smp_photon_record *records;       // trace mode only (indexed by photon - first_photon)
     int event_batch;                  // lanes that must finish a march before the warp runs events
     FieldParams field;
+    // batched sweep (FK_BATCH): photon k of the sweep belongs to instance i with
+    // inst_first[i] <= k < inst_first[i+1] and is that instance's photon k - inst_first[i]
+    const Inst *insts;
+    const long long *inst_first;
+    int n_inst;                       // 0 outside a batched sweep
 };
 
 enum Counter : int {

@@ -60,7 +60,24 @@ struct Lane {
     int prec, ctx, first;
     float large, d2s, rem, sampled;
     const float4 *tab;        // Bessel table in this block's shared memory
+    const Inst *inst;         // batched sweep: the photon's instance
 };
+
+// Per-photon medium, weight, film and seed: the instance's in a batched sweep (n_inst is uniform
+// over the grid, so these are uniform branches), else the plan's.
+__device__ __forceinline__ float med_g(const Lane &L, const KParams &P) { return P.n_inst ? L.inst->g : P.g; }
+__device__ __forceinline__ float med_albedo(const Lane &L, const KParams &P) { return P.n_inst ? L.inst->albedo : P.albedo; }
+__device__ __forceinline__ float med_sigma_t(const Lane &L, const KParams &P) { return P.n_inst ? L.inst->sigma_t : P.sigma_t; }
+__device__ __forceinline__ float med_mfp(const Lane &L, const KParams &P) { return P.n_inst ? L.inst->mfp : P.mfp; }
+__device__ __forceinline__ float med_weight(const Lane &L, const KParams &P) { return P.n_inst ? L.inst->weight : P.weight; }
+__device__ __forceinline__ float med_large(const Lane &L, const KParams &P) { return P.n_inst ? L.inst->large_dist : P.large_dist; }
+__device__ __forceinline__ void *med_film(const Lane &L, const KParams &P) { return P.n_inst ? L.inst->film : P.film; }
+__device__ __forceinline__ unsigned long long med_seed(const Lane &L, const KParams &P) { return P.n_inst ? L.inst->seed : P.seed; }
+// the field the photon marches through
+template <int FK, class S>
+__device__ __forceinline__ const FieldParams &field_of(const S &L, const KParams &P) {
+    return FK == FK_BATCH ? L.inst->field : P.field;
+}
 
 // ---- uniforms -----------------------------------------------------------------------------
 __device__ __forceinline__ void philox_block(unsigned &c0, unsigned &c1, unsigned &c2, unsigned &c3,
@@ -93,7 +110,8 @@ __device__ __forceinline__ float draw(Lane &L, const KParams &P) {
         return 0.5f;
     }
     if (L.rhave == 0) {
-        uint4 b = philox_refill(L.rblk++, unsigned(L.idx), unsigned(L.idx >> 32), unsigned(P.seed), unsigned(P.seed >> 32));
+        const unsigned long long seed = med_seed(L, P);
+        uint4 b = philox_refill(L.rblk++, unsigned(L.idx), unsigned(L.idx >> 32), unsigned(seed), unsigned(seed >> 32));
         L.r0 = b.x; L.r1 = b.y; L.r2 = b.z; L.r3 = b.w;
         L.rhave = 4;
     }
@@ -185,11 +203,11 @@ __device__ __forceinline__ bool propagate_till_sensor(const KParams &P, float3 &
 }
 
 // Scene::addEnergyToImage (scene.cpp:782-829) with bilinear sharing (USE_PIXEL_SHARING)
-__device__ __forceinline__ void add_pixel(const KParams &P, int x, int y, int z, float v) {
+__device__ __forceinline__ void add_pixel(const KParams &P, void *film, int x, int y, int z, float v) {
     if (x >= 0 && x < P.X && y >= 0 && y < P.Y && z >= 0 && z < P.Z) {
         size_t i = (size_t(z) * P.Y + y) * P.X + x;
-        if (P.fp64) atomicAdd(reinterpret_cast<double *>(P.film) + i, double(v));
-        else atomicAdd(reinterpret_cast<float *>(P.film) + i, v);
+        if (P.fp64) atomicAdd(reinterpret_cast<double *>(film) + i, double(v));
+        else atomicAdd(reinterpret_cast<float *>(film) + i, v);
     }
 }
 
@@ -220,22 +238,23 @@ __device__ __forceinline__ void splat(Lane &L, const KParams &P, float3 p, doubl
     else if (P.fp64) iz = int(floor((pl - double(P.pl_min)) / (double(P.pl_max) - double(P.pl_min)) * double(P.Z)));
     else iz = int(floorf(((float(pl) - P.pl_min) / (P.pl_max - P.pl_min)) * float(P.Z)));
     float fx = x - flx, fy = y - fly;
-    add_pixel(P, ix, iy, iz, val * (1.0f - fx) * (1.0f - fy));
-    add_pixel(P, ix + 1, iy, iz, val * fx * (1.0f - fy));
-    add_pixel(P, ix, iy + 1, iz, val * (1.0f - fx) * fy);
-    add_pixel(P, ix + 1, iy + 1, iz, val * fx * fy);
+    void *film = med_film(L, P);
+    add_pixel(P, film, ix, iy, iz, val * (1.0f - fx) * (1.0f - fy));
+    add_pixel(P, film, ix + 1, iy, iz, val * fx * (1.0f - fy));
+    add_pixel(P, film, ix, iy + 1, iz, val * (1.0f - fx) * fy);
+    add_pixel(P, film, ix + 1, iy + 1, iz, val * fx * fy);
 }
 
 // Henyey-Greenstein (phase.cpp:17-21, :40-76; util.h:17-27)
-__device__ __forceinline__ float hg_f(const KParams &P, float3 in, float3 out) {
+__device__ __forceinline__ float hg_f(float g, float3 in, float3 out) {
     float c = dot3(in, out);
-    float b = 1.0f + P.g * P.g - 2.0f * P.g * c;
-    return (1.0f / (4.0f * 3.14159265358979f)) * (1.0f - P.g * P.g) / (b * sqrtf(b));
+    float b = 1.0f + g * g - 2.0f * g * c;
+    return (1.0f / (4.0f * 3.14159265358979f)) * (1.0f - g * g) / (b * sqrtf(b));
 }
 __device__ __forceinline__ float3 hg_sample(Lane &L, const KParams &P, float3 in) {
     float sx = draw(L, P);
     float sy = draw(L, P);
-    float g = P.g, cosT;
+    float g = med_g(L, P), cosT;
     if (fabsf(g) < kEps) cosT = 1.0f - 2.0f * sx;
     else {
         float sq = (1.0f - g * g) / (1.0f - g + 2.0f * g * sx);
@@ -269,7 +288,8 @@ __device__ __forceinline__ float3 random_direction(Lane &L, const KParams &P) {
 }
 
 __device__ __forceinline__ bool roulette(Lane &L, const KParams &P) {
-    return (P.albedo > 0.0f) && ((P.albedo >= 1.0f) || (draw(L, P) < P.albedo));
+    const float albedo = med_albedo(L, P);
+    return (albedo > 0.0f) && ((albedo >= 1.0f) || (draw(L, P) < albedo));
 }
 
 // area_textured_source::sample_ray (scene.cpp:107-137) + DiscreteDistribution::sample (pmf.h:109-121)
@@ -311,7 +331,7 @@ __device__ __forceinline__ bool gen_ray(Lane &L, const KParams &P, float3 &pos, 
 // ---- the traceTillBlock step ----------------------------------------------------------------
 template <int FK>
 __device__ __forceinline__ void begin_march(Lane &L, const KParams &P, float dlimit, bool eval) {
-    if (eval) Field<FK>::eval(P.field, L.tab, L.mp, L.s, L.mn, L.mg);
+    if (eval) Field<FK>::eval(field_of<FK>(L, P), L.tab, L.mp, L.s, L.mn, L.mg);
     L.dist_acc = 0.0f;
     L.dlimit = dlimit;
     L.cur = P.h0;
@@ -341,7 +361,7 @@ __device__ __forceinline__ bool march_step(S &L, const KParams &P) {
     const float3 p = f3(fmaf(d.x, hinv, L.mp.x), fmaf(d.y, hinv, L.mp.y), fmaf(d.z, hinv, L.mp.z));
     float n2;
     float3 g2;
-    Field<FK>::eval(P.field, L.tab, p, L.s, n2, g2);
+    Field<FK>::eval(field_of<FK>(L, P), L.tab, p, L.s, n2, g2);
     const float3 d2 = f3(fmaf(L.hh, g2.x, d.x), fmaf(L.hh, g2.y, d.y), fmaf(L.hh, g2.z, d.z));
     ++L.steps;
     const float sacc = L.dist_acc + L.cur;
@@ -404,9 +424,20 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
                 L.spos = P.offsets[k];
                 L.send = P.offsets[k + 1];
             }
+            if (FK == FK_BATCH) {
+                // sweep photon index -> (instance, the instance's photon index)
+                int lo = 0, hi = P.n_inst;
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (P.inst_first[mid] <= L.idx) lo = mid; else hi = mid;
+                }
+                L.inst = P.insts + lo;
+                L.idx -= P.inst_first[lo];
+                L.tab = L.inst->field.btab;
+            }
             if (!gen_ray(L, P, L.pos, L.dir, L.total)) { L.end = SMP_END_GENRAY_FAIL; ev = EV_FINISH; break; }
             float u = draw(L, P);
-            const FieldParams &F = P.field;
+            const FieldParams &F = field_of<FK>(L, P);
             if (FK == FK_PLANEWAVE) L.s = fmaf(F.phi_range, u, F.phi_min);
             else if (FK == FK_SOURCES) L.s = 0.0f;
             else {
@@ -422,7 +453,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
                 L.md = L.dir;
                 L.mtot = L.total;
                 L.first = 1;
-                L.large = P.large_dist;
+                L.large = med_large(L, P);
                 begin_march<FK>(L, P, L.large, false);
                 if (march_has_steps(L)) return ST_MARCH;
                 ev = EV_MARCH_END;
@@ -473,7 +504,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
                         float dts = 0.0f;
                         if (propagate_till_sensor(P, p1, refr, dts)) {
                             acc_total(L.total, dts, P.fp64);
-                            float val = P.weight * expf(-P.sigma_t * L.d2s) * fw;
+                            float val = med_weight(L, P) * expf(-med_sigma_t(L, P) * L.d2s) * fw;
                             splat(L, P, p1, L.total, 0, val);
                         }
                     }
@@ -496,8 +527,8 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
                         float dts = 0.0f;
                         if (propagate_till_sensor(P, p1, refr, dts)) {
                             acc_total(tot, dts, P.fp64);
-                            float val = P.weight * 6.28318548202514648f * expf(-P.sigma_t * L.d2s) *
-                                        hg_f(P, divs(L.dir, len3(L.dir)), dsen) * fore * fw;
+                            float val = med_weight(L, P) * 6.28318548202514648f * expf(-med_sigma_t(L, P) * L.d2s) *
+                                        hg_f(med_g(L, P), divs(L.dir, len3(L.dir)), dsen) * fore * fw;
                             splat(L, P, p1, tot, L.depth, val);
                         }
                     }
@@ -532,7 +563,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
         }
         case EV_SCATTER: {
             if (!roulette(L, P)) { L.end = SMP_END_NO_SCATTER; ev = EV_FINISH; break; }
-            float dist = -P.mfp * logf(draw(L, P));
+            float dist = -med_mfp(L, P) * logf(draw(L, P));
             L.ctx = CTX_MOVE_FIRST;
             L.sampled = dist;
             L.rem = dist;
@@ -556,7 +587,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
                 L.ctx = CTX_CONNECT;
                 L.mtot = L.total;
                 L.first = 1;
-                L.large = P.large_dist;
+                L.large = med_large(L, P);
                 begin_march<FK>(L, P, L.large, false);
                 if (march_has_steps(L)) return ST_MARCH;
                 ev = EV_MARCH_END;
@@ -570,7 +601,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
             float mag = len3(L.dir);
             float3 d1 = hg_sample(L, P, divs(L.dir, mag));
             L.dir = mul(d1, mag);
-            float dist = -P.mfp * logf(draw(L, P));
+            float dist = -med_mfp(L, P) * logf(draw(L, P));
             L.ctx = CTX_MOVE_VERTEX;
             L.rem = dist;
             L.mp = L.pos;

@@ -37,6 +37,7 @@ struct MarchState {
     double mtot, cur_d;
     int steps, end, prec, stop;
     const float4 *tab;
+    const Inst *inst;          // batched sweep only
 };
 
 // the rest of a Lane, stored per slot as one 128-byte record moved with 16-byte accesses
@@ -50,6 +51,7 @@ struct __align__(16) EventPart {
     unsigned r0, r1, r2, r3, rblk;
     int rhave, ctx, first;
     float large, d2s, rem, sampled;
+    int inst;                  // batched sweep: instance index
 };
 static_assert(sizeof(EventPart) % 16 == 0, "EventPart is moved as float4s");
 
@@ -71,7 +73,7 @@ struct WaveParams {
     float4 *ma;        // mp.xyz, mn
     float4 *mb;        // md.xyz, cur
     float4 *mc;        // mg.xyz, dist_acc
-    float4 *mdd;       // dlimit, s, mtotf, -
+    float4 *mdd;       // dlimit, s, mtotf, instance index (bits; batched sweep)
     int4 *mi;          // steps, end, prec, stop
     double *mt;        // mtot (FP64 path-length form only)
     EventPart *ev;
@@ -90,6 +92,7 @@ __device__ __forceinline__ void wf_load_march(const WaveParams &W, const KParams
     M.mg = f3(c.x, c.y, c.z); M.dist_acc = c.w;
     M.dlimit = d.x; M.s = d.y; M.mtotf = d.z;
     M.steps = e.x; M.end = e.y; M.prec = e.z; M.stop = e.w;
+    M.inst = P.n_inst ? P.insts + __float_as_int(d.w) : nullptr;
     M.hh = 0.5f * M.cur;
     M.cur_d = double(M.cur);
     M.mtot = P.fp64 ? W.mt[slot] : 0.0;
@@ -100,7 +103,7 @@ __device__ __forceinline__ void wf_store_march(const WaveParams &W, const KParam
     W.ma[slot] = make_float4(M.mp.x, M.mp.y, M.mp.z, M.mn);
     W.mb[slot] = make_float4(M.md.x, M.md.y, M.md.z, M.cur);
     W.mc[slot] = make_float4(M.mg.x, M.mg.y, M.mg.z, M.dist_acc);
-    W.mdd[slot] = make_float4(M.dlimit, M.s, M.mtotf, 0.0f);
+    W.mdd[slot] = make_float4(M.dlimit, M.s, M.mtotf, __int_as_float(P.n_inst ? int(M.inst - P.insts) : 0));
     W.mi[slot] = make_int4(M.steps, M.end, M.prec, M.stop);
     if (P.fp64) W.mt[slot] = M.mtot;
 }
@@ -111,7 +114,7 @@ __device__ __forceinline__ void wf_load_lane(const WaveParams &W, const KParams 
     L.mp = M.mp; L.mn = M.mn; L.md = M.md; L.cur = M.cur; L.mg = M.mg; L.dist_acc = M.dist_acc;
     L.dlimit = M.dlimit; L.s = M.s; L.mtotf = M.mtotf; L.mtot = M.mtot;
     L.steps = M.steps; L.end = M.end; L.prec = M.prec; L.stop = M.stop;
-    L.hh = M.hh; L.cur_d = M.cur_d;
+    L.hh = M.hh; L.cur_d = M.cur_d; L.inst = M.inst;
     EventPart E;
     ev_load(W.ev + slot, E);
     L.idx = E.idx; L.total = E.total; L.spos = E.spos; L.send = E.send;
@@ -131,6 +134,7 @@ __device__ __forceinline__ void wf_store_lane(const WaveParams &W, const KParams
     E.r0 = L.r0; E.r1 = L.r1; E.r2 = L.r2; E.r3 = L.r3; E.rblk = L.rblk; E.rhave = L.rhave;
     E.ctx = L.ctx; E.first = L.first;
     E.large = L.large; E.d2s = L.d2s; E.rem = L.rem; E.sampled = L.sampled;
+    E.inst = P.n_inst ? int(L.inst - P.insts) : 0;
     ev_store(W.ev + slot, E);
 }
 
@@ -185,7 +189,12 @@ wf_march_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
             M.hh = 0.5f * M.cur;
             M.cur_d = double(M.cur);
             M.mtot = F64 ? W.mt[slot] : 0.0;
-            M.tab = smem_tab;
+            if (FK == FK_BATCH) {
+                M.inst = P.insts + __float_as_int(d.w);
+                M.tab = M.inst->field.btab;
+            } else {
+                M.tab = smem_tab;
+            }
             const int steps0 = M.steps;
             for (int k = 0; k < chunk; k += 2) {
                 if (march_step<FK, F64>(M, P) || march_step<FK, F64>(M, P)) { ended = true; break; }
@@ -195,7 +204,7 @@ wf_march_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
             W.mb[slot] = make_float4(M.md.x, M.md.y, M.md.z, M.cur);
             W.mc[slot] = make_float4(M.mg.x, M.mg.y, M.mg.z, M.dist_acc);
             if (F64) W.mt[slot] = M.mtot;
-            else W.mdd[slot] = make_float4(M.dlimit, M.s, M.mtotf, 0.0f);
+            else W.mdd[slot] = make_float4(M.dlimit, M.s, M.mtotf, d.w);
             W.mi[slot] = make_int4(M.steps, M.end, M.prec, M.stop);
         }
         const unsigned em = __ballot_sync(kFull, valid && ended);
@@ -239,11 +248,11 @@ wf_event_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
                 st = ST_FETCH;
             } else {
                 wf_load_lane(W, P, slot, L);
-                L.tab = P.field.btab;
+                L.tab = FK == FK_BATCH ? L.inst->field.btab : P.field.btab;
                 st = run_events<FK>(L, P, EV_MARCH_END);
                 if (st == ST_FETCH) finish_photon_stats<FK>(L, S);
             }
-            L.tab = P.field.btab;
+            if (FK != FK_BATCH) L.tab = P.field.btab;         // a batched photon's table is set at its start
             while (st == ST_FETCH) {
                 const unsigned long long k = atomicAdd(P.counters + CNT_NEXT_PHOTON, 1ull);
                 if (k < (unsigned long long)P.n_photons) {
@@ -285,11 +294,12 @@ wf_finish_kernel(const __grid_constant__ KParams P, const __grid_constant__ Wave
     L.end = 0;
     L.idx = 0;
     int st = ST_FETCH;
+    L.inst = nullptr;
     if (gid < n) {
         wf_load_lane(W, P, W.list[cur][gid], L);
         st = ST_MARCH;
     }
-    L.tab = tab;
+    L.tab = (FK == FK_BATCH && L.inst) ? L.inst->field.btab : tab;
     LaneStats S;
     lane_loop<FK>(L, st, P, S, lane);
     flush_stats(S, P, lane);

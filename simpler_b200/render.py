@@ -85,6 +85,35 @@ class Plan:
             pass
 
 
+def render_batch(setup: Setup, instances: list) -> tuple[np.ndarray, L.Stats]:
+    """A sweep of many field / medium configurations over one scene, in one slot pool.
+
+    `instances` is a list of dicts: any Setup field or medium attribute to override
+    (mode, n_max, n_clip, f_u, speed_u, phi_min, phi_max, sigma_t, albedo, g, ...) plus
+    `n_photons` and `seed`. Returns the films as an (n_inst, z, y, x) float64 array and the
+    statistics of the whole sweep. Photon j of instance i draws the stream (seed_i, j), so each
+    film equals a single render of that configuration with that seed."""
+    import dataclasses
+    lib = L.load()
+    n = len(instances)
+    arr = (L.InstanceDesc * n)()
+    keep = []
+    for i, inst in enumerate(instances):
+        over = {k: v for k, v in inst.items() if k not in ("n_photons", "seed")}
+        s = dataclasses.replace(setup, **over)
+        fd = s.field_desc()
+        keep.append(s)
+        arr[i].field = fd
+        arr[i].medium = s.medium_desc()
+        arr[i].n_photons = int(inst["n_photons"])
+        arr[i].seed = int(inst.get("seed", 0))
+    sc, _, _, op = setup.descs()
+    films = np.zeros((n,) + setup.film_shape(), dtype=np.float64)
+    st = L.Stats()
+    L.check(lib.smp_render_batch(C.byref(sc), arr, n, C.byref(op), _ptr(films), C.byref(st)))
+    return films, st
+
+
 def trace_photons(setup: Setup, first: int, n: int, weight_photons: int,
                   uniforms: np.ndarray | None = None, offsets: np.ndarray | None = None,
                   with_image: bool = True):

@@ -237,3 +237,24 @@ def config_planewave(**kw) -> Setup:
     for kk, v in kw.items():
         setattr(s, kk, v)
     return s
+
+
+def config_batch_sweep(n_inst: int = 256, seed: int = 2, scale: float = 1.0, **kw):
+    """The batched sweep: n_inst cylindrical-transducer instances over the plain small scene
+    (medium, optics and 128x128 x 32 film of config_plain_small), with amplitude n_max ~ U[0, 2e-3],
+    frequency ~ U[0.5, 2] MHz, mode in {0, 1, 2}, duty cycle D ~ U[1, 100] % (phase range
+    [0, 2 pi D)) and a photon budget log-uniform in [1e5, 1e7] (times `scale`), all drawn from
+    numpy's default_rng(seed); instance i draws Philox stream seed (seed << 32) + i.
+    Returns (setup, instances) for render_batch."""
+    rng = np.random.default_rng(seed)
+    setup = config_plain_small(**kw)
+    insts = []
+    for i in range(n_inst):
+        n_max = float(rng.uniform(0.0, 2e-3))
+        f_u = float(rng.uniform(0.5e6, 2e6))
+        mode = int(rng.integers(0, 3))
+        duty = float(rng.uniform(0.01, 1.0))
+        n_ph = int(round(10.0 ** rng.uniform(5.0, 7.0) * scale))
+        insts.append({"mode": mode, "n_max": n_max, "n_clip": n_max, "f_u": f_u, "phi_min": 0.0,
+                      "phi_max": 2.0 * math.pi * duty, "n_photons": max(n_ph, 1), "seed": (seed << 32) + i})
+    return setup, insts
