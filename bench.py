@@ -46,6 +46,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--photons-per-step", type=int, default=PHOTONS_PER_STEP)
+    ap.add_argument("--workload", choices=["precision", "sweep"], default="precision",
+                    help="precision: the headline line (default); sweep: the batched 256-instance sweep "
+                         "against the same instances rendered one by one")
+    ap.add_argument("--sweep-scale", type=float, default=1.0,
+                    help="sweep: multiply every instance's photon budget")
     return ap.parse_args()
 
 
@@ -308,10 +313,53 @@ def run_e2e(args, setup, steps: int, per_step: int) -> dict:
             "call": "smp_render (one-shot plan, host film) per step, wall clock"}
 
 
+def run_sweep(args):
+    """The batched sweep (256 cylindrical-transducer instances over the plain small scene, budgets
+    log-uniform 1e5-1e7, seed 2) rendered in one slot pool with smp_render_batch, against the same
+    instances rendered one smp_render call each (the reference's per-configuration loop). Both
+    host-timed end to end (films read back to host memory); one JSON line."""
+    import torch
+    torch.cuda.set_device(0)
+    setup, insts = sb.config_batch_sweep(n_inst=256, seed=2, scale=args.sweep_scale)
+    total = sum(i["n_photons"] for i in insts)
+    sb.render_batch(setup, insts[:4])                    # warm-up: module load, first allocations
+    clocks = ClockSampler(0)
+    clocks.start()
+    t0 = time.perf_counter()
+    films, st = sb.render_batch(setup, insts)
+    t_batch = time.perf_counter() - t0
+    import dataclasses
+    t0 = time.perf_counter()
+    serial_sum = 0.0
+    for i, inst in enumerate(insts):
+        over = {k: v for k, v in inst.items() if k != "n_photons"}
+        img, _ = sb.render(dataclasses.replace(setup, **over), inst["n_photons"])
+        serial_sum += float(img.sum())
+    t_serial = time.perf_counter() - t0
+    clk = clocks.stop()
+    out = {
+        "metric": METRIC, "value": total / t_batch, "unit": METRIC, "n_gpus": 1, "steps": 1, "warmup": 1,
+        "ms_per_step": t_batch * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": "batched sweep: 256 Bessel instances (n_max U[0,2e-3], f U[0.5,2] MHz, mode 0-2, "
+                               "duty U[1,100]%, budgets log-uniform 1e5-1e7 x scale), medium and film of the "
+                               "plain small configuration, seed 2", "photons": total, "scale": args.sweep_scale,
+                   "film": list(setup.film_shape())},
+        "serial": {"value": total / t_serial, "unit": METRIC, "seconds": t_serial,
+                   "call": "one smp_render per instance, host film"},
+        "batch_seconds": t_batch, "speedup_vs_serial": t_serial / t_batch,
+        "film_sum_relative_difference": abs(float(films.sum()) - serial_sum) / max(serial_sum, 1e-300),
+        "er_steps_per_s": st.er_steps / t_batch, "gpu_launches": st.launches, "clocks": clk,
+    }
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "sweep":
+        run_sweep(args)
     else:
         run_ours(args)
 

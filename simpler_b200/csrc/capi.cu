@@ -1121,19 +1121,32 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
     // host side of the per-instance records and tables
     std::vector<Inst> hi(n_inst);
     std::vector<long long> first(size_t(n_inst) + 1, 0);
+    // the tables depend on the order and the largest k r only: one per order, as long as the
+    // largest k r any instance of that order meets
+    double xmax[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < n_inst; ++i) {
+        FieldParams F;
+        fill_field_params(instances[i].field, fks[i], F);
+        xmax[fks[i]] = std::max(xmax[fks[i]], box_max_kr(*scene, F.k_r));
+    }
     std::vector<float4> tabs;
-    std::vector<size_t> tab_off(n_inst);
+    size_t tab_off[3] = {0, 0, 0};
+    int tab_int[3] = {0, 0, 0};
+    for (int m = 0; m < 3; ++m) {
+        if (xmax[m] <= 0.0) continue;
+        std::vector<float4> t;
+        bessel_table(m, xmax[m], t);
+        tab_off[m] = tabs.size();
+        tab_int[m] = int(t.size() / 2);
+        tabs.insert(tabs.end(), t.begin(), t.end());
+    }
     for (int i = 0; i < n_inst; ++i) {
         const smp_instance_desc &d = instances[i];
         Inst &I = hi[i];
         std::memset(&I, 0, sizeof(I));
         fill_field_params(d.field, fks[i], I.field);
-        std::vector<float4> t;
-        bessel_table(d.field.mode, box_max_kr(*scene, I.field.k_r), t);
-        tab_off[i] = tabs.size();
-        tabs.insert(tabs.end(), t.begin(), t.end());
-        I.field.bnodes = int(t.size());
-        I.field.bint = int(t.size() / 2);
+        I.field.bnodes = 2 * tab_int[fks[i]];
+        I.field.bint = tab_int[fks[i]];
         I.sigma_t = float(d.medium.sigma_t);                      // medium.h:24-38
         I.albedo = float(d.medium.albedo);
         I.mfp = 1.0f / float(d.medium.sigma_t);
@@ -1155,7 +1168,7 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
     if (e == cudaSuccess) e = cudaMemset(d_films, 0, px * bpp * size_t(n_inst));
     if (e == cudaSuccess) {
         for (int i = 0; i < n_inst; ++i) {
-            hi[i].field.btab = d_tabs + tab_off[i];
+            hi[i].field.btab = d_tabs + tab_off[fks[i]];
             hi[i].film = static_cast<char *>(d_films) + px * bpp * size_t(i);
         }
         e = cudaMemcpy(d_insts, hi.data(), sizeof(Inst) * size_t(n_inst), cudaMemcpyHostToDevice);
@@ -1179,7 +1192,7 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
             if (p->kp.fp64) {
                 e = cudaMemcpy(images_out, d_films, px * 8 * size_t(n_inst), cudaMemcpyDeviceToHost);
             } else {
-                std::vector<float> h(px * size_t(n_inst));
+                std::vector<float> h(px * size_t(n_inst));           // FP32 films, widened on the host
                 e = cudaMemcpy(h.data(), d_films, h.size() * 4, cudaMemcpyDeviceToHost);
                 for (size_t j = 0; j < h.size(); ++j) images_out[j] = double(h[j]);
             }

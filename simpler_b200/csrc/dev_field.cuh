@@ -236,17 +236,59 @@ template <> struct Field<FK_BESSEL2> {
     static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) { bessel_field<2>(F, tab, p, s, n, g); }
     static __device__ __forceinline__ void eval_ng(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) { bessel_field_ng<2>(F, tab, p, s, n, g); }
 };
-// batched sweep: the instance's Bessel field, its order chosen per photon
+// Bessel mode m in 0..2 chosen at run time, one branch-free path for all orders (lanes of a warp
+// may hold photons of different instances and orders): cos/sin(m phi) by selects from
+// (z + iy)/r, J_m' = (m/kr) J_m - J_{m+1}; beyond the table the order-specific formulas.
+__device__ __forceinline__ void bessel_field_rt(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) {
+    const int M = F.mode;
+    const float A = F.amp * (in_gap(F, p) ? 0.0f : s);
+    float y = p.y, z = p.z;
+    const float r2 = fmaf(y, y, z * z);
+    float rs = rsqrt_fast(r2);                 // +inf at r2 = 0
+    float r = r2 > 0.0f ? r2 * rs : 0.0f;
+    float cm = 1.0f, sm = 0.0f;
+    if (r2 > 0.0f) {
+        const float c = z * rs, sn = y * rs;
+        cm = M == 0 ? 1.0f : (M == 1 ? c : fmaf(c, c, -sn * sn));
+        sm = M == 0 ? 0.0f : (M == 1 ? sn : 2.0f * c * sn);
+    }
+    float jm, jm1;
+    const float t = F.kb * r;
+    if (t < float(F.bint)) {
+        const float tb = __fadd_rd(t, 8388608.0f);
+        const int i = __float_as_int(tb) - 0x4B000000;
+        const float f = t - (tb - 8388608.0f);
+        const float4 a = tab[2 * i], b = tab[2 * i + 1];
+        jm = fmaf(fmaf(fmaf(a.w, f, a.z), f, a.y), f, a.x);
+        jm1 = fmaf(fmaf(fmaf(b.w, f, b.z), f, b.y), f, b.x);
+    } else if (M == 0) {
+        bessel_pair<0>(F.k_r * r, jm, jm1);
+    } else if (M == 1) {
+        bessel_pair<1>(F.k_r * r, jm, jm1);
+    } else {
+        bessel_pair<2>(F.k_r * r, jm, jm1);
+    }
+    n = fmaf(A * jm, cm, F.n_o);
+    if (!(r >= kEps)) {                        // the gradient's near-axis substitution (scene.cpp:229-234)
+        y = kEps; z = kEps; r = kEps; rs = 1.0f / kEps;
+        if (M == 0) bessel_pair_table<0>(tab, F.bint, F.binv_h, F.k_r * kEps, jm, jm1);
+        else if (M == 1) bessel_pair_table<1>(tab, F.bint, F.binv_h, F.k_r * kEps, jm, jm1);
+        else bessel_pair_table<2>(tab, F.bint, F.binv_h, F.k_r * kEps, jm, jm1);
+    }
+    const float fm = float(M);
+    const float djm = fmaf(fm * F.inv_k * rs, jm, -jm1);
+    const float a1 = A * djm * F.k_r * rs * cm;
+    const float a2 = A * jm * fm * sm * rs * rs;
+    g = f3(0.0f, fmaf(a1, y, -a2 * z), fmaf(a1, z, a2 * y));
+}
+
+// batched sweep: the instance's Bessel field
 template <> struct Field<FK_BATCH> {
     static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) {
-        if (F.mode == 0) bessel_field<0>(F, tab, p, s, n, g);
-        else if (F.mode == 1) bessel_field<1>(F, tab, p, s, n, g);
-        else bessel_field<2>(F, tab, p, s, n, g);
+        bessel_field_rt(F, tab, p, s, n, g);
     }
     static __device__ __forceinline__ void eval_ng(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) {
-        if (F.mode == 0) bessel_field_ng<0>(F, tab, p, s, n, g);
-        else if (F.mode == 1) bessel_field_ng<1>(F, tab, p, s, n, g);
-        else bessel_field_ng<2>(F, tab, p, s, n, g);
+        bessel_field_rt(F, tab, p, s, n, g);
     }
 };
 template <> struct Field<FK_PLANEWAVE> {
