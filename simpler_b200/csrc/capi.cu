@@ -415,8 +415,15 @@ struct smp_plan {
     size_t wave_bytes = 0;
     WaveParams wp;
     int grid_march = 0, grid_event = 0, grid_finish = 0;
-    unsigned *h_live = nullptr; // pinned
-    cudaEvent_t live_ev = nullptr;
+    unsigned long long *h_live = nullptr;   // pinned: [live slots, march-kernel steps] x 2 batches
+    cudaEvent_t live_ev[2] = {nullptr, nullptr};
+    cudaEvent_t batch_ev[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    // online chunk tuning: steady-state batches (pool full) cycle through the candidates, two
+    // each, and the plan keeps the fastest for the rest of its life (no extra work is traced)
+    bool tune_chunk = true;
+    int tuned_chunk = 0;
+    double tune_rate[4] = {0, 0, 0, 0};
+    int tune_n[4] = {0, 0, 0, 0};
     std::vector<cudaEvent_t> march_ev;   // event pairs around march-kernel launches (a reused pool)
     size_t march_ev_used = 0;            // since the last clear
     long long n_launched = 0;            // kernels launched since the last clear
@@ -440,7 +447,10 @@ static void plan_free(smp_plan *p) {
     cudaFree(p->d_counters);
     cudaFree(p->d_wave);
     if (p->h_live) cudaFreeHost(p->h_live);
-    if (p->live_ev) cudaEventDestroy(p->live_ev);
+    for (int i = 0; i < 2; ++i) {
+        if (p->live_ev[i]) cudaEventDestroy(p->live_ev[i]);
+        for (int j = 0; j < 2; ++j) if (p->batch_ev[i][j]) cudaEventDestroy(p->batch_ev[i][j]);
+    }
     for (cudaEvent_t e : p->march_ev) cudaEventDestroy(e);
     drop_launch_events(p);
     delete p;
@@ -554,7 +564,11 @@ int smp_plan_create(const smp_scene_desc *scene, const smp_medium_desc *medium, 
     p->device = opts->device;
     if (const char *eb = std::getenv("SMP_EVENT_BATCH")) p->event_batch = std::max(1, std::min(32, std::atoi(eb)));
     if (const char *kn = std::getenv("SMP_KERNEL")) p->persistent = std::strcmp(kn, "persistent") == 0;
-    if (const char *c = std::getenv("SMP_WF_CHUNK")) p->wave_chunk = std::max(2, std::min(4096, std::atoi(c)));
+    if (const char *c = std::getenv("SMP_WF_CHUNK")) {
+        p->wave_chunk = std::max(2, std::min(4096, std::atoi(c)));
+        p->tune_chunk = false;
+    }
+    if (const char *c = std::getenv("SMP_WF_TUNE")) p->tune_chunk = p->tune_chunk && std::atoi(c) != 0;
     if (const char *c = std::getenv("SMP_WF_SLOTS")) p->wave_slots_per_lane = std::max(1, std::min(16, std::atoi(c)));
     if (const char *c = std::getenv("SMP_WF_BATCH")) p->wave_batch = std::max(1, std::min(256, std::atoi(c)));
     p->scene = *scene;
@@ -727,8 +741,11 @@ static int wave_setup(smp_plan *p) {
     W.queue[1] = reinterpret_cast<int *>(b); b += bl;
     W.cnt = reinterpret_cast<unsigned *>(b);
     W.n_slots = int(n);
-    if (!p->h_live) SMP_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&p->h_live), 2 * sizeof(unsigned), cudaHostAllocDefault));
-    if (!p->live_ev) SMP_CUDA(cudaEventCreateWithFlags(&p->live_ev, cudaEventDisableTiming));
+    if (!p->h_live) SMP_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&p->h_live), 4 * sizeof(unsigned long long), cudaHostAllocDefault));
+    for (int i = 0; i < 2; ++i) {
+        if (!p->live_ev[i]) SMP_CUDA(cudaEventCreateWithFlags(&p->live_ev[i], cudaEventDisableTiming));
+        for (int j = 0; j < 2; ++j) if (!p->batch_ev[i][j]) SMP_CUDA(cudaEventCreate(&p->batch_ev[i][j]));
+    }
     return SMP_OK;
 }
 
@@ -751,12 +768,26 @@ static int wave_run(smp_plan *p, const KParams &k, cudaStream_t s) {
     const long long max_iter = (long long)k.step_cap * 4 + (1LL << 20);
     long long it = 0;
     bool pending = false;
+    int par = 0;                                     // ring slot of this batch's events and readback
+    int cand_of[2] = {-1, -1};                       // tuning candidate a batch ran, -1: none
+    unsigned long long prev_live = 0, prev_steps = 0;
+    bool have_prev = false;
+    static const int kChunkCand[4] = {64, 96, 128, 160};
     for (;;) {
         while (p->march_ev.size() < p->march_ev_used + 2 * size_t(p->wave_batch)) {
             cudaEvent_t e;
             SMP_CUDA(cudaEventCreate(&e));
             p->march_ev.push_back(e);
         }
+        // chunk of this batch: the tuned value, or the next tuning candidate
+        cand_of[par] = -1;
+        W.chunk = p->tuned_chunk > 0 ? p->tuned_chunk : p->wave_chunk;
+        if (p->tune_chunk && p->tuned_chunk == 0 && have_prev && prev_live == (unsigned long long)W.n_slots) {
+            int c = 0;
+            while (c < 3 && p->tune_n[c] >= 2) ++c;
+            if (p->tune_n[c] < 2) { cand_of[par] = c; W.chunk = kChunkCand[c]; }
+        }
+        SMP_CUDA(cudaEventRecord(p->batch_ev[par][0], s));
         for (int j = 0; j < p->wave_batch; ++j, ++it) {
             SMP_CUDA(cudaEventRecord(p->march_ev[p->march_ev_used], s));
             fm<<<p->grid_march, kBlock, p->smem_bytes, s>>>(k, W, int(it & 0x3fffffff));
@@ -764,25 +795,51 @@ static int wave_run(smp_plan *p, const KParams &k, cudaStream_t s) {
             p->march_ev_used += 2;
             fe<<<p->grid_event, kBlock, 0, s>>>(k, W, int(it & 0x3fffffff));
         }
+        SMP_CUDA(cudaEventRecord(p->batch_ev[par][1], s));
         p->n_launched += 2 * p->wave_batch;
         SMP_CUDA(cudaGetLastError());
-        if (pending) {                              // the previous batch's count
-            SMP_CUDA(cudaEventSynchronize(p->live_ev));
-            const unsigned live = p->h_live[0];
+        if (pending) {                              // the previous batch's readback
+            const int q = par ^ 1;
+            SMP_CUDA(cudaEventSynchronize(p->live_ev[q]));
+            const unsigned long long live = p->h_live[2 * q], steps = p->h_live[2 * q + 1];
+            if (cand_of[q] >= 0 && have_prev && live == (unsigned long long)W.n_slots && steps > prev_steps) {
+                float ms = 0.0f;
+                SMP_CUDA(cudaEventElapsedTime(&ms, p->batch_ev[q][0], p->batch_ev[q][1]));
+                if (ms > 0.0f) {
+                    p->tune_rate[cand_of[q]] += double(steps - prev_steps) / double(ms);
+                    p->tune_n[cand_of[q]] += 1;
+                    bool all = true;
+                    for (int c = 0; c < 4; ++c) all = all && p->tune_n[c] >= 2;
+                    if (all) {
+                        int best = 0;
+                        for (int c = 1; c < 4; ++c)
+                            if (p->tune_rate[c] / p->tune_n[c] > p->tune_rate[best] / p->tune_n[best]) best = c;
+                        p->tuned_chunk = kChunkCand[best];
+                    }
+                }
+            }
+            prev_live = live;
+            prev_steps = steps;
+            have_prev = true;
             if (live == 0u) break;
             // Fewer live slots than the slot pool means the photon counter is exhausted, and from
             // then on the count only falls, so the batch queued since holds at most `live`.
-            if (live <= finish_at && live < unsigned(W.n_slots)) {
+            if (live <= finish_at && live < (unsigned long long)W.n_slots) {
                 ff<<<p->grid_finish, kBlock, p->smem_bytes, s>>>(k, W, int(it & 0x3fffffff));
                 SMP_CUDA(cudaGetLastError());
                 p->n_launched += 1;
                 break;
             }
         }
-        // live slots after this batch = the march list the next march launch reads
-        SMP_CUDA(cudaMemcpyAsync(p->h_live, W.cnt + (it & 1), sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-        SMP_CUDA(cudaEventRecord(p->live_ev, s));
+        // live slots after this batch = the march list the next march launch reads; the march
+        // kernel's step counter for the tuner
+        p->h_live[2 * par] = 0;                       // free: its last readback was consumed above
+        SMP_CUDA(cudaMemcpyAsync(p->h_live + 2 * par, W.cnt + (it & 1), sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        SMP_CUDA(cudaMemcpyAsync(p->h_live + 2 * par + 1, k.counters + CNT_MARCH_STEPS, sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, s));
+        SMP_CUDA(cudaEventRecord(p->live_ev[par], s));
         pending = true;
+        par ^= 1;
         if (it > max_iter) return set_error(SMP_ERR_CUDA, "march loop did not drain after %lld launches", it);
     }
     return SMP_OK;

@@ -731,4 +731,60 @@ int run(const RenderConfig &c, std::ostream &log, std::string &err) {
     return SMP_OK;
 }
 
+// ================================================================================================
+// merging (helperScripts/mergeMultipleRenderings.cpp:207-231, with photon weights)
+// ================================================================================================
+bool merge_films(const std::vector<const std::vector<double> *> &films, const std::vector<double> &photons,
+                 std::vector<double> &out, std::string &err) {
+    if (films.empty() || films.size() != photons.size()) { err = "one photon count per film"; return false; }
+    double total = 0.0;
+    for (double n : photons) {
+        if (!(n >= 0.0)) { err = "photon counts must be non-negative"; return false; }
+        total += n;
+    }
+    if (!(total > 0.0)) { err = "photon counts sum to zero"; return false; }
+    const size_t n = films[0]->size();
+    out.assign(n, 0.0);
+    for (size_t i = 0; i < films.size(); ++i) {
+        if (films[i]->size() != n) { err = "film sizes differ"; return false; }
+        const double w = photons[i] / total;
+        for (size_t k = 0; k < n; ++k) out[k] += w * (*films[i])[k];
+    }
+    return true;
+}
+
+// Image2::writePFM's layout (rows bottom first), the inverse of read_pfm_texture
+bool write_pfm_texture(const std::string &path, const Texture &t, std::string &err) {
+    std::ofstream f(path, std::ios::binary);
+    if (!f) { err = "Problem writing output file " + path; return false; }
+    f << "Pf" << '\n' << t.x << ' ' << t.y << '\n' << static_cast<float>(-1.0) << '\n';
+    for (int i = 0; i < t.y; ++i)
+        f.write(reinterpret_cast<const char *>(&t.texels[size_t(t.y - i - 1) * t.x]), std::streamsize(size_t(t.x) * sizeof(double)));
+    if (!f) { err = "Problem writing output file " + path; return false; }
+    return true;
+}
+
+bool merge_reference_bins(const std::string &prefix, int renderings, int bins, const std::vector<double> &photons,
+                          std::string &err) {
+    if (renderings < 1 || bins < 1) { err = "renderings and pathLengthBins must be positive"; return false; }
+    std::vector<double> w = photons;
+    if (w.empty()) w.assign(size_t(renderings), 1.0);
+    if (int(w.size()) != renderings) { err = "photons= needs one count per rendering"; return false; }
+    for (int j = 0; j < bins; ++j) {
+        std::vector<Texture> tex(static_cast<size_t>(renderings));
+        std::vector<const std::vector<double> *> films;
+        for (int i = 0; i < renderings; ++i) {
+            if (!read_pfm_texture(prefix + "_" + std::to_string(i) + "_" + std::to_string(j) + ".pfm", tex[i], err)) return false;
+            if (tex[i].x != tex[0].x || tex[i].y != tex[0].y) { err = "image sizes differ in bin " + std::to_string(j); return false; }
+            films.push_back(&tex[i].texels);
+        }
+        Texture out;
+        out.x = tex[0].x;
+        out.y = tex[0].y;
+        if (!merge_films(films, w, out.texels, err)) return false;
+        if (!write_pfm_texture(prefix + "_mean_" + std::to_string(j) + ".pfm", out, err)) return false;
+    }
+    return true;
+}
+
 }  // namespace smp_host

@@ -122,4 +122,15 @@ void print_descs(const Built &b, std::ostream &os);
 // whole run: build, render (smp_render), write <outputFile>; returns 0 or a negative smp_status
 int run(const RenderConfig &cfg, std::ostream &log, std::string &err);
 
+// ---- merging renders (helperScripts/mergeMultipleRenderings.cpp) ----------------------------------
+// Photon-weighted mean sum_i N_i film_i / sum_i N_i of equally shaped films, in place into out.
+// The reference helper's running mean (mean (i+1) + x_i) / (i+2) over-weights its first rendering;
+// with equal N_i this is the plain mean.
+bool merge_films(const std::vector<const std::vector<double> *> &films, const std::vector<double> &photons,
+                 std::vector<double> &out, std::string &err);
+// the helper's file set <prefix>_<i>_<j>.pfm (rendering i, path-length bin j) -> <prefix>_mean_<j>.pfm
+bool merge_reference_bins(const std::string &prefix, int renderings, int bins, const std::vector<double> &photons,
+                          std::string &err);
+bool write_pfm_texture(const std::string &path, const Texture &t, std::string &err);
+
 }  // namespace smp_host
