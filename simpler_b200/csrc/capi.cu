@@ -422,6 +422,11 @@ struct smp_plan {
     // each, and the plan keeps the fastest for the rest of its life (no extra work is traced)
     bool tune_chunk = true;
     int tuned_chunk = 0;
+    // SMP_WF_GRAPH=1: once the chunk is fixed, each batch of march/event pairs is one CUDA graph
+    // launch (captured once per trace); march launches inside graphs are not timed individually
+    bool use_graph = false;
+    cudaStream_t cap_stream = nullptr;
+    long long graph_march_launches = 0;
     double tune_rate[4] = {0, 0, 0, 0};
     int tune_n[4] = {0, 0, 0, 0};
     std::vector<cudaEvent_t> march_ev;   // event pairs around march-kernel launches (a reused pool)
@@ -452,6 +457,7 @@ static void plan_free(smp_plan *p) {
         for (int j = 0; j < 2; ++j) if (p->batch_ev[i][j]) cudaEventDestroy(p->batch_ev[i][j]);
     }
     for (cudaEvent_t e : p->march_ev) cudaEventDestroy(e);
+    if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
     drop_launch_events(p);
     delete p;
 }
@@ -569,6 +575,7 @@ int smp_plan_create(const smp_scene_desc *scene, const smp_medium_desc *medium, 
         p->tune_chunk = false;
     }
     if (const char *c = std::getenv("SMP_WF_TUNE")) p->tune_chunk = p->tune_chunk && std::atoi(c) != 0;
+    if (const char *c = std::getenv("SMP_WF_GRAPH")) p->use_graph = std::atoi(c) != 0;
     if (const char *c = std::getenv("SMP_WF_SLOTS")) p->wave_slots_per_lane = std::max(1, std::min(16, std::atoi(c)));
     if (const char *c = std::getenv("SMP_WF_BATCH")) p->wave_batch = std::max(1, std::min(256, std::atoi(c)));
     p->scene = *scene;
@@ -679,6 +686,7 @@ int smp_plan_clear(smp_plan *plan, void *stream) {
     SMP_CUDA(cudaStreamSynchronize(s));
     drop_launch_events(plan);
     plan->march_ev_used = 0;
+    plan->graph_march_launches = 0;
     plan->n_launched = 0;
     std::memset(&plan->stats, 0, sizeof(plan->stats));
     return SMP_OK;
@@ -773,6 +781,11 @@ static int wave_run(smp_plan *p, const KParams &k, cudaStream_t s) {
     unsigned long long prev_live = 0, prev_steps = 0;
     bool have_prev = false;
     static const int kChunkCand[4] = {64, 96, 128, 160};
+    cudaGraphExec_t gexec = nullptr;                 // this trace's batch graph (graph mode)
+    struct GraphGuard {
+        cudaGraphExec_t *g;
+        ~GraphGuard() { if (*g) cudaGraphExecDestroy(*g); }
+    } gguard{&gexec};
     for (;;) {
         while (p->march_ev.size() < p->march_ev_used + 2 * size_t(p->wave_batch)) {
             cudaEvent_t e;
@@ -788,12 +801,33 @@ static int wave_run(smp_plan *p, const KParams &k, cudaStream_t s) {
             if (p->tune_n[c] < 2) { cand_of[par] = c; W.chunk = kChunkCand[c]; }
         }
         SMP_CUDA(cudaEventRecord(p->batch_ev[par][0], s));
-        for (int j = 0; j < p->wave_batch; ++j, ++it) {
-            SMP_CUDA(cudaEventRecord(p->march_ev[p->march_ev_used], s));
-            fm<<<p->grid_march, kBlock, p->smem_bytes, s>>>(k, W, int(it & 0x3fffffff));
-            SMP_CUDA(cudaEventRecord(p->march_ev[p->march_ev_used + 1], s));
-            p->march_ev_used += 2;
-            fe<<<p->grid_event, kBlock, 0, s>>>(k, W, int(it & 0x3fffffff));
+        const bool graphed = p->use_graph && cand_of[par] < 0 && (p->tuned_chunk > 0 || !p->tune_chunk);
+        if (graphed) {
+            // batches start at even iterations, so one capture with it = 0 .. batch-1 serves all
+            if (!gexec) {
+                if (!p->cap_stream) SMP_CUDA(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
+                cudaGraph_t g = nullptr;
+                SMP_CUDA(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
+                for (int j = 0; j < p->wave_batch; ++j) {
+                    fm<<<p->grid_march, kBlock, p->smem_bytes, p->cap_stream>>>(k, W, j);
+                    fe<<<p->grid_event, kBlock, 0, p->cap_stream>>>(k, W, j);
+                }
+                SMP_CUDA(cudaStreamEndCapture(p->cap_stream, &g));
+                cudaError_t e = cudaGraphInstantiate(&gexec, g, 0ULL);
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess) return set_error(SMP_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+            }
+            SMP_CUDA(cudaGraphLaunch(gexec, s));
+            it += p->wave_batch;
+            p->graph_march_launches += p->wave_batch;
+        } else {
+            for (int j = 0; j < p->wave_batch; ++j, ++it) {
+                SMP_CUDA(cudaEventRecord(p->march_ev[p->march_ev_used], s));
+                fm<<<p->grid_march, kBlock, p->smem_bytes, s>>>(k, W, int(it & 0x3fffffff));
+                SMP_CUDA(cudaEventRecord(p->march_ev[p->march_ev_used + 1], s));
+                p->march_ev_used += 2;
+                fe<<<p->grid_event, kBlock, 0, s>>>(k, W, int(it & 0x3fffffff));
+            }
         }
         SMP_CUDA(cudaEventRecord(p->batch_ev[par][1], s));
         p->n_launched += 2 * p->wave_batch;
@@ -906,7 +940,8 @@ static int collect_stats(smp_plan *plan) {
     plan->stats.march_ms = plan->persistent ? ms_total : march_ms;
     plan->stats.march_steps = plan->persistent ? (int64_t)c[CNT_STEPS] : (int64_t)c[CNT_MARCH_STEPS];
     plan->stats.launches = plan->n_launched;
-    plan->stats.march_launches = plan->persistent ? plan->n_launched : (int64_t)(plan->march_ev_used / 2);
+    plan->stats.march_launches = plan->persistent ? plan->n_launched
+                                                  : (int64_t)(plan->march_ev_used / 2) + plan->graph_march_launches;
     if (c[CNT_STAGE_TIMEOUT]) return set_error(SMP_ERR_CUDA, "%llu block(s) timed out staging the field table", c[CNT_STAGE_TIMEOUT]);
     if (c[CNT_LOST]) return set_error(SMP_ERR_CUDA, "internal: %llu live slot(s) had no lane in the tail kernel", c[CNT_LOST]);
     if (c[CNT_STEP_CAP]) return set_error(SMP_ERR_STEP_CAP, "%llu photon(s) hit the per-photon step cap", c[CNT_STEP_CAP]);
