@@ -31,7 +31,7 @@ sys.path.insert(0, ROOT)
 
 import simpler_b200 as sb  # noqa: E402
 from simpler_b200 import _lib as L  # noqa: E402
-from simpler_b200.roofline import flop_per_step_bessel  # noqa: E402
+from simpler_b200.roofline import flop_per_step  # noqa: E402
 
 METRIC = "photon paths/s"
 RENDER_PHOTONS = 100_000_000
@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--photons-per-step", type=int, default=PHOTONS_PER_STEP)
-    ap.add_argument("--workload", choices=["precision", "sweep"], default="precision",
+    ap.add_argument("--workload", choices=["precision", "sweep", "plain", "planewave", "spline"], default="precision",
                     help="precision: the headline line (default); sweep: the batched 256-instance sweep "
                          "against the same instances rendered one by one")
     ap.add_argument("--sweep-scale", type=float, default=1.0,
@@ -54,12 +54,43 @@ def parse():
     return ap.parse_args()
 
 
-def workload(device: int = 0) -> sb.Setup:
+# secondary workloads (--workload): the other configurations of the same path, one JSON line each
+OTHER = {
+    "plain": (lambda d: sb.config_plain_small(device=d), 1_000_000, 1_000_000,
+              "plain small: Bessel mode 0, dn 1e-3 at 848 kHz, sigma_s 0.1/mm, albedo 0.9, g 0.9, "
+              "0.5 mm beam, 128x128 x 32 bins, fp32, 1e6 photons"),
+    "planewave": (lambda d: sb.config_planewave(device=d), 10_000_000, 10_000_000,
+                  "two plane waves a = 1e-3 at 1 MHz along +y and +z, phases U[0, 2 pi) (seed 3), "
+                  "sigma_s 0.5/mm, albedo 0.9, g 0.9, 128x128 x 32 bins, fp32, 1e7 photons"),
+    "spline": (lambda d: sb.config_spline(device=d), 10_000_000, 1_000_000_000,
+               "tricubic spline 64^3 over the 10 mm cube (Gaussian-filtered noise, max dn 1e-3, seed 4), "
+               "sigma_s 1/mm, albedo 0.95, g 0.8, 256x256 x 64 bins, fp32; 1e7-photon steps of a "
+               "1e9-photon render"),
+}
+
+
+_ARGS = None           # the parsed command line (set in main)
+
+
+def workload(args=None, device: int = 0) -> sb.Setup:
+    args = args or _ARGS
+    if args is not None and args.workload in OTHER:
+        return OTHER[args.workload][0](device)
     return sb.config_precision(device=device)
 
 
+def render_photons(args=None) -> int:
+    args = args or _ARGS
+    return OTHER[args.workload][2] if args is not None and args.workload in OTHER else RENDER_PHOTONS
+
+
 def config_json(args, per_step: int) -> dict:
-    s = workload()
+    s = workload(args)
+    if args.workload in OTHER:
+        return {"workload": OTHER[args.workload][3], "photons_per_step_per_gpu": per_step,
+                "render_photons": render_photons(args), "film": [s.spatial_x, s.spatial_y, s.path_length_bins],
+                "er_stepsize_m": s.er_stepsize, "precision_levels": s.precision,
+                "rng": "philox-4x32-10 keyed by global photon index"}
     return {
         "workload": WORKLOAD,
         "photons_per_step_per_gpu": per_step,
@@ -136,7 +167,7 @@ def cpu_trace(n: int, first: int, threads: int) -> float:
     s = workload()
     sc, md, fd, op = s.descs()
     t0 = time.perf_counter()
-    rc = lib.orc_render(C.byref(sc), C.byref(md), C.byref(fd), C.byref(op), 32, threads, first, n, RENDER_PHOTONS,
+    rc = lib.orc_render(C.byref(sc), C.byref(md), C.byref(fd), C.byref(op), 32, threads, first, n, render_photons(),
                         None, None, None, None)
     dt = time.perf_counter() - t0
     assert rc == 0
@@ -197,8 +228,9 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
-    per_step = args.photons_per_step
-    setup = workload(local)
+    per_step = args.photons_per_step if args.workload not in OTHER or args.photons_per_step != PHOTONS_PER_STEP \
+        else OTHER[args.workload][1]
+    setup = workload(args, local)
     plan = sb.Plan(setup)
     stream = torch.cuda.current_stream()
     h = stream.cuda_stream
@@ -207,7 +239,7 @@ def run_ours(args):
 
     def step(i):
         first = (i * world + rank) * per_step
-        plan.trace(first, per_step, RENDER_PHOTONS, stream=h)
+        plan.trace(first, per_step, render_photons(args), stream=h)
         if world > 1:
             plan.read_image_device(film.data_ptr(), stream=h)
             dist.reduce(film, dst=0)
@@ -248,14 +280,18 @@ def run_ours(args):
     if rank == 0:
         peak = C.c_double()
         L.check(L.load().smp_fp32_peak(local, C.byref(peak)))
-        fps = flop_per_step_bessel(setup.mode)
+        fps = flop_per_step(setup)
         # the dominant kernel is the ER-march kernel: its launches are timed with CUDA events on
         # this stream inside the library, and it counts the steps it executes
         n_march = max(1, st1.march_launches - st0.march_launches)
         achieved = fps * march_steps / (march_ms / 1e3) / 1e12
-        roof = {"bound": "fp32", "kernel": "wf_march_kernel<FK_BESSEL1, fp64 path length>",
+        kname = {L.FIELD_PLANEWAVE: "FK_PLANEWAVE", L.FIELD_SPLINE: "FK_SPLINE"}.get(
+            setup.field_type, f"FK_BESSEL{setup.mode}")
+        form = "fp64 path length" if setup.precision_mode == L.PREC_MIXED else "fp32"
+        roof = {"bound": "fp32", "kernel": f"wf_march_kernel<{kname}, {form}>",
                 "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-                "frac": achieved / peak.value, "traffic": _profile_traffic(),
+                "frac": achieved / peak.value,
+                "traffic": _profile_traffic() if args.workload == "precision" else None,
                 "flop_per_er_step": fps, "er_steps_per_launch": march_steps / n_march,
                 "march_kernel_share_of_step_time": march_ms / ms,
                 "peak_source": "FP32 FMA throughput measured live on this GPU (smp_fp32_peak)"}
@@ -355,7 +391,9 @@ def run_sweep(args):
 
 
 def main():
+    global _ARGS
     args = parse()
+    _ARGS = args
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "sweep":

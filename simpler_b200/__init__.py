@@ -7,11 +7,11 @@ if it is missing: there is no CPU fallback.
 from . import _lib
 from ._lib import SmpError, check_layout, load
 from .render import Plan, field_eval, records_to_arrays, render, render_batch, trace_photons
-from .scene import (Setup, bernoulli_texture, config_batch_sweep, config_planewave, config_plain_small,
+from .scene import (Setup, bernoulli_texture, config_batch_sweep, config_planewave, config_plain_small, config_spline,
                     config_precision, disk_texture)
 
 __all__ = [
     "SmpError", "check_layout", "load", "Plan", "field_eval", "records_to_arrays", "render", "render_batch",
-    "trace_photons", "config_batch_sweep",
+    "trace_photons", "config_batch_sweep", "config_spline",
     "Setup", "bernoulli_texture", "config_planewave", "config_plain_small", "config_precision", "disk_texture",
 ]

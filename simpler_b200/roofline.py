@@ -12,6 +12,14 @@ add/sub/mul/div/sqrt and one per transcendental call (jn, atan2, sin, cos):
                        1/r, 1/r^2 (2); m = 0: grad (2 x 4)                                      = 10
                        m >= 1: atan2, m*phi, cos, sin (4) + J' (3) + grad (2 x 11)              = 31
   mode 0: 55 FLOP/step, mode >= 1: 78 FLOP/step.
+
+  plane waves (each)   phase k.p - tau + phase (7) + sin, cos (2) + n (2) + grad (7)           = 18
+                       n = n_o + sum (1): two waves 37, 71 FLOP/step
+  tricubic spline      per axis: floor, fraction, 4 weights, 4 derivative weights (25)          = 75
+                       16 rows of 4 taps: value and x-derivative sums (14) + y/z/value/x
+                       accumulation (11) (spline.h:415-448, separable)                          = 400
+                       scale of the gradient (3) + base (1)                                      = 4
+                       479, 513 FLOP/step
 """
 
 FLOP_LEAPFROG = 24
@@ -21,3 +29,21 @@ FLOP_BOOKKEEPING = 10
 def flop_per_step_bessel(mode: int) -> int:
     field = 11 + 2 + (8 if mode == 0 else 31)
     return FLOP_LEAPFROG + FLOP_BOOKKEEPING + field
+
+
+def flop_per_step_planewave(n_waves: int) -> int:
+    return FLOP_LEAPFROG + FLOP_BOOKKEEPING + 18 * n_waves + 1
+
+
+def flop_per_step_spline() -> int:
+    return FLOP_LEAPFROG + FLOP_BOOKKEEPING + 75 + 400 + 4
+
+
+def flop_per_step(setup) -> int:
+    """FLOP per ER step of a Setup's field."""
+    from . import _lib as L
+    if setup.field_type == L.FIELD_PLANEWAVE:
+        return flop_per_step_planewave(len(setup.wave_amp))
+    if setup.field_type == L.FIELD_SPLINE:
+        return flop_per_step_spline()
+    return flop_per_step_bessel(setup.mode)

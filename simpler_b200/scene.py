@@ -258,3 +258,19 @@ def config_batch_sweep(n_inst: int = 256, seed: int = 2, scale: float = 1.0, **k
         insts.append({"mode": mode, "n_max": n_max, "n_clip": n_max, "f_u": f_u, "phi_min": 0.0,
                       "phi_max": 2.0 * math.pi * duty, "n_photons": max(n_ph, 1), "seed": (seed << 32) + i})
     return setup, insts
+
+
+def config_spline(n: int = 64, seed: int = 4, **kw) -> Setup:
+    """The spline-field configuration: an n^3 tricubic B-spline coefficient grid over the 10 mm
+    cube whose coefficients are n_o + Gaussian-filtered (sigma 4 voxels) N(0, 1) noise from
+    numpy's default_rng(seed), scaled to a largest |dn| of 1e-3; sigma_s 1/mm, albedo 0.95,
+    g 0.8, 256x256 px x 64 bins."""
+    from scipy.ndimage import gaussian_filter
+    noise = gaussian_filter(np.random.default_rng(seed).standard_normal((n, n, n)), sigma=4.0, mode="wrap")
+    coeff = 1.3333 + noise * (1e-3 / np.abs(noise).max())
+    s = Setup(field_type=L.FIELD_SPLINE, grid_coeff=coeff.astype(np.float32), grid_min=(-0.005,) * 3,
+              grid_max=(0.005,) * 3, sigma_t=1000.0 / 0.95, albedo=0.95, g=0.8, spatial_x=256, spatial_y=256,
+              path_length_bins=64, path_length_max=0.1)
+    for kk, v in kw.items():
+        setattr(s, kk, v)
+    return s
