@@ -22,6 +22,10 @@
  *   smp_texture_cdf                <- area_textured_source texture CDF      renderer/src/area_textured_source.cpp:41-45
  *   smp_render_batch               <- the serial per-configuration loops    renderer/pybindFiles/tests/FUS_configurations.ipynb
  *                                     (one renderImage per configuration)   (cells at lines 591-603, 713-725)
+ *   smp_render_adjoint /           <- no counterpart: the reference has forward-mode tangents of
+ *   smp_plan_adjoint                  single leapfrog steps only (er_derivativestep scene.cpp:351-359,
+ *                                     bessel_HessianRIF :259-320, Spline::hessian spline.h:359-413),
+ *                                     used by no render path
  */
 #ifndef SIMPLER_B200_H_
 #define SIMPLER_B200_H_
@@ -310,6 +314,39 @@ int smp_render_noalloc(const smp_scene_desc *scene, const smp_medium_desc *mediu
                        int64_t first_photon, int64_t n_photons, int64_t weight_photons,
                        void *d_film, void *stream, smp_stats *stats_out);
 
+/* ---- adjoint: gradient of a sensor objective with respect to the field's parameters ---------- */
+typedef struct smp_adjoint_stats {
+    int64_t photons;              /* photons differentiated                                         */
+    int64_t dropped;              /* photons left out: more scatter vertices than the checkpoint
+                                     buffer holds, or a move longer than the trajectory buffer      */
+    int64_t skipped;              /* sensor marches (direct, connections) left out: longer than the
+                                     trajectory buffer (SMP_ADJ_TCAP accepted steps, default 8192);
+                                     their value carries exp(-sigma_t d) of that length            */
+    int64_t aborted;              /* photons left out: step cap or non-finite state                 */
+    int64_t replay_mismatch;      /* segment replays that did not reproduce their checkpoint (0)    */
+    int64_t er_steps_forward;     /* er_step evaluations of the checkpointing trace                 */
+    int64_t er_steps_replay;      /* er_step evaluations of the segment replays                     */
+    int64_t points;               /* trajectory points swept backwards                              */
+    int64_t splats;               /* splats whose value entered the objective                       */
+    double  kernel_ms;            /* device time of the adjoint launch                              */
+} smp_adjoint_stats;
+/* Number of parameters smp_render_adjoint returns for this field, or a negative smp_status:
+   plane waves 2*n_waves (amplitudes a_0..a_{W-1}, then phases phase_0..phase_{W-1});
+   spline grid_n[0]*grid_n[1]*grid_n[2] coefficients in grid_coeff's order. */
+int64_t smp_adjoint_param_count(const smp_field_desc *field);
+/* Gradient of J = sum_pixels dJ_dfilm[pixel] * film[pixel] with respect to the field parameters,
+   where film is the image smp_render would produce for photons [first_photon, first_photon +
+   n_photons) with the same opts (Philox streams, same seed; weight_photons as in smp_plan_trace).
+   It is the pathwise derivative of that estimator: per photon, random numbers, discrete events
+   and ER step sequences are held fixed, and marches ending on a face end on the face plane.
+   dJ_dfilm: host, X*Y*Z doubles (Image3 layout); grad_out: host, smp_adjoint_param_count doubles,
+   overwritten. Plane-wave and spline fields, Philox streams, no lenses; others return
+   SMP_ERR_UNSUPPORTED. Synchronous. */
+int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, int64_t weight_photons,
+                     const double *dJ_dfilm, double *grad_out, smp_adjoint_stats *stats_out);
+int smp_render_adjoint(const smp_scene_desc *scene, const smp_medium_desc *medium,
+                       const smp_field_desc *field, const smp_render_opts *opts, int64_t n_photons,
+                       const double *dJ_dfilm, double *grad_out, smp_adjoint_stats *stats_out);
 /* Measurement utility with no counterpart in the reference: the device's FP32 FMA throughput
    (TFLOP/s, 2 FLOP per FMA) measured with independent FMA chains on every SM; the roofline
    denominator for the march, which is bound by the FP32 and issue pipes. */

@@ -131,10 +131,19 @@ class InstanceDesc(C.Structure):
     _fields_ = [("field", FieldDesc), ("medium", MediumDesc), ("n_photons", C.c_int64), ("seed", C.c_uint64)]
 
 
+class AdjointStats(C.Structure):
+    _fields_ = [
+        ("photons", C.c_int64), ("dropped", C.c_int64), ("skipped", C.c_int64), ("aborted", C.c_int64),
+        ("replay_mismatch", C.c_int64), ("er_steps_forward", C.c_int64), ("er_steps_replay", C.c_int64),
+        ("points", C.c_int64), ("splats", C.c_int64), ("kernel_ms", C.c_double),
+    ]
+
+
 STRUCTS = {
     "smp_field_desc": FieldDesc, "smp_scene_desc": SceneDesc, "smp_medium_desc": MediumDesc,
     "smp_render_opts": RenderOpts, "smp_stats": Stats, "smp_photon_record": PhotonRecord,
     "smp_splat_record": SplatRecord, "smp_instance_desc": InstanceDesc,
+    "smp_adjoint_stats": AdjointStats,
 }
 
 # every entry point declared in include/simpler_b200.h
@@ -143,7 +152,7 @@ EXPORTS = [
     "smp_plan_create", "smp_plan_destroy", "smp_plan_set_field", "smp_plan_clear", "smp_plan_trace",
     "smp_plan_read_image", "smp_plan_film", "smp_plan_stats", "smp_plan_render", "smp_trace_photons",
     "smp_field_eval", "smp_texture_cdf", "smp_spline_prefilter", "smp_render_batch", "smp_fp32_peak",
-    "smp_render_noalloc",
+    "smp_render_noalloc", "smp_adjoint_param_count", "smp_plan_adjoint", "smp_render_adjoint",
 ]
 
 _lib = None
@@ -189,6 +198,11 @@ def load() -> C.CDLL:
     lib.smp_fp32_peak.argtypes = [C.c_int, P(C.c_double)]
     lib.smp_render_noalloc.argtypes = [P(SceneDesc), P(MediumDesc), P(FieldDesc), P(RenderOpts), C.c_int64, C.c_int64,
                                        C.c_int64, vp, vp, P(Stats)]
+    lib.smp_adjoint_param_count.restype = C.c_int64
+    lib.smp_adjoint_param_count.argtypes = [P(FieldDesc)]
+    lib.smp_plan_adjoint.argtypes = [vp, C.c_int64, C.c_int64, C.c_int64, vp, vp, P(AdjointStats)]
+    lib.smp_render_adjoint.argtypes = [P(SceneDesc), P(MediumDesc), P(FieldDesc), P(RenderOpts), C.c_int64, vp, vp,
+                                       P(AdjointStats)]
     _lib = lib
     return lib
 

@@ -34,7 +34,7 @@ NVCC_FLAGS = [
 ]
 
 CU_SOURCES = ["capi.cu", "host/smp_host.cpp"]
-HEADERS = ["kparams.h", "dev_math.cuh", "dev_field.cuh", "march.cuh", "wavefront.cuh", "host/smp_host.h"]
+HEADERS = ["kparams.h", "dev_math.cuh", "dev_field.cuh", "march.cuh", "wavefront.cuh", "adjoint.cuh", "host/smp_host.h"]
 BIN = os.path.join(HERE, "bin")
 MAINS = {"renderer3d": "host/renderer3d_main.cpp", "simplER": "host/simpler_main.cpp",
          "merge_renderings": "host/merge_main.cpp"}

@@ -1,0 +1,793 @@
+// adjoint.cuh -- reverse-mode derivative of a render's sensor objective with respect to the
+// refractive-index field's parameters (plane-wave amplitudes and phases, spline coefficients).
+//
+// Objective: J = sum_pixels G[pixel] * film[pixel] for a caller-given weight image G (dJ/dfilm;
+// a region-of-interest mask gives ROI throughput). The film is the render's own estimator
+// (Philox streams keyed by photon index), so J and its gradient are per-photon sums and the
+// gradient is the pathwise derivative of exactly the estimator the forward render evaluates on
+// the same seed: random numbers, discrete choices (roulette, Fresnel reflect/refract, texel,
+// z bin) and the ER step sequence of every march are held fixed, and the continuous chain
+//
+//   source -> n(p0) omega0 -> [march] -> vertex 1 -> [connection march] -> sensor splat
+//                                     \-> HG rotation -> [march] -> vertex 2 -> ...
+//
+// is differentiated. Marches that end on a face are differentiated as ending ON the face: the
+// end point moves along the ray to the face plane (the implicit crossing of the continuous
+// path), which shifts the arc length (exp(-sigma_t d) of connections; the remaining distance of
+// a move after a reflection).
+//
+// Path replay with checkpointed scatter vertices, one photon per thread:
+//   phase A  trace the photon (run_events + march_step, the render's own code) and record a
+//            checkpoint at the source and at every scatter vertex: position, optical direction,
+//            path length, step count and the Philox draw index (draw k of photon i is a pure
+//            function of (seed, i, k), so any segment can be replayed from its checkpoint);
+//   phase B  walk the vertices backwards. For each segment (connection from vertex k, move from
+//            vertex k-1 to k, the direct march), replay it forward from its checkpoint writing the
+//            accepted ER-step positions to this thread's trajectory buffer, then sweep the buffer
+//            backwards: the adjoint of kick-drift-kick (scene.cpp:323-330)
+//              dh = d + h/2 g(p),  p' = p + dh h/n(p),  d' = dh + h/2 g(p')
+//            needs n, grad n and the Hessian of n at every point, and accumulates
+//            dJ/dtheta through dn/dtheta and dgrad n/dtheta at every point.
+// The splat's value (Fresnel exit, foreshortening, Henyey-Greenstein, exp(-sigma_t d), bilinear
+// weights) and the HG frame rotation at a vertex are differentiated with forward-mode dual numbers.
+#pragma once
+#include "march.cuh"
+
+namespace smp {
+
+// ---- forward-mode dual numbers (event-level functions of a few inputs) -----------------------
+template <int N> struct Dual {
+    float v;
+    float d[N];
+};
+template <int N> __device__ __forceinline__ Dual<N> dc(float v) {
+    Dual<N> r; r.v = v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = 0.0f;
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> dvar(float v, int i) { Dual<N> r = dc<N>(v); r.d[i] = 1.0f; return r; }
+template <int N> __device__ __forceinline__ Dual<N> operator+(const Dual<N> &a, const Dual<N> &b) {
+    Dual<N> r; r.v = a.v + b.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] + b.d[i];
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator-(const Dual<N> &a, const Dual<N> &b) {
+    Dual<N> r; r.v = a.v - b.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] - b.d[i];
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator*(const Dual<N> &a, const Dual<N> &b) {
+    Dual<N> r; r.v = a.v * b.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator*(const Dual<N> &a, float s) {
+    Dual<N> r; r.v = a.v * s;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * s;
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator*(float s, const Dual<N> &a) { return a * s; }
+template <int N> __device__ __forceinline__ Dual<N> operator+(const Dual<N> &a, float s) { Dual<N> r = a; r.v += s; return r; }
+template <int N> __device__ __forceinline__ Dual<N> operator+(float s, const Dual<N> &a) { return a + s; }
+template <int N> __device__ __forceinline__ Dual<N> operator-(const Dual<N> &a, float s) { Dual<N> r = a; r.v -= s; return r; }
+template <int N> __device__ __forceinline__ Dual<N> operator-(float s, const Dual<N> &a) {
+    Dual<N> r; r.v = s - a.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = -a.d[i];
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator/(const Dual<N> &a, const Dual<N> &b) {
+    Dual<N> r; r.v = a.v / b.v;
+    const float ib = 1.0f / b.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) * ib;
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator/(const Dual<N> &a, float s) {
+    Dual<N> r; r.v = a.v / s;
+    const float is = 1.0f / s;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * is;
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> operator/(float s, const Dual<N> &b) {
+    Dual<N> r; r.v = s / b.v;
+    const float k = -r.v / b.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = b.d[i] * k;
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> dsqrt(const Dual<N> &a) {
+    Dual<N> r; r.v = sqrtf(a.v);
+    const float h = 0.5f / r.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * h;
+    return r;
+}
+template <int N> __device__ __forceinline__ Dual<N> dexp(const Dual<N> &a) {
+    Dual<N> r; r.v = expf(a.v);
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * r.v;
+    return r;
+}
+
+// ---- device-side parameters of an adjoint launch -----------------------------------------------
+struct AdjVertex {             // a checkpoint (source: index 0, scatter vertex k: index k)
+    float pos[3], dir[3];      // photon position and optical direction v = n omega
+    float total_dist;          // first sampled distance (maxPathlength test)
+    int depth;
+    int draws_v, steps_v;      // Philox draw index and ER-step count at EV_VERTEX (after its depth test)
+    int draws_so, steps_so;    // the same at EV_SCATTER_ONCE (source: at EV_SCATTER)
+    double total;              // optical path length
+};
+
+enum AdjCounter : int {
+    ADJ_NEXT = 0,          // work distribution
+    ADJ_PHOTONS = 1,       // photons differentiated
+    ADJ_DROPPED = 2,       // photons left out: more vertices than checkpoints, or a move longer than the buffer
+    ADJ_ABORTED = 3,       // photons left out: step cap or non-finite state in the forward trace
+    ADJ_MISMATCH = 4,      // replays whose end state differed from the checkpoint (a defect)
+    ADJ_STEPS_FWD = 5,     // er_step evaluations of phase A
+    ADJ_STEPS_REPLAY = 6,  // er_step evaluations of phase B's replays
+    ADJ_POINTS = 7,        // trajectory points swept backwards
+    ADJ_SPLATS = 8,        // splats differentiated
+    ADJ_MIS_CONN = 9,      // mismatch detail: a connection replay did not reach its end event
+    ADJ_MIS_MOVE = 10,     //                  a move replay did not reach its vertex
+    ADJ_MIS_DIRECT = 11,   //                  the direct replay did not reach the scatter stage
+    ADJ_MIS_POS = 12,      //                  a move replay reached a different position
+    ADJ_MIS_DIR = 13,      //                  ... the same position with a different direction
+    ADJ_SKIPPED = 14,      // sensor marches (direct, connections) longer than the trajectory buffer
+    ADJ_COUNT = 15
+};
+
+struct AdjParams {
+    int X, Y, Z;               // film shape (KParams.X is 0 in an adjoint launch: replays splat nothing)
+    const double *G;           // dJ/dfilm, X*Y*Z, Image3 layout
+    float4 *traj;              // [tcap][lanes]: (position, step size); step size 0 = segment start,
+                               // -1 = a face reflection between two marches of the segment
+    AdjVertex *verts;          // [lanes][vcap]
+    int tcap, vcap, lanes;
+    double *grad;              // dJ/dtheta (layout per field kind, see FieldAdj)
+    unsigned long long *cnt;   // AdjCounter
+};
+
+// ---- field: n, grad n, Hessian, and the parameter vector-Jacobian product -------------------------
+// H = (xx, yy, zz, xy, xz, yz).
+__device__ __forceinline__ float3 hmul(const float H[6], float3 b) {
+    return f3(H[0] * b.x + H[3] * b.y + H[4] * b.z,
+              H[3] * b.x + H[1] * b.y + H[5] * b.z,
+              H[4] * b.x + H[5] * b.y + H[2] * b.z);
+}
+
+template <int FK> struct FieldAdj;
+
+// Plane waves n = n_o + sum_i a_i sin(k_i.p - tau + phase_i):
+//   grad n = sum_i a_i cos(.) k_i,  H = -sum_i a_i sin(.) k_i k_i^T,
+//   dJ/da_i += a sin + cos (k_i.b),  dJ/dphase_i += a a_i cos - a_i sin (k_i.b)
+// for the cotangent (a, b) of (n, grad n). Gradient layout: a_0..a_{W-1}, phase_0..phase_{W-1}.
+template <> struct FieldAdj<FK_PLANEWAVE> {
+    struct Acc { float ga[SMP_MAX_WAVES], gp[SMP_MAX_WAVES]; };
+    static __device__ __forceinline__ void clear(Acc &c) {
+#pragma unroll
+        for (int i = 0; i < SMP_MAX_WAVES; ++i) { c.ga[i] = 0.0f; c.gp[i] = 0.0f; }
+    }
+    static __device__ __forceinline__ void eval_h(const FieldParams &F, float3 p, float tau, float &n, float3 &g, float H[6]) {
+#pragma unroll
+        for (int j = 0; j < 6; ++j) H[j] = 0.0f;
+        n = F.n_o;
+        g = f3(0.0f, 0.0f, 0.0f);
+        if (in_gap(F, p)) return;
+#pragma unroll
+        for (int i = 0; i < SMP_MAX_WAVES; ++i) {
+            if (i < F.n_waves) {
+                const float kx = F.wk[i][0], ky = F.wk[i][1], kz = F.wk[i][2];
+                float sn, cs;
+                sincos_red(kx * p.x + ky * p.y + kz * p.z - tau + F.wphase[i], sn, cs);
+                n += F.wamp[i] * sn;
+                const float ac = F.wamp[i] * cs, as = -F.wamp[i] * sn;
+                g.x += ac * kx; g.y += ac * ky; g.z += ac * kz;
+                H[0] += as * kx * kx; H[1] += as * ky * ky; H[2] += as * kz * kz;
+                H[3] += as * kx * ky; H[4] += as * kx * kz; H[5] += as * ky * kz;
+            }
+        }
+    }
+    static __device__ __forceinline__ void theta(const FieldParams &F, float3 p, float tau, float a, float3 b, Acc &c, const AdjParams &) {
+        if (in_gap(F, p)) return;
+#pragma unroll
+        for (int i = 0; i < SMP_MAX_WAVES; ++i) {
+            if (i < F.n_waves) {
+                const float kx = F.wk[i][0], ky = F.wk[i][1], kz = F.wk[i][2];
+                float sn, cs;
+                sincos_red(kx * p.x + ky * p.y + kz * p.z - tau + F.wphase[i], sn, cs);
+                const float kb = kx * b.x + ky * b.y + kz * b.z;
+                c.ga[i] += a * sn + cs * kb;
+                c.gp[i] += F.wamp[i] * (a * cs - sn * kb);
+            }
+        }
+    }
+    static __device__ __forceinline__ void flush(const Acc &c, const FieldParams &F, const AdjParams &A) {
+#pragma unroll
+        for (int i = 0; i < SMP_MAX_WAVES; ++i) {
+            if (i < F.n_waves) {
+                atomicAdd(A.grad + i, double(c.ga[i]));
+                atomicAdd(A.grad + F.n_waves + i, double(c.gp[i]));
+            }
+        }
+    }
+};
+
+// Tricubic B-spline n = sum_taps c w_x w_y w_z (the coefficient mean is stored apart, which is the
+// same function because the weights sum to 1). dJ/dc for each of the 64 taps is
+// a W + b . grad W, scattered with double atomics into the N0 x N1 x N2 gradient grid (taps outside
+// the grid land on their mirrored coefficient, as they are read). B-spline second-derivative
+// weights: (1 - f, 3f - 2, 1 - 3f, f).
+__device__ __forceinline__ void bspline_dd(float t, float dd[4]) {
+    float f = t - floorf(t);
+    dd[0] = 1.0f - f;
+    dd[1] = 3.0f * f - 2.0f;
+    dd[2] = 1.0f - 3.0f * f;
+    dd[3] = f;
+}
+template <> struct FieldAdj<FK_SPLINE> {
+    struct Acc {};
+    static __device__ __forceinline__ void clear(Acc &) {}
+    static __device__ __forceinline__ void taps(const FieldParams &F, float3 p, float wx[4], float wy[4], float wz[4],
+                                                float dx[4], float dy[4], float dz[4], float ddx[4], float ddy[4],
+                                                float ddz[4], int ix[4], int iy[4], int iz[4]) {
+        const float t0 = (p.x - F.xmin[0]) * F.xres[0], t1 = (p.y - F.xmin[1]) * F.xres[1], t2 = (p.z - F.xmin[2]) * F.xres[2];
+        bspline_weights(t0, wx, dx);
+        bspline_weights(t1, wy, dy);
+        bspline_weights(t2, wz, dz);
+        bspline_dd(t0, ddx);
+        bspline_dd(t1, ddy);
+        bspline_dd(t2, ddz);
+        const int bx = int(floorf(t0)) - 1, by = int(floorf(t1)) - 1, bz = int(floorf(t2)) - 1;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            ix[q] = spline_wrap(bx + q, F.N[0]);
+            iy[q] = spline_wrap(by + q, F.N[1]) * F.N[0];
+            iz[q] = spline_wrap(bz + q, F.N[2]) * F.N[0] * F.N[1];
+        }
+    }
+    static __device__ __forceinline__ void eval_h(const FieldParams &F, float3 p, float, float &n, float3 &g, float H[6]) {
+#pragma unroll
+        for (int j = 0; j < 6; ++j) H[j] = 0.0f;
+        if (in_gap(F, p)) { n = F.n_o; g = f3(0.0f, 0.0f, 0.0f); return; }
+        float wx[4], wy[4], wz[4], dx[4], dy[4], dz[4], ddx[4], ddy[4], ddz[4];
+        int ix[4], iy[4], iz[4];
+        taps(F, p, wx, wy, wz, dx, dy, dz, ddx, ddy, ddz, ix, iy, iz);
+        float v = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
+        float hxx = 0.0f, hyy = 0.0f, hzz = 0.0f, hxy = 0.0f, hxz = 0.0f, hyz = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const float *row = F.coeff + iz[c] + iy[b];
+                const float r0 = __ldg(row + ix[0]), r1 = __ldg(row + ix[1]), r2 = __ldg(row + ix[2]), r3 = __ldg(row + ix[3]);
+                const float sv = r0 * wx[0] + r1 * wx[1] + r2 * wx[2] + r3 * wx[3];
+                const float sd = r0 * dx[0] + r1 * dx[1] + r2 * dx[2] + r3 * dx[3];
+                const float sdd = r0 * ddx[0] + r1 * ddx[1] + r2 * ddx[2] + r3 * ddx[3];
+                const float yz = wy[b] * wz[c], dyz = dy[b] * wz[c], ydz = wy[b] * dz[c];
+                v += sv * yz;
+                gx += sd * yz; gy += sv * dyz; gz += sv * ydz;
+                hxx += sdd * yz; hyy += sv * ddy[b] * wz[c]; hzz += sv * wy[b] * ddz[c];
+                hxy += sd * dyz; hxz += sd * ydz; hyz += sv * dy[b] * dz[c];
+            }
+        }
+        const float r0 = F.xres[0], r1 = F.xres[1], r2 = F.xres[2];
+        n = F.spline_base + v;
+        g = f3(gx * r0, gy * r1, gz * r2);
+        H[0] = hxx * r0 * r0; H[1] = hyy * r1 * r1; H[2] = hzz * r2 * r2;
+        H[3] = hxy * r0 * r1; H[4] = hxz * r0 * r2; H[5] = hyz * r1 * r2;
+    }
+    static __device__ __forceinline__ void theta(const FieldParams &F, float3 p, float, float a, float3 b, Acc &, const AdjParams &A) {
+        if (in_gap(F, p)) return;
+        float wx[4], wy[4], wz[4], dx[4], dy[4], dz[4], ddx[4], ddy[4], ddz[4];
+        int ix[4], iy[4], iz[4];
+        taps(F, p, wx, wy, wz, dx, dy, dz, ddx, ddy, ddz, ix, iy, iz);
+        const float bx = b.x * F.xres[0], by = b.y * F.xres[1], bz = b.z * F.xres[2];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float ar = a * wy[q] * wz[c] + by * dy[q] * wz[c] + bz * wy[q] * dz[c];
+                const float br = bx * wy[q] * wz[c];
+                double *row = A.grad + iz[c] + iy[q];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) atomicAdd(row + ix[i], double(ar * wx[i] + br * dx[i]));
+            }
+        }
+    }
+    static __device__ __forceinline__ void flush(const Acc &, const FieldParams &, const AdjParams &) {}
+};
+
+// ---- replay hook: checkpoints (phase A), stop at a segment's end (phase B), splat capture ----------
+struct AdjHook {
+    static constexpr bool on = true;
+    int record;                // phase A: record checkpoints, never stop
+    int stop_ev;               // phase B: stop at the entry of this event
+    AdjVertex *v;              // this thread's checkpoints
+    int nv, vcap, overflow;
+    int seg_len, max_seg;      // trajectory entries of the current segment / the longest move
+    int splat;                 // a splat happened in this segment
+    float3 sp;                 // its sensor point, path length, depth, value
+    double spl;
+    int sdepth;
+    float sval;
+    // a segment ends at each hook: the direct march at EV_SCATTER, a move at EV_VERTEX, a
+    // connection at EV_SCATTER_ONCE. A move too long for the buffer drops the photon (everything
+    // after it depends on it); a sensor march too long is skipped on its own.
+    __device__ void boundary(int ev) {
+        if (ev == EV_VERTEX) max_seg = max(max_seg, seg_len);
+        seg_len = 0;
+    }
+    __device__ void put(int k, const Lane &L) {
+        AdjVertex &c = v[k];
+        c.pos[0] = L.pos.x; c.pos[1] = L.pos.y; c.pos[2] = L.pos.z;
+        c.dir[0] = L.dir.x; c.dir[1] = L.dir.y; c.dir[2] = L.dir.z;
+        c.total_dist = L.totalDist;
+        c.depth = L.depth;
+        c.total = L.total;
+        c.draws_v = L.draws; c.steps_v = L.steps;
+        c.draws_so = L.draws; c.steps_so = L.steps;
+    }
+    __device__ bool at(Lane &L, int ev) {
+        if (!record) return ev == stop_ev;
+        boundary(ev);
+        if (ev == EV_SCATTER) {
+            put(0, L);
+            nv = 1;
+        } else if (ev == EV_VERTEX) {
+            if (nv < vcap) put(nv, L);
+            else overflow = 1;
+            ++nv;
+        } else if (ev == EV_SCATTER_ONCE && nv - 1 < vcap && nv >= 1) {
+            v[nv - 1].draws_so = L.draws;
+            v[nv - 1].steps_so = L.steps;
+        }
+        return false;
+    }
+    __device__ void splatted(const Lane &, float3 p, double pl, int depth, float val) {
+        splat = 1; sp = p; spl = pl; sdepth = depth; sval = val;
+    }
+};
+
+// Position the lane's Philox stream at draw index d (draw k uses word k % 4 of block k / 4).
+__device__ __forceinline__ void rng_seek(Lane &L, const KParams &P, int d) {
+    L.rblk = unsigned(d >> 2);
+    L.rhave = 0;
+    L.draws = d & ~3;
+    for (int i = 0; i < (d & 3); ++i) (void)draw(L, P);
+}
+
+__device__ __forceinline__ void traj_put(const AdjParams &A, int lane, int i, float4 e) {
+    if (i < A.tcap) A.traj[size_t(i) * A.lanes + lane] = e;
+}
+__device__ __forceinline__ float4 traj_get(const AdjParams &A, int lane, int i) {
+    return A.traj[size_t(i) * A.lanes + lane];
+}
+
+// Run the lane's events from `ev` and every march they start, until the hook stops them
+// (ST_HOOK) or the photon ends (ST_FETCH). With `rec`, the segment's points go to the trajectory
+// buffer: its start point, each accepted step's end point with its step size, and a marker at
+// every face reflection between two of its marches. h.seg_len counts the entries either way.
+template <int FK>
+__device__ __forceinline__ int replay(Lane &L, const KParams &P, int ev, AdjHook &h, const AdjParams &A, int lane,
+                                      bool rec, float3 &md_start, long long &steps) {
+    bool first = true;
+    for (;;) {
+        const int st = run_events<FK, AdjHook>(L, P, ev, &h);
+        if (st != ST_MARCH) return st;
+        if (rec) {
+            if (first) { traj_put(A, lane, h.seg_len, make_float4(L.mp.x, L.mp.y, L.mp.z, 0.0f)); md_start = L.md; }
+            else traj_put(A, lane, h.seg_len, make_float4(0.0f, 0.0f, 0.0f, -1.0f));
+        }
+        ++h.seg_len;
+        first = false;
+        for (;;) {
+            const float3 q = L.mp;
+            const bool end = march_step<FK>(L, P);
+            ++steps;
+            if (q.x != L.mp.x || q.y != L.mp.y || q.z != L.mp.z) {
+                if (rec) traj_put(A, lane, h.seg_len, make_float4(L.mp.x, L.mp.y, L.mp.z, L.cur));
+                ++h.seg_len;
+            }
+            if (end) break;
+        }
+        ev = EV_MARCH_END;
+    }
+}
+
+__device__ __forceinline__ int face_axis(float3 nf) { return nf.x != 0.0f ? 0 : (nf.y != 0.0f ? 1 : 2); }
+__device__ __forceinline__ float3 reflect_n(float3 v, float3 nf) { return sub(v, mul(nf, 2.0f * dot3(v, nf))); }
+__device__ __forceinline__ void add_axis(float3 &v, int ax, float x) {
+    if (ax == 0) v.x += x; else if (ax == 1) v.y += x; else v.z += x;
+}
+
+// Backward sweep over one recorded segment (entries [0, nent) of this thread's buffer).
+// In:  (Pa, Da) adjoints of the segment's end position and optical direction, a_end the adjoint of
+//      n at the end point, T the adjoint of each face crossing's arc-length shift, face_end whether
+//      the last march ends on a face (connections, direct) or at its sampled distance (moves;
+//      then T is derived here from the end adjoints), md_end the end direction.
+// Out: (P, D) adjoints of the start position (field terms included) and start direction, with the
+//      start point's parameter cotangent (a0, b0) left to the caller, and n, grad n there.
+struct SweepOut { float3 P, D, b0, g0; float a0, n0; };
+
+template <int FK>
+__device__ __forceinline__ SweepOut sweep(const KParams &P, const AdjParams &A, int lane, int nent, float3 md_end,
+                                          float3 Pa, float3 Da, float a_end, float T, bool face_end, float s,
+                                          typename FieldAdj<FK>::Acc &acc, long long &pts) {
+    const FieldParams &F = P.field;
+    int i = nent - 1;
+    float4 e = traj_get(A, lane, i);
+    float n_k, H[6];
+    float3 g_k;
+    float3 d = md_end;
+    FieldAdj<FK>::eval_h(F, f3(e.x, e.y, e.z), s, n_k, g_k, H);
+    {
+        const float3 u = divs(d, n_k);
+        const float At = dot3(u, Pa) + dot3(g_k, Da) + dot3(g_k, u) * a_end;
+        if (face_end) {
+            const int ax = face_axis(face_normal(P, f3(e.x, e.y, e.z)));
+            add_axis(Pa, ax, -(At + T) / comp(u, ax));
+        } else {
+            T = -At;        // each earlier face crossing delays the sampled end by its own shift
+        }
+    }
+    // second kick of the last step, and the end point's own use of n
+    {
+        const float3 b = mul(Da, 0.5f * e.w);
+        Pa = add(Pa, add(mul(g_k, a_end), hmul(H, b)));
+        FieldAdj<FK>::theta(F, f3(e.x, e.y, e.z), s, a_end, b, acc, A);
+    }
+    SweepOut o;
+    for (;;) {
+        const float c = e.w, hh = 0.5f * c;
+        int j = i - 1;
+        if (j < 0) break;                       // no start entry: malformed segment, give up on it
+        float4 pe = traj_get(A, lane, j);
+        const bool junction = pe.w < 0.0f;
+        if (junction) {
+            j -= 1;
+            if (j < 0) break;
+            pe = traj_get(A, lane, j);
+        }
+        const float3 pp = f3(pe.x, pe.y, pe.z);
+        float n1;
+        float3 g1;
+        FieldAdj<FK>::eval_h(F, pp, s, n1, g1, H);
+        const float3 dh = sub(d, mul(g_k, hh));
+        const float3 dprev = sub(dh, mul(g1, hh));
+        const float q = c / n1;
+        const float3 Dh = add(Da, mul(Pa, q));
+        const float a1 = -(q / n1) * dot3(dh, Pa);
+        float3 b1 = mul(Dh, hh);
+        Pa = add(Pa, add(mul(g1, a1), hmul(H, b1)));
+        Da = Dh;
+        d = dprev;
+        g_k = g1;
+        ++pts;
+        if (junction) {
+            // the previous march ended on a face and reflected: undo the reflection, then the crossing
+            const float3 nf = face_normal(P, pp);
+            Da = reflect_n(Da, nf);
+            d = reflect_n(d, nf);
+            const float3 u = divs(d, n1);
+            const int ax = face_axis(nf);
+            const float At = dot3(u, Pa) + dot3(g1, Da) + T;
+            add_axis(Pa, ax, -At / comp(u, ax));
+        }
+        if (pe.w == 0.0f) {             // the segment's start point
+            o.P = Pa; o.D = Da; o.a0 = a1; o.b0 = b1; o.g0 = g1; o.n0 = n1;
+            return o;
+        }
+        // second kick of the previous step
+        const float3 b2 = mul(Da, 0.5f * pe.w);
+        Pa = add(Pa, hmul(H, b2));
+        b1 = add(b1, b2);
+        FieldAdj<FK>::theta(F, pp, s, a1, b1, acc, A);
+        i = j;
+        e = pe;
+    }
+    o.P = f3(0.0f, 0.0f, 0.0f); o.D = o.P; o.b0 = o.P; o.g0 = o.P; o.a0 = 0.0f; o.n0 = 1.0f;
+    return o;
+}
+
+// ---- the splat's value as a function of the march's end state --------------------------------------
+// Inputs (the order of the derivative components): end position p (0-2), end direction md (3-5),
+// n at the end (6), the connection's marched distance d2s (7), the vertex direction dv (8-10, used
+// by the Henyey-Greenstein factor of a connection). Follows run_events' exit at the sensor face
+// (directTracing photon.cpp:41-87; addEnergyInParticle scene.cpp:866-946; propagate_till_sensor
+// camera.cpp:54-75 without a lens) and the bilinear split of addEnergyToImage with the base
+// pixel (ix, iy) held fixed. Returns dJ/d(inputs) for J = value * sum_taps G w.
+__device__ __noinline__ void sensor_grad(const KParams &P, int X, float weight, float sigma_t, float g, bool connect,
+                                         float3 p, float3 md, float n, float d2s, float3 dv, int ix, int iy,
+                                         float G00, float G10, float G01, float G11, float *out) {
+    typedef Dual<11> D;
+    D px = dvar<11>(p.x, 0), py = dvar<11>(p.y, 1), pz = dvar<11>(p.z, 2);
+    D mx = dvar<11>(md.x, 3), my = dvar<11>(md.y, 4), mz = dvar<11>(md.z, 5);
+    D nn = dvar<11>(n, 6), dd = dvar<11>(d2s, 7);
+    D l = dsqrt(mx * mx + my * my + mz * mz);
+    D sx = mx / l, sy = my / l, sz = mz / l;
+    D rx = sx, ry = sy, rz = sz;
+    D fw = dc<11>(1.0f);
+    if (n > 1.0f) {
+        rx = rx / nn;
+        D lr = dsqrt(rx * rx + ry * ry + rz * rz);
+        rx = rx / lr; ry = ry / lr; rz = rz / lr;
+        D eta = 1.0f / nn;
+        D F = dc<11>(0.0f);
+        if (!(fabsf(eta.v - 1.0f) < kEps * fmaxf(1.0f, fabsf(eta.v)))) {
+            D Rs = (sx - eta * rx) / (sx + eta * rx);
+            D Rp = (rx - eta * sx) / (rx + eta * sx);
+            F = 0.5f * (Rs * Rs + Rp * Rp);
+        }
+        fw = (1.0f - F) / nn / nn;
+    }
+    D val = weight * dexp(dd * (-sigma_t)) * fw;
+    if (connect) {
+        const float cx = P.cam_dir[0], cy = P.cam_dir[1], cz = P.cam_dir[2];
+        D fore = (rx * cx + ry * cy + rz * cz) / (sx * cx + sy * cy + sz * cz);
+        D vx = dvar<11>(dv.x, 8), vy = dvar<11>(dv.y, 9), vz = dvar<11>(dv.z, 10);
+        D il = 1.0f / dsqrt(vx * vx + vy * vy + vz * vz);
+        D c = (vx * il) * sx + (vy * il) * sy + (vz * il) * sz;
+        D b = (1.0f + g * g) - (2.0f * g) * c;
+        D hg = ((1.0f / (4.0f * 3.14159265358979f)) * (1.0f - g * g)) / (b * dsqrt(b));
+        val = val * 6.28318548202514648f * hg * fore;
+    }
+    D dist = (P.cam_origin[0] - px) / rx;
+    D qx = px + rx * dist, qy = py + ry * dist, qz = pz + rz * dist;
+    D x = ((qx * P.cam_h[0] + qy * P.cam_h[1] + qz * P.cam_h[2]) - P.cam_origin[1]) / P.cam_plane[0];
+    D y = ((qx * P.cam_v[0] + qy * P.cam_v[1] + qz * P.cam_v[2]) - P.cam_origin[2]) / P.cam_plane[1];
+    D fx = (x + 0.5f) * float(X) - float(ix);
+    D fy = (y + 0.5f) * float(P.Y) - float(iy);
+    D gx = 1.0f - fx, gy = 1.0f - fy;
+    D w = gx * gy * G00 + fx * gy * G10 + gx * fy * G01 + fx * fy * G11;
+    D J = val * w;
+#pragma unroll
+    for (int i = 0; i < 11; ++i) out[i] = J.d[i];
+}
+
+// Jacobian^T of the scatterOnce direction update (photon.cpp:20-38: v' = |v| HG(v/|v|), the HG
+// sample drawn in the frame of util::coordinateSystem, util.h:17-27) applied to D.
+__device__ __noinline__ float3 hg_vjp(float3 v, float cosT, float sinT, float cP, float sP, float3 Dout) {
+    typedef Dual<3> D;
+    D x = dvar<3>(v.x, 0), y = dvar<3>(v.y, 1), z = dvar<3>(v.z, 2);
+    D mag = dsqrt(x * x + y * y + z * z);
+    D r = 1.0f / mag;
+    D ix = x * r, iy = y * r, iz = z * r;
+    D ax, ay, az, bx, by, bz;     // ay-axis (b) of the frame, then ax = ay x in
+    if (fabsf(ix.v) > fabsf(iy.v)) {
+        D inv = 1.0f / dsqrt(ix * ix + iz * iz);
+        bx = iz * inv; by = dc<3>(0.0f); bz = dc<3>(0.0f) - ix * inv;
+    } else {
+        D inv = 1.0f / dsqrt(iy * iy + iz * iz);
+        bx = dc<3>(0.0f); by = iz * inv; bz = dc<3>(0.0f) - iy * inv;
+    }
+    ax = by * iz - bz * iy; ay = bz * ix - bx * iz; az = bx * iy - by * ix;
+    const float u = sinT * cP, w = sinT * sP;
+    D ox = (ax * u + bx * w + ix * cosT) * mag;
+    D oy = (ay * u + by * w + iy * cosT) * mag;
+    D oz = (az * u + bz * w + iz * cosT) * mag;
+    return f3(Dout.x * ox.d[0] + Dout.y * oy.d[0] + Dout.z * oz.d[0],
+              Dout.x * ox.d[1] + Dout.y * oy.d[1] + Dout.z * oz.d[1],
+              Dout.x * ox.d[2] + Dout.y * oy.d[2] + Dout.z * oz.d[2]);
+}
+
+__device__ __forceinline__ float g_at(const AdjParams &A, int x, int y, int z) {
+    if (x < 0 || x >= A.X || y < 0 || y >= A.Y || z < 0 || z >= A.Z) return 0.0f;
+    return float(__ldg(A.G + (size_t(z) * A.Y + y) * A.X + x));
+}
+
+__device__ __forceinline__ void restore(Lane &L, const KParams &P, const AdjVertex &c, bool at_vertex) {
+    L.pos = f3(c.pos[0], c.pos[1], c.pos[2]);
+    L.dir = f3(c.dir[0], c.dir[1], c.dir[2]);
+    L.total = c.total;
+    L.totalDist = c.total_dist;
+    L.depth = c.depth;
+    L.end = 0;
+    L.steps = at_vertex ? c.steps_v : c.steps_so;
+    rng_seek(L, P, at_vertex ? c.draws_v : c.draws_so);
+}
+
+// Jobs of one photon's backward pass, in order: connection from vertex K, the move into vertex K,
+// ..., connection from vertex 1, the move into vertex 1 (from the source), the direct march, the
+// source direction n(p0) omega0.
+enum AdjJob : int { JOB_FWD = 0, JOB_CONN = 1, JOB_MOVE = 2, JOB_DIRECT = 3, JOB_SOURCE = 4, JOB_END = 5 };
+
+// One thread per photon at a time, photons from a global counter. P is the render's parameter
+// block with P.X = 0 (replays write no film); A carries the film shape, dJ/dfilm and the buffers.
+template <int FK>
+__global__ void __launch_bounds__(128) adjoint_kernel(const __grid_constant__ KParams P, const __grid_constant__ AdjParams A) {
+    const int lane = blockIdx.x * blockDim.x + threadIdx.x;
+    if (lane >= A.lanes) return;
+    const FieldParams &F = P.field;
+    AdjHook h;
+    h.v = A.verts + size_t(lane) * A.vcap;
+    h.vcap = A.vcap;
+    Lane L;
+    L.tab = nullptr;
+    L.inst = nullptr;
+    L.s = 0.0f;
+    long long fsteps = 0, rsteps = 0, pts = 0;
+    unsigned long long nph = 0, ndrop = 0, nabort = 0, nspl = 0, nskip = 0;
+    const float albedo = P.albedo;
+    const int rr_draw = (albedo > 0.0f && albedo < 1.0f) ? 1 : 0;
+    for (;;) {
+        const long long k = (long long)atomicAdd(A.cnt + ADJ_NEXT, 1ull);
+        if (k >= P.n_photons) break;
+        const long long idx = P.first_photon + k;
+        typename FieldAdj<FK>::Acc acc;
+        FieldAdj<FK>::clear(acc);
+        float3 lp = f3(0.0f, 0.0f, 0.0f), ld = f3(0.0f, 0.0f, 0.0f);   // adjoint of (pos, dir) at vertex kv
+        int job = JOB_FWD, kv = 0, K = 0;
+        float s = 0.0f;
+        while (job != JOB_END) {
+            // ---- set up the segment ----
+            int ev = EV_NEW;
+            bool rec = true;
+            h.seg_len = 0;
+            h.splat = 0;
+            h.record = 0;
+            if (job == JOB_FWD) {
+                L.idx = idx;
+                L.end = 0;                          // run_events tests the end code before EV_NEW
+                h.record = 1; h.nv = 0; h.overflow = 0; h.max_seg = 0;
+                rec = false;
+            } else if (job == JOB_CONN) {
+                const AdjVertex &c = h.v[kv];
+                restore(L, P, c, true);
+                L.mp = L.pos;
+                Field<FK>::eval(F, L.tab, L.mp, s, L.mn, L.mg);
+                ev = EV_VERTEX;
+                h.stop_ev = EV_SCATTER_ONCE;
+            } else if (job == JOB_MOVE) {
+                if (lp.x == 0.0f && lp.y == 0.0f && lp.z == 0.0f && ld.x == 0.0f && ld.y == 0.0f && ld.z == 0.0f) {
+                    // nothing downstream of this move depends on it
+                    if (kv == 1) job = P.use_direct ? JOB_DIRECT : JOB_SOURCE;
+                    else { --kv; job = JOB_CONN; }
+                    continue;
+                }
+                restore(L, P, h.v[kv - 1], false);
+                ev = kv == 1 ? EV_SCATTER : EV_SCATTER_ONCE;
+                h.stop_ev = EV_VERTEX;
+            } else if (job == JOB_DIRECT) {
+                L.idx = idx;
+                L.end = 0;
+                h.stop_ev = EV_SCATTER;
+            }
+            float3 md0 = f3(0.0f, 0.0f, 0.0f);
+            int st = ST_FETCH;
+            if (job != JOB_SOURCE) st = replay<FK>(L, P, ev, h, A, lane, rec, md0, job == JOB_FWD ? fsteps : rsteps);
+
+            // ---- differentiate it ----
+            if (job == JOB_FWD) {
+                if (L.end == SMP_END_STEP_CAP || L.end == SMP_END_NAN) { ++nabort; break; }
+                if (h.overflow || h.max_seg > A.tcap) { ++ndrop; break; }
+                ++nph;
+                s = L.s;
+                K = h.nv - 1;
+                if (h.nv == 0) break;                       // never reached the scatter stage
+                if (K >= 1) { kv = K; job = JOB_CONN; }
+                else job = P.use_direct ? JOB_DIRECT : JOB_SOURCE;
+                continue;
+            }
+            if (job != JOB_SOURCE && st != ST_HOOK) {
+                atomicAdd(A.cnt + ADJ_MISMATCH, 1ull);
+                atomicAdd(A.cnt + (job == JOB_CONN ? ADJ_MIS_CONN : job == JOB_MOVE ? ADJ_MIS_MOVE : ADJ_MIS_DIRECT), 1ull);
+                break;
+            }
+            if (job == JOB_MOVE) {
+                const AdjVertex &c = h.v[kv];
+                const bool pos_ok = L.pos.x == c.pos[0] && L.pos.y == c.pos[1] && L.pos.z == c.pos[2];
+                const bool dir_ok = L.dir.x == c.dir[0] && L.dir.y == c.dir[1] && L.dir.z == c.dir[2];
+                if (!pos_ok || !dir_ok) {
+                    atomicAdd(A.cnt + ADJ_MISMATCH, 1ull);
+                    atomicAdd(A.cnt + (pos_ok ? ADJ_MIS_DIR : ADJ_MIS_POS), 1ull);
+                    break;
+                }
+            }
+            bool do_sweep = false, face_end = true;
+            float3 Pa = f3(0.0f, 0.0f, 0.0f), Da = Pa, Ddir = Pa;
+            float a_end = 0.0f, T = 0.0f;
+            if ((job == JOB_CONN || job == JOB_DIRECT) && h.splat) {
+                int ix, iy, iz;
+                float fx, fy;
+                if (splat_bin(P, A.X, h.sp, h.spl, h.sdepth, ix, iy, iz, fx, fy)) {
+                    const float G00 = g_at(A, ix, iy, iz), G10 = g_at(A, ix + 1, iy, iz);
+                    const float G01 = g_at(A, ix, iy + 1, iz), G11 = g_at(A, ix + 1, iy + 1, iz);
+                    if (G00 != 0.0f || G10 != 0.0f || G01 != 0.0f || G11 != 0.0f) {
+                        float gr[11];
+                        sensor_grad(P, A.X, P.weight, P.sigma_t, P.g, job == JOB_CONN, L.mp, L.md, L.mn, L.d2s, L.dir,
+                                    ix, iy, G00, G10, G01, G11, gr);
+                        Pa = f3(gr[0], gr[1], gr[2]);
+                        Da = f3(gr[3], gr[4], gr[5]);
+                        a_end = gr[6];
+                        T = gr[7];
+                        Ddir = f3(gr[8], gr[9], gr[10]);
+                        do_sweep = true;
+                        ++nspl;
+                    }
+                }
+            } else if (job == JOB_MOVE) {
+                Pa = lp; Da = ld;
+                face_end = false;
+                do_sweep = true;
+            }
+            if (do_sweep && h.seg_len >= 2 && h.seg_len <= A.tcap) {
+                const SweepOut o = sweep<FK>(P, A, lane, h.seg_len, L.md, Pa, Da, a_end, T, face_end, s, acc, pts);
+                const float4 e0 = traj_get(A, lane, 0);
+                const float3 p0 = f3(e0.x, e0.y, e0.z);
+                if (job == JOB_CONN) {
+                    // md0 = omega n(pos): the start direction's dependence on n at the vertex
+                    const float as = dot3(md0, o.D) / o.n0;
+                    lp = add(lp, add(o.P, mul(o.g0, as)));
+                    ld = add(ld, Ddir);
+                    FieldAdj<FK>::theta(F, p0, s, o.a0 + as, o.b0, acc, A);
+                } else if (job == JOB_MOVE) {
+                    FieldAdj<FK>::theta(F, p0, s, o.a0, o.b0, acc, A);
+                    lp = o.P;
+                    if (kv >= 2) {
+                        // the move began with v' = |v| HG(v / |v|) at vertex kv - 1
+                        const AdjVertex &c = h.v[kv - 1];
+                        rng_seek(L, P, c.draws_so + rr_draw);
+                        const float u1 = draw(L, P), u2 = draw(L, P);
+                        const float gg = P.g;
+                        float cosT;
+                        if (fabsf(gg) < kEps) cosT = 1.0f - 2.0f * u1;
+                        else {
+                            const float sq = (1.0f - gg * gg) / (1.0f - gg + 2.0f * gg * u1);
+                            cosT = (1.0f + gg * gg - sq * sq) / (2.0f * gg);
+                        }
+                        const float sinT = sqrtf(fmaxf(0.0f, 1.0f - cosT * cosT));
+                        float sP, cP;
+                        sincos_red(6.28318548202514648f * u2, sP, cP);
+                        ld = hg_vjp(f3(c.dir[0], c.dir[1], c.dir[2]), cosT, sinT, cP, sP, o.D);
+                    } else {
+                        ld = o.D;
+                    }
+                } else {   // JOB_DIRECT: starts from the source state, as the first move does
+                    lp = add(lp, o.P);
+                    ld = add(ld, o.D);
+                    FieldAdj<FK>::theta(F, p0, s, o.a0, o.b0, acc, A);
+                }
+            } else if (do_sweep) {
+                ++nskip;                                // a sensor march longer than the buffer
+            }
+            if (job == JOB_SOURCE) {
+                // dir0 = n(p0) omega0 (photon.cpp:329)
+                const AdjVertex &c = h.v[0];
+                const float3 p0 = f3(c.pos[0], c.pos[1], c.pos[2]);
+                float n0, H[6];
+                float3 g0;
+                FieldAdj<FK>::eval_h(F, p0, s, n0, g0, H);
+                const float as = (c.dir[0] * ld.x + c.dir[1] * ld.y + c.dir[2] * ld.z) / n0;
+                FieldAdj<FK>::theta(F, p0, s, as, f3(0.0f, 0.0f, 0.0f), acc, A);
+                job = JOB_END;
+            } else if (job == JOB_CONN) {
+                job = JOB_MOVE;
+            } else if (job == JOB_MOVE) {
+                if (kv == 1) job = P.use_direct ? JOB_DIRECT : JOB_SOURCE;
+                else { --kv; job = JOB_CONN; }
+            } else {
+                job = JOB_SOURCE;
+            }
+        }
+        FieldAdj<FK>::flush(acc, F, A);
+    }
+    atomicAdd(A.cnt + ADJ_PHOTONS, nph);
+    atomicAdd(A.cnt + ADJ_DROPPED, ndrop);
+    atomicAdd(A.cnt + ADJ_ABORTED, nabort);
+    atomicAdd(A.cnt + ADJ_STEPS_FWD, (unsigned long long)fsteps);
+    atomicAdd(A.cnt + ADJ_STEPS_REPLAY, (unsigned long long)rsteps);
+    atomicAdd(A.cnt + ADJ_POINTS, (unsigned long long)pts);
+    atomicAdd(A.cnt + ADJ_SPLATS, nspl);
+    atomicAdd(A.cnt + ADJ_SKIPPED, nskip);
+}
+
+}  // namespace smp

@@ -20,6 +20,7 @@
 #include "kparams.h"
 #include "march.cuh"
 #include "wavefront.cuh"
+#include "adjoint.cuh"
 
 using namespace smp;
 
@@ -538,6 +539,7 @@ size_t smp_sizeof(const char *t) {
     if (!std::strcmp(t, "smp_photon_record")) return sizeof(smp_photon_record);
     if (!std::strcmp(t, "smp_splat_record")) return sizeof(smp_splat_record);
     if (!std::strcmp(t, "smp_instance_desc")) return sizeof(smp_instance_desc);
+    if (!std::strcmp(t, "smp_adjoint_stats")) return sizeof(smp_adjoint_stats);
     return 0;
 }
 
@@ -1298,6 +1300,142 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
     cudaFree(d_first);
     cudaFree(d_tabs);
     cudaFree(d_films);
+    smp_plan_destroy(p);
+    g_last_error = err;
+    return rc;
+}
+
+// ---- adjoint ------------------------------------------------------------------------------------
+int64_t smp_adjoint_param_count(const smp_field_desc *f) {
+    if (!f) return set_error(SMP_ERR_BAD_ARG, "NULL field");
+    if (f->type == SMP_FIELD_PLANEWAVE) {
+        if (f->n_waves < 1 || f->n_waves > SMP_MAX_WAVES) return set_error(SMP_ERR_BAD_ARG, "n_waves %d", f->n_waves);
+        return 2 * int64_t(f->n_waves);
+    }
+    if (f->type == SMP_FIELD_SPLINE) {
+        if (f->grid_n[0] < 2 || f->grid_n[1] < 2 || f->grid_n[2] < 2) return set_error(SMP_ERR_BAD_ARG, "bad spline grid");
+        return int64_t(f->grid_n[0]) * f->grid_n[1] * f->grid_n[2];
+    }
+    return set_error(SMP_ERR_UNSUPPORTED, "the adjoint is built for plane-wave and spline fields");
+}
+
+typedef void (*AdjFn)(KParams, AdjParams);
+static AdjFn adjoint_fn(int fk) {
+    switch (fk) {
+        case FK_PLANEWAVE: return adjoint_kernel<FK_PLANEWAVE>;
+        case FK_SPLINE: return adjoint_kernel<FK_SPLINE>;
+        default: return nullptr;
+    }
+}
+
+static int env_int(const char *name, int def, int lo, int hi) {
+    const char *v = std::getenv(name);
+    if (!v) return def;
+    return std::max(lo, std::min(hi, std::atoi(v)));
+}
+
+int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, int64_t weight_photons,
+                     const double *dJ_dfilm, double *grad_out, smp_adjoint_stats *stats_out) {
+    if (!plan || !dJ_dfilm || !grad_out || n_photons < 0 || first_photon < 0)
+        return set_error(SMP_ERR_BAD_ARG, "bad adjoint arguments");
+    if (weight_photons <= 0) return set_error(SMP_ERR_BAD_ARG, "weight_photons must be positive");
+    const int64_t np = smp_adjoint_param_count(&plan->field);
+    if (np < 0) return int(np);
+    AdjFn fn = adjoint_fn(plan->fk);
+    if (!fn) return set_error(SMP_ERR_UNSUPPORTED, "no adjoint for field kind %d", plan->fk);
+    if (plan->kp.rng != SMP_RNG_PHILOX) return set_error(SMP_ERR_UNSUPPORTED, "the adjoint replays Philox streams only");
+    if (plan->kp.src_lens_active || plan->kp.cam_lens_active)
+        return set_error(SMP_ERR_UNSUPPORTED, "the adjoint is built for scenes without lenses");
+    SMP_CUDA(cudaSetDevice(plan->device));
+    int sms = 0, per_sm = 0;
+    SMP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, plan->device));
+    SMP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0));
+    // per-thread buffers: trajectory entries of one segment (16 B each) and vertex checkpoints
+    per_sm = env_int("SMP_ADJ_BLOCKS", std::max(per_sm, 1), 1, 64);
+    const int grid = sms * per_sm;
+    AdjParams a;
+    std::memset(&a, 0, sizeof(a));
+    a.X = plan->kp.X; a.Y = plan->kp.Y; a.Z = plan->kp.Z;
+    a.lanes = grid * kBlock;
+    a.tcap = env_int("SMP_ADJ_TCAP", 8192, 16, 1 << 24);
+    a.vcap = env_int("SMP_ADJ_VCAP", 256, 2, 1 << 20);
+    const size_t film = size_t(a.X) * a.Y * a.Z;
+    double *d_G = nullptr, *d_grad = nullptr;
+    float4 *d_traj = nullptr;
+    AdjVertex *d_verts = nullptr;
+    unsigned long long *d_cnt = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = SMP_OK;
+    cudaError_t e = cudaMalloc(&d_G, film * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_grad, size_t(np) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_traj, size_t(a.tcap) * a.lanes * sizeof(float4));
+    if (e == cudaSuccess) e = cudaMalloc(&d_verts, size_t(a.vcap) * a.lanes * sizeof(AdjVertex));
+    if (e == cudaSuccess) e = cudaMalloc(&d_cnt, ADJ_COUNT * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemcpy(d_G, dJ_dfilm, film * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(d_grad, 0, size_t(np) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(d_cnt, 0, ADJ_COUNT * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    unsigned long long c[ADJ_COUNT] = {0};
+    float ms = 0.0f;
+    if (e != cudaSuccess) {
+        rc = set_error(e == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "adjoint setup: %s", cudaGetErrorString(e));
+    } else if (n_photons > 0) {
+        a.G = d_G; a.grad = d_grad; a.traj = d_traj; a.verts = d_verts; a.cnt = d_cnt;
+        KParams k = plan->kp;
+        k.weight = photon_weight(plan->scene, weight_photons);
+        k.first_photon = first_photon;
+        k.n_photons = n_photons;
+        k.records = nullptr;
+        k.stream = nullptr;
+        k.offsets = nullptr;
+        k.X = 0;                          // replays add nothing to any film
+        cudaEventRecord(e0, 0);
+        fn<<<grid, kBlock>>>(k, a);
+        e = cudaGetLastError();
+        cudaEventRecord(e1, 0);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e == cudaSuccess) e = cudaMemcpy(grad_out, d_grad, size_t(np) * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(c, d_cnt, sizeof(c), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = set_error(SMP_ERR_CUDA, "adjoint: %s", cudaGetErrorString(e));
+    } else {
+        std::memset(grad_out, 0, size_t(np) * sizeof(double));
+    }
+    if (stats_out) {
+        stats_out->photons = (int64_t)c[ADJ_PHOTONS];
+        stats_out->dropped = (int64_t)c[ADJ_DROPPED];
+        stats_out->skipped = (int64_t)c[ADJ_SKIPPED];
+        stats_out->aborted = (int64_t)c[ADJ_ABORTED];
+        stats_out->replay_mismatch = (int64_t)c[ADJ_MISMATCH];
+        stats_out->er_steps_forward = (int64_t)c[ADJ_STEPS_FWD];
+        stats_out->er_steps_replay = (int64_t)c[ADJ_STEPS_REPLAY];
+        stats_out->points = (int64_t)c[ADJ_POINTS];
+        stats_out->splats = (int64_t)c[ADJ_SPLATS];
+        stats_out->kernel_ms = ms;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(d_G);
+    cudaFree(d_grad);
+    cudaFree(d_traj);
+    cudaFree(d_verts);
+    cudaFree(d_cnt);
+    if (!rc && c[ADJ_MISMATCH])
+        rc = set_error(SMP_ERR_CUDA, "internal: %llu segment replay(s) diverged from their checkpoint "
+                       "(connection %llu, move %llu, direct %llu, position %llu, direction %llu)",
+                       c[ADJ_MISMATCH], c[ADJ_MIS_CONN], c[ADJ_MIS_MOVE], c[ADJ_MIS_DIRECT], c[ADJ_MIS_POS], c[ADJ_MIS_DIR]);
+    return rc;
+}
+
+int smp_render_adjoint(const smp_scene_desc *scene, const smp_medium_desc *medium, const smp_field_desc *field,
+                       const smp_render_opts *opts, int64_t n_photons, const double *dJ_dfilm, double *grad_out,
+                       smp_adjoint_stats *stats_out) {
+    smp_plan *p = nullptr;
+    int rc = smp_plan_create(scene, medium, field, opts, &p);
+    if (rc) return rc;
+    rc = smp_plan_adjoint(p, 0, n_photons, n_photons > 0 ? n_photons : 1, dJ_dfilm, grad_out, stats_out);
+    std::string err = g_last_error;
     smp_plan_destroy(p);
     g_last_error = err;
     return rc;

@@ -26,7 +26,7 @@ static constexpr unsigned kFull = 0xffffffffu;
 #define SMP_MIN_BLOCKS 4
 #endif
 
-enum LaneState : int { ST_FETCH = 0, ST_EVENT = 1, ST_MARCH = 2, ST_DONE = 3 };
+enum LaneState : int { ST_FETCH = 0, ST_EVENT = 1, ST_MARCH = 2, ST_DONE = 3, ST_HOOK = 4 };
 enum Event : int {
     EV_NEW = 0,          // photon fetched: genRay, scaling, direct or scatter
     EV_MARCH_END = 1,    // a traceTillBlock call finished
@@ -211,6 +211,29 @@ __device__ __forceinline__ void add_pixel(const KParams &P, void *film, int x, i
     }
 }
 
+// Film cell of a splat at sensor point p with path length pl (scene.cpp:782-829) on a film X
+// pixels wide: the bilinear base pixel (ix, iy), its fractions (fx, fy) and the bin iz; false when
+// pl is outside the binned range.
+__device__ __forceinline__ bool splat_bin(const KParams &P, int X, float3 p, double pl, int depth,
+                                          int &ix, int &iy, int &iz, float &fx, float &fy) {
+    float x = dot3(ld3(P.cam_h), p) - P.cam_origin[1];
+    float y = dot3(ld3(P.cam_v), p) - P.cam_origin[2];
+    bool nobin = (P.pl_min == -1.0f) && (P.pl_max == -1.0f);
+    bool inrange = P.fp64 ? (pl > double(P.pl_min) && pl < double(P.pl_max))
+                          : (float(pl) > P.pl_min && float(pl) < P.pl_max);
+    if (!(nobin || inrange)) return false;
+    x = (x / P.cam_plane[0] + 0.5f) * float(X);
+    y = (y / P.cam_plane[1] + 0.5f) * float(P.Y);
+    float flx = floorf(x), fly = floorf(y);
+    ix = int(flx); iy = int(fly);
+    if (P.bounce) iz = depth;
+    else if (nobin) iz = 0;
+    else if (P.fp64) iz = int(floor((pl - double(P.pl_min)) / (double(P.pl_max) - double(P.pl_min)) * double(P.Z)));
+    else iz = int(floorf(((float(pl) - P.pl_min) / (P.pl_max - P.pl_min)) * float(P.Z)));
+    fx = x - flx; fy = y - fly;
+    return true;
+}
+
 __device__ __forceinline__ void splat(Lane &L, const KParams &P, float3 p, double pl, int depth, float val) {
     if (P.records) {
         smp_photon_record *rec = P.records + (L.idx - P.first_photon);
@@ -223,21 +246,9 @@ __device__ __forceinline__ void splat(Lane &L, const KParams &P, float3 p, doubl
         }
     }
     ++L.nspl;
-    float x = dot3(ld3(P.cam_h), p) - P.cam_origin[1];
-    float y = dot3(ld3(P.cam_v), p) - P.cam_origin[2];
-    bool nobin = (P.pl_min == -1.0f) && (P.pl_max == -1.0f);
-    bool inrange = P.fp64 ? (pl > double(P.pl_min) && pl < double(P.pl_max))
-                          : (float(pl) > P.pl_min && float(pl) < P.pl_max);
-    if (!(nobin || inrange)) return;
-    x = (x / P.cam_plane[0] + 0.5f) * float(P.X);
-    y = (y / P.cam_plane[1] + 0.5f) * float(P.Y);
-    float flx = floorf(x), fly = floorf(y);
-    int ix = int(flx), iy = int(fly), iz;
-    if (P.bounce) iz = depth;
-    else if (nobin) iz = 0;
-    else if (P.fp64) iz = int(floor((pl - double(P.pl_min)) / (double(P.pl_max) - double(P.pl_min)) * double(P.Z)));
-    else iz = int(floorf(((float(pl) - P.pl_min) / (P.pl_max - P.pl_min)) * float(P.Z)));
-    float fx = x - flx, fy = y - fly;
+    int ix, iy, iz;
+    float fx, fy;
+    if (!splat_bin(P, P.X, p, pl, depth, ix, iy, iz, fx, fy)) return;
     void *film = med_film(L, P);
     add_pixel(P, film, ix, iy, iz, val * (1.0f - fx) * (1.0f - fy));
     add_pixel(P, film, ix + 1, iy, iz, val * fx * (1.0f - fy));
@@ -397,10 +408,20 @@ __device__ __forceinline__ bool march_step(S &L, const KParams &P) {
 }
 
 // ---- discrete logic between marches ---------------------------------------------------------
+// Observation points for path replay (adjoint.cuh). The render kernels use NoHook, for which every
+// hook call below is compiled out.
+struct NoHook {
+    static constexpr bool on = false;
+    __device__ bool at(Lane &, int) { return false; }
+    __device__ void splatted(const Lane &, float3, double, int, float) {}
+};
+
 // Runs the lane's events until it starts a march (returns ST_MARCH) or its photon ends
-// (returns ST_FETCH).
-template <int FK>
-__device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
+// (returns ST_FETCH). With a hook, h->at(L, ev) is asked at the entry of EV_SCATTER and
+// EV_SCATTER_ONCE and at EV_VERTEX once the depth test has passed; true stops here with ST_HOOK
+// (the lane state is that of the event's entry). h->splatted sees every splat.
+template <int FK, class H = NoHook>
+__device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev, H *h = nullptr) {
     for (;;) {
         if (ev == EV_MARCH_END) {
             if (!P.fp64) L.mtot = double(L.mtotf);
@@ -506,6 +527,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
                             acc_total(L.total, dts, P.fp64);
                             float val = med_weight(L, P) * expf(-med_sigma_t(L, P) * L.d2s) * fw;
                             splat(L, P, p1, L.total, 0, val);
+                            if (H::on) h->splatted(L, p1, L.total, 0, val);
                         }
                     }
                     ev = EV_SCATTER;
@@ -530,6 +552,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
                             float val = med_weight(L, P) * 6.28318548202514648f * expf(-med_sigma_t(L, P) * L.d2s) *
                                         hg_f(med_g(L, P), divs(L.dir, len3(L.dir)), dsen) * fore * fw;
                             splat(L, P, p1, tot, L.depth, val);
+                            if (H::on) h->splatted(L, p1, tot, L.depth, val);
                         }
                     }
                     ev = EV_SCATTER_ONCE;
@@ -562,6 +585,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
             break;
         }
         case EV_SCATTER: {
+            if (H::on && h->at(L, EV_SCATTER)) return ST_HOOK;
             if (!roulette(L, P)) { L.end = SMP_END_NO_SCATTER; ev = EV_FINISH; break; }
             float dist = -med_mfp(L, P) * logf(draw(L, P));
             L.ctx = CTX_MOVE_FIRST;
@@ -580,6 +604,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
                   (P.max_pathlength < 0.0f || L.totalDist <= P.max_pathlength))) {
                 L.end = SMP_END_MAX_DEPTH; ev = EV_FINISH; break;
             }
+            if (H::on && h->at(L, EV_VERTEX)) return ST_HOOK;
             if (P.use_angular && !(double(L.pos.x - P.cam_origin[0]) < 1e-4)) {
                 float3 dts = random_direction(L, P);
                 // mp == pos and (mn, mg) are the field at pos: the move march ended there
@@ -597,6 +622,7 @@ __device__ __forceinline__ int run_events(Lane &L, const KParams &P, int ev) {
             break;
         }
         case EV_SCATTER_ONCE: {
+            if (H::on && h->at(L, EV_SCATTER_ONCE)) return ST_HOOK;
             if (!roulette(L, P)) { L.end = SMP_END_ABSORBED; ev = EV_FINISH; break; }
             float mag = len3(L.dir);
             float3 d1 = hg_sample(L, P, divs(L.dir, mag));

@@ -2,6 +2,7 @@
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
 
 import numpy as np
 
@@ -67,6 +68,23 @@ class Plan:
         st = L.Stats()
         L.check(self.lib.smp_plan_render(self.handle, int(n_photons), _ptr(img), C.byref(st)))
         return img, st
+
+    def adjoint(self, dJ_dfilm: np.ndarray, first: int = 0, n: int | None = None,
+                weight_photons: int | None = None) -> tuple[np.ndarray, L.AdjointStats]:
+        """Gradient of J = sum(dJ_dfilm * film) over the field parameters (`field_params` order)
+        for the film of photons [first, first + n) of this plan's render (weight_photons as in
+        `trace`; each defaults to the other)."""
+        g = np.ascontiguousarray(dJ_dfilm, dtype=np.float64)
+        if g.shape != self.setup.film_shape():
+            raise ValueError(f"dJ_dfilm shape {g.shape} != film {self.setup.film_shape()}")
+        if n is None and weight_photons is None:
+            raise ValueError("give n or weight_photons")
+        n = int(n if n is not None else weight_photons)
+        w = int(weight_photons if weight_photons is not None else n)
+        grad = np.zeros(param_count(self.setup), dtype=np.float64)
+        st = L.AdjointStats()
+        L.check(self.lib.smp_plan_adjoint(self.handle, int(first), n, w, _ptr(g), _ptr(grad), C.byref(st)))
+        return grad, st
 
     def set_field(self, setup: Setup) -> None:
         fd = setup.field_desc()
@@ -155,3 +173,58 @@ def records_to_arrays(recs) -> dict:
     ])
     assert dt.itemsize == C.sizeof(L.PhotonRecord), (dt.itemsize, C.sizeof(L.PhotonRecord))
     return raw.view(dt).copy()
+
+
+# ---- field parameters of the adjoint -------------------------------------------------------------
+def param_count(setup: Setup) -> int:
+    """Length of the parameter vector `adjoint` differentiates (plane waves: amplitudes then
+    phases; spline: the coefficient grid, x fastest)."""
+    fd = setup.field_desc()
+    n = L.load().smp_adjoint_param_count(C.byref(fd))
+    if n < 0:
+        L.check(int(n))
+    return int(n)
+
+
+def field_params(setup: Setup) -> np.ndarray:
+    """The setup's differentiable field parameters as one float64 vector."""
+    if setup.field_type == L.FIELD_PLANEWAVE:
+        return np.concatenate([np.asarray(setup.wave_amp, np.float64), np.asarray(setup.wave_phase, np.float64)])
+    if setup.field_type == L.FIELD_SPLINE:
+        return np.asarray(setup.grid_coeff, np.float64).ravel().copy()
+    raise ValueError("the adjoint is built for plane-wave and spline fields")
+
+
+def with_field_params(setup: Setup, theta) -> Setup:
+    """A copy of `setup` with its field parameters replaced by `theta` (`field_params` order)."""
+    theta = np.asarray(theta, dtype=np.float64)
+    if setup.field_type == L.FIELD_PLANEWAVE:
+        w = len(setup.wave_amp)
+        return dataclasses.replace(setup, wave_amp=tuple(float(x) for x in theta[:w]),
+                                   wave_phase=tuple(float(x) for x in theta[w:2 * w]))
+    if setup.field_type == L.FIELD_SPLINE:
+        return dataclasses.replace(setup, grid_coeff=theta.reshape(np.shape(setup.grid_coeff)).astype(np.float32))
+    raise ValueError("the adjoint is built for plane-wave and spline fields")
+
+
+def roi_weights(setup: Setup, size: int = 32) -> np.ndarray:
+    """dJ/dfilm of the throughput of a central size x size pixel region, summed over all bins."""
+    g = np.zeros(setup.film_shape(), dtype=np.float64)
+    z, y, x = g.shape
+    y0, x0 = (y - size) // 2, (x - size) // 2
+    g[:, y0:y0 + size, x0:x0 + size] = 1.0
+    return g
+
+
+def adjoint(setup: Setup, n_photons: int, dJ_dfilm: np.ndarray) -> tuple[np.ndarray, L.AdjointStats]:
+    """One-shot gradient of sum(dJ_dfilm * film) for the n_photons render of `setup`."""
+    lib = L.load()
+    sc, md, fd, op = setup.descs()
+    g = np.ascontiguousarray(dJ_dfilm, dtype=np.float64)
+    if g.shape != setup.film_shape():
+        raise ValueError(f"dJ_dfilm shape {g.shape} != film {setup.film_shape()}")
+    grad = np.zeros(param_count(setup), dtype=np.float64)
+    st = L.AdjointStats()
+    L.check(lib.smp_render_adjoint(C.byref(sc), C.byref(md), C.byref(fd), C.byref(op), int(n_photons), _ptr(g),
+                                   _ptr(grad), C.byref(st)))
+    return grad, st

@@ -1,0 +1,207 @@
+"""The adjoint (gradient of sum(G * film) over the field parameters) against common-random-number
+finite differences of the forward render.
+
+The adjoint is the pathwise derivative: per photon, random numbers and discrete events are held
+fixed. Two finite-difference checks isolate exactly that quantity:
+
+* direct light only (albedo 0): every photon marches source -> sensor face -> film with no
+  discrete event that depends on the field, so the CRN difference of two renders is the pathwise
+  derivative itself;
+* full scattering: photon records at theta +- h; photons whose discrete event sequence (end code,
+  uniforms drawn, depth, splat count and depths) is the same in both runs are differenced photon
+  by photon ("matched paths"). Photons whose sequence changes -- an escape instead of a scatter, a
+  Fresnel reflection instead of a transmission -- carry the boundary term that a pathwise
+  derivative does not contain; they are a fraction O(h) of the photons.
+
+Tolerances are set by the finite differences' own noise (FP32 marches: the rounding of each
+photon's path changes with the parameters), measured at these photon counts and steps.
+"""
+import numpy as np
+import pytest
+
+import simpler_b200 as sb
+from simpler_b200 import _lib as L
+
+
+def smooth_weights(s):
+    z, y, x = s.film_shape()
+    X, Y = np.meshgrid(np.arange(x) / x, np.arange(y) / y)
+    g = 1.0 + 0.5 * np.sin(2 * np.pi * 3 * X) * np.cos(2 * np.pi * 2 * Y)
+    return np.broadcast_to(g, (z, y, x)).copy()
+
+
+def camera(s):
+    sc = s.scene_desc()
+    d = np.array(sc.view_dir[:]); h = np.array(sc.view_horizontal[:])
+    d /= np.linalg.norm(d); h /= np.linalg.norm(h)
+    return np.array(sc.view_origin[:]), h, np.cross(d, h), np.array(sc.view_plane[:])
+
+
+def photon_objective(s, rec, G):
+    """Per-photon sum(G * film contribution) from its splat records (addEnergyToImage's bilinear
+    split, scene.cpp:782-829)."""
+    o, h, v, plane = camera(s)
+    Z, Y, X = G.shape
+    J = np.zeros(len(rec))
+    lo, hi = s.path_length_min, s.path_length_max
+    for k in range(rec["splats"].shape[1]):
+        idx = np.nonzero(k < rec["n_splats"])[0]
+        sp = rec["splats"][idx, k]
+        p = sp["p"].astype(np.float64)
+        pl = sp["pathlength"]
+        ok = (pl > lo) & (pl < hi)
+        idx, p, pl, val = idx[ok], p[ok], pl[ok], sp["value"][ok]
+        x = ((p @ h - o[1]) / plane[0] + 0.5) * X
+        y = ((p @ v - o[2]) / plane[1] + 0.5) * Y
+        iz = np.floor((pl - lo) / (hi - lo) * Z).astype(np.int64)
+        ix = np.floor(x).astype(np.int64); iy = np.floor(y).astype(np.int64)
+        fx, fy = x - ix, y - iy
+
+        def g(a, b):
+            inb = (a >= 0) & (a < X) & (b >= 0) & (b < Y) & (iz >= 0) & (iz < Z)
+            out = np.zeros(len(a))
+            out[inb] = G[iz[inb], b[inb], a[inb]]
+            return out
+
+        w = ((1 - fx) * (1 - fy) * g(ix, iy) + fx * (1 - fy) * g(ix + 1, iy) + (1 - fx) * fy * g(ix, iy + 1)
+             + fx * fy * g(ix + 1, iy + 1))
+        np.add.at(J, idx, val * w)
+    return J
+
+
+def signature_match(a, b):
+    same = (a["end"] == b["end"]) & (a["draws"] == b["draws"]) & (a["depth"] == b["depth"]) & (a["n_splats"] == b["n_splats"])
+    for k in range(a["splats"].shape[1]):
+        same &= (a["splats"][:, k]["depth"] == b["splats"][:, k]["depth"]) | (k >= a["n_splats"])
+    return same
+
+
+def matched_fd(s, sp, sm, n, G):
+    """sum over matched photons of J(theta + h) - J(theta - h)."""
+    rp = sb.records_to_arrays(sb.trace_photons(sp, 0, n, n, with_image=False)[0])
+    rm = sb.records_to_arrays(sb.trace_photons(sm, 0, n, n, with_image=False)[0])
+    same = signature_match(rp, rm)
+    Jp, Jm = photon_objective(s, rp, G), photon_objective(s, rm, G)
+    return float((Jp[same] - Jm[same]).sum()), float(same.mean())
+
+
+def stepped(theta, i, h):
+    tp, tm = theta.copy(), theta.copy()
+    tp[i] += h
+    tm[i] -= h
+    return tp, tm, float(np.float32(tp[i]) - np.float32(tm[i]))
+
+
+# ---- CPU -----------------------------------------------------------------------------------------
+def test_param_layout():
+    pw = sb.config_planewave()
+    assert sb.param_count(pw) == 2 * len(pw.wave_amp)
+    th = sb.field_params(pw)
+    np.testing.assert_array_equal(th, list(pw.wave_amp) + list(pw.wave_phase))
+    pw2 = sb.with_field_params(pw, th * 2.0)
+    assert pw2.wave_amp == tuple(2.0 * a for a in pw.wave_amp)
+    sp = sb.config_spline(n=8)
+    assert sb.param_count(sp) == 8 ** 3
+    c = sb.field_params(sp)
+    np.testing.assert_array_equal(sb.with_field_params(sp, c).grid_coeff, sp.grid_coeff)
+    with pytest.raises(L.SmpError):
+        sb.param_count(sb.config_plain_small())          # Bessel: no adjoint built
+    g = sb.roi_weights(pw, 32)
+    assert g.shape == pw.film_shape() and g.sum() == 32 * 32 * pw.path_length_bins
+
+
+def test_adjoint_stats_layout():
+    assert sb.check_layout()["smp_adjoint_stats"][0] == 80
+
+
+# ---- GPU -----------------------------------------------------------------------------------------
+@pytest.mark.gpu
+def test_planewave_direct_light_fd():
+    s = sb.config_planewave(albedo=0.0)
+    G = smooth_weights(s)
+    n = 200_000
+    grad, st = sb.adjoint(s, n, G)
+    assert st.photons == n and st.replay_mismatch == 0 and st.dropped == 0 and st.aborted == 0
+    _, fst = sb.render(s, n)
+    assert st.er_steps_forward == fst.er_steps            # phase A traces the render's own photons
+    th = sb.field_params(s)
+    for i, h, tol in [(0, 3e-5, 2e-3), (2, 3e-2, 2e-3)]:   # amplitude and phase of wave 0
+        tp, tm, dh = stepped(th, i, h)
+        fp, _ = sb.render(sb.with_field_params(s, tp), n)
+        fm, _ = sb.render(sb.with_field_params(s, tm), n)
+        fd = float(((fp - fm) * G).sum()) / dh
+        assert abs(grad[i] - fd) <= tol * abs(fd), (i, grad[i], fd)
+
+
+@pytest.mark.gpu
+def test_planewave_scattering_matched_fd():
+    s = sb.config_planewave(max_depth=7)                 # <= 8 splats per photon: all in the records
+    G = sb.roi_weights(s, 32)
+    n = 300_000
+    grad, st = sb.adjoint(s, n, G)
+    assert st.replay_mismatch == 0 and st.dropped == 0
+    th = sb.field_params(s)
+    for i, h, tol in [(0, 3e-5, 0.08), (1, 3e-5, 0.03), (2, 3e-2, 0.02)]:
+        tp, tm, dh = stepped(th, i, h)
+        fd, frac = matched_fd(s, sb.with_field_params(s, tp), sb.with_field_params(s, tm), n, G)
+        assert frac > 0.99
+        fd /= dh
+        assert abs(grad[i] - fd) <= tol * abs(fd), (i, grad[i], fd)
+
+
+@pytest.mark.gpu
+def test_spline_direction_fd():
+    """All 262144 coefficients at once: the gradient dotted with a random perturbation."""
+    n = 100_000
+    s = sb.config_spline(albedo=0.0)
+    G = smooth_weights(s)
+    grad, st = sb.adjoint(s, n, G)
+    assert st.replay_mismatch == 0 and st.dropped == 0
+    th = sb.field_params(s)
+    u = np.random.default_rng(1).standard_normal(th.shape) * 1e-3
+    cp, cm = (th + 0.03 * u).astype(np.float32), (th - 0.03 * u).astype(np.float32)
+    pred = float(grad @ (cp.astype(np.float64) - cm.astype(np.float64)))
+    fp, _ = sb.render(sb.with_field_params(s, cp), n)
+    fm, _ = sb.render(sb.with_field_params(s, cm), n)
+    fd = float(((fp - fm) * G).sum())
+    assert abs(pred - fd) <= 1e-2 * abs(fd), (pred, fd)
+
+    s = sb.config_spline(max_depth=7)
+    G = sb.roi_weights(s, 32)
+    n = 50_000
+    grad, st = sb.adjoint(s, n, G)
+    assert st.replay_mismatch == 0
+    rng = np.random.default_rng(1)
+    rng.standard_normal(th.shape)
+    u = rng.standard_normal(th.shape) * 1e-3
+    cp, cm = (th + 0.03 * u).astype(np.float32), (th - 0.03 * u).astype(np.float32)
+    pred = float(grad @ (cp.astype(np.float64) - cm.astype(np.float64)))
+    fd, frac = matched_fd(s, sb.with_field_params(s, cp), sb.with_field_params(s, cm), n, G)
+    assert frac > 0.99
+    assert abs(pred - fd) <= 3e-2 * abs(fd), (pred, fd)
+
+
+@pytest.mark.gpu
+def test_plan_adjoint_and_autograd():
+    import torch
+    from simpler_b200.pybind.autograd import render_torch
+    s = sb.config_planewave()
+    n = 50_000
+    G = sb.roi_weights(s, 32)
+    g1, _ = sb.adjoint(s, n, G)
+    p = sb.Plan(s)
+    try:
+        g2, _ = p.adjoint(G, 0, n, n)
+        # two halves of the photon range add up to the whole
+        ga, _ = p.adjoint(G, 0, n // 2, n)
+        gb, _ = p.adjoint(G, n // 2, n - n // 2, n)
+    finally:
+        p.close()
+    np.testing.assert_allclose(g2, g1, rtol=1e-6)
+    np.testing.assert_allclose(ga + gb, g1, rtol=1e-6)
+    theta = torch.tensor(sb.field_params(s), requires_grad=True)
+    film = render_torch(theta, s, n)
+    ref, _ = sb.render(s, n)
+    np.testing.assert_allclose(film.detach().numpy(), ref, rtol=1e-5, atol=1e-12)   # FP32 film atomics
+    (film * torch.from_numpy(G)).sum().backward()
+    np.testing.assert_allclose(theta.grad.numpy(), g1, rtol=1e-6)
