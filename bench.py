@@ -31,7 +31,7 @@ sys.path.insert(0, ROOT)
 
 import simpler_b200 as sb  # noqa: E402
 from simpler_b200 import _lib as L  # noqa: E402
-from simpler_b200.roofline import flop_per_step  # noqa: E402
+from simpler_b200.roofline import flop_per_point_adjoint, flop_per_step  # noqa: E402
 
 METRIC = "photon paths/s"
 RENDER_PHOTONS = 100_000_000
@@ -46,9 +46,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--photons-per-step", type=int, default=PHOTONS_PER_STEP)
-    ap.add_argument("--workload", choices=["precision", "sweep", "plain", "planewave", "spline"], default="precision",
+    ap.add_argument("--workload", choices=["precision", "sweep", "plain", "planewave", "spline", "adjoint",
+                                           "adjoint-spline"], default="precision",
                     help="precision: the headline line (default); sweep: the batched 256-instance sweep "
-                         "against the same instances rendered one by one")
+                         "against the same instances rendered one by one; adjoint / adjoint-spline: gradients "
+                         "of the central 32x32 px ROI throughput")
     ap.add_argument("--sweep-scale", type=float, default=1.0,
                     help="sweep: multiply every instance's photon budget")
     return ap.parse_args()
@@ -68,6 +70,19 @@ OTHER = {
                "1e9-photon render"),
 }
 
+
+# adjoint workloads: (setup, photons per gradient, description)
+ADJOINT = {
+    "adjoint": (lambda d: sb.config_planewave(device=d), 10_000_000,
+                "traveling-wave adjoint: two plane waves a = 1e-3 at 1 MHz along +y and +z, phases U[0, 2 pi) "
+                "(seed 3), sigma_s 0.5/mm, albedo 0.9, g 0.9, 128x128 x 32 bins, fp32, 1e7 photons; gradient "
+                "of the central 32x32 px ROI throughput w.r.t. (a_i, phase_i)"),
+    "adjoint-spline": (lambda d: sb.config_spline(device=d), 1_000_000,
+                       "spline adjoint: 64^3 tricubic coefficients over the 10 mm cube (Gaussian-filtered noise, "
+                       "max dn 1e-3, seed 4), sigma_s 1/mm, albedo 0.95, g 0.8, 256x256 x 64 bins, fp32; "
+                       "gradient of the central 32x32 px ROI throughput w.r.t. all 262144 coefficients over "
+                       "1e6-photon steps of the 1e9-photon render"),
+}
 
 _ARGS = None           # the parsed command line (set in main)
 
@@ -390,6 +405,73 @@ def run_sweep(args):
     print(json.dumps(out), flush=True)
 
 
+def run_adjoint(args):
+    """Gradients of the central 32x32 px ROI throughput per second. Each step differentiates its own
+    photon range (photons [i N, (i+1) N)); device time from CUDA events around the adjoint launch.
+    Beside it: the forward render of the same photons, and central finite differences, which cost
+    two forward renders per parameter."""
+    import torch
+    torch.cuda.set_device(0)
+    make, n, desc = ADJOINT[args.workload]
+    setup = make(0)
+    G = sb.roi_weights(setup, 32)
+    npar = sb.param_count(setup)
+    plan = sb.Plan(setup)
+    for i in range(args.warmup):
+        plan.adjoint(G, i * n, n, n)
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms, tot = [], {k: 0 for k in ("er_steps_forward", "er_steps_replay", "points", "splats", "dropped", "skipped",
+                                  "replay_mismatch", "photons", "trace_ms")}
+    for i in range(args.steps):
+        _, st = plan.adjoint(G, (args.warmup + i) * n, n, n)
+        ms.append(st.kernel_ms)
+        for k in tot:
+            tot[k] += getattr(st, k)
+    clk = clocks.stop()
+    # the forward render of the same photon ranges, device-timed
+    fwd = []
+    for i in range(args.steps):
+        plan.clear(0)
+        plan.trace((args.warmup + i) * n, n, n, 0)
+        fwd.append(plan.stats().kernel_ms)
+    plan.close()
+    adj_ms = sum(ms) / len(ms)
+    fwd_ms = sum(fwd) / len(fwd)
+    # e2e: the one-shot C-ABI call with host dJ/dfilm and host gradient, wall clock
+    t0 = time.perf_counter()
+    sb.adjoint(setup, n, G)
+    e2e_s = time.perf_counter() - t0
+    peak = C.c_double()
+    L.check(L.load().smp_fp32_peak(0, C.byref(peak)))
+    flop = (tot["er_steps_forward"] + tot["er_steps_replay"]) * flop_per_step(setup) + \
+        tot["points"] * flop_per_point_adjoint(setup)
+    achieved = flop / (sum(ms) / 1e3) / 1e12
+    out = {
+        "metric": "adjoint gradients/s", "value": 1e3 / adj_ms, "unit": "gradients/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": adj_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": desc, "photons_per_gradient": n, "parameters": npar,
+                   "objective": "sum of the film over the central 32x32 px, all bins"},
+        "photon_paths_per_s": n / (adj_ms / 1e3),
+        "forward_ms": fwd_ms, "cost_vs_forward": adj_ms / fwd_ms,
+        "finite_differences": {"renders": 2 * npar, "ms": 2 * npar * fwd_ms,
+                               "speedup_of_adjoint": 2 * npar * fwd_ms / adj_ms},
+        "roofline": {"bound": "fp32", "kernel": f"adjoint_kernel<{'FK_PLANEWAVE' if npar < 100 else 'FK_SPLINE'}>",
+                     "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s", "frac": achieved / peak.value,
+                     "traffic": None,
+                     "flop_model": "er_steps (checkpointing trace + replays) x flop_per_step + swept points x "
+                                   "flop_per_point_adjoint (simpler_b200/roofline.py)",
+                     "peak_source": "FP32 FMA throughput measured live on this GPU (smp_fp32_peak)"},
+        "counts_per_step": {k: v / args.steps for k, v in tot.items()},
+        "e2e": {"value": 1.0 / e2e_s, "unit": "gradients/s", "h2d_bytes_per_step": G.nbytes + 4096,
+                "d2h_bytes_per_step": npar * 8 + 80, "call": "smp_render_adjoint (one-shot plan, host dJ/dfilm "
+                                                            "and gradient), wall clock"},
+        "gpu_launches": args.steps, "clocks": clk,
+    }
+    print(json.dumps(out), flush=True)
+
+
 def main():
     global _ARGS
     args = parse()
@@ -398,6 +480,8 @@ def main():
         run_reference(args)
     elif args.workload == "sweep":
         run_sweep(args)
+    elif args.workload in ADJOINT:
+        run_adjoint(args)
     else:
         run_ours(args)
 

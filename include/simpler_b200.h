@@ -328,7 +328,8 @@ typedef struct smp_adjoint_stats {
     int64_t er_steps_replay;      /* er_step evaluations of the segment replays                     */
     int64_t points;               /* trajectory points swept backwards                              */
     int64_t splats;               /* splats whose value entered the objective                       */
-    double  kernel_ms;            /* device time of the adjoint launch                              */
+    double  kernel_ms;            /* device time of the adjoint, both kernels, all batches          */
+    double  trace_ms;             /* of which the checkpointing trace                               */
 } smp_adjoint_stats;
 /* Number of parameters smp_render_adjoint returns for this field, or a negative smp_status:
    plane waves 2*n_waves (amplitudes a_0..a_{W-1}, then phases phase_0..phase_{W-1});

@@ -123,35 +123,70 @@ struct AdjVertex {             // a checkpoint (source: index 0, scatter vertex 
     int depth;
     int draws_v, steps_v;      // Philox draw index and ER-step count at EV_VERTEX (after its depth test)
     int draws_so, steps_so;    // the same at EV_SCATTER_ONCE (source: at EV_SCATTER)
+    int hits;                  // the splat that follows lands where dJ/dfilm is nonzero: bit 0 the
+                               // connection from this vertex, bit 1 (source) the direct splat
+    int pad;
     double total;              // optical path length
 };
 
 enum AdjCounter : int {
     ADJ_NEXT = 0,          // work distribution
     ADJ_PHOTONS = 1,       // photons differentiated
-    ADJ_DROPPED = 2,       // photons left out: more vertices than checkpoints, or a move longer than the buffer
+    ADJ_DROPPED = 2,       // photons left out: more vertices than checkpoints, pool or trajectory buffer full
     ADJ_ABORTED = 3,       // photons left out: step cap or non-finite state in the forward trace
     ADJ_MISMATCH = 4,      // replays whose end state differed from the checkpoint (a defect)
-    ADJ_STEPS_FWD = 5,     // er_step evaluations of phase A
-    ADJ_STEPS_REPLAY = 6,  // er_step evaluations of phase B's replays
+    ADJ_STEPS_FWD = 5,     // (unused: the trace counts its steps in KParams.counters)
+    ADJ_STEPS_REPLAY = 6,  // er_step evaluations of the replays
     ADJ_POINTS = 7,        // trajectory points swept backwards
     ADJ_SPLATS = 8,        // splats differentiated
-    ADJ_MIS_CONN = 9,      // mismatch detail: a connection replay did not reach its end event
-    ADJ_MIS_MOVE = 10,     //                  a move replay did not reach its vertex
-    ADJ_MIS_DIRECT = 11,   //                  the direct replay did not reach the scatter stage
-    ADJ_MIS_POS = 12,      //                  a move replay reached a different position
-    ADJ_MIS_DIR = 13,      //                  ... the same position with a different direction
-    ADJ_SKIPPED = 14,      // sensor marches (direct, connections) longer than the trajectory buffer
-    ADJ_COUNT = 15
+    ADJ_SKIPPED = 9,       // segments left out of the sweep: a malformed or truncated record
+    ADJ_COUNT = 10
+};
+
+// One photon's result of the checkpointing trace, and where its replayed segments go.
+enum AdjStatus : int { PH_OK = 0, PH_ABORTED = 1, PH_DROPPED = 2 };
+struct AdjPhoton {
+    int off, nv;               // its checkpoints: pool[off .. off + nv), source first
+    int status;                // AdjStatus
+    int hits;                  // bit 0: some connection splat reaches dJ/dfilm, bit 1: the direct one
+    float s;                   // its temporal scaling / phase draw
+    int tlen;                  // trajectory entries its needed segments can take (an upper bound)
+    int round;                 // replay round that took it (0: not yet)
+    int last;                  // the last vertex whose connection reaches dJ/dfilm (0: none)
+    long long toff;            // its trajectory entries: traj[toff .. toff + tlen)
+    long long pad;
+};
+
+// A replayed segment. Segment c of a photon (c = 0 the direct march, 2k - 1 the move into vertex k,
+// 2k the connection from vertex k) is segs[2 * off + c].
+struct AdjSeg {
+    long long off;             // trajectory entries traj[off .. off + len)
+    int len;
+    int ok;                    // the replay reproduced its checkpoint and, for a sensor march, splatted
+    float mp[3], md[3];        // end position and direction
+    float mn, d2s;             // n at the end, the marched distance (sensor marches)
+    float dir[3];              // the photon direction at the end (the vertex direction of a connection)
+    float md0[3];              // start direction
+    float sp[3];               // splat point, path length and depth (sensor marches)
+    int sdepth;
+    double spl;
 };
 
 struct AdjParams {
     int X, Y, Z;               // film shape (KParams.X is 0 in an adjoint launch: replays splat nothing)
     const double *G;           // dJ/dfilm, X*Y*Z, Image3 layout
-    float4 *traj;              // [tcap][lanes]: (position, step size); step size 0 = segment start,
-                               // -1 = a face reflection between two marches of the segment
-    AdjVertex *verts;          // [lanes][vcap]
-    int tcap, vcap, lanes;
+    float4 *traj;              // replayed trajectories, segment after segment: (position, step size);
+                               // step size 0 = segment start, -1 = a face reflection between marches
+    long long traj_cap;
+    unsigned long long *traj_next;
+    AdjSeg *segs;              // 2 * pool_cap entries
+    int *pending;              // a replay round left photons for the next round
+    AdjVertex *tverts;         // checkpointing trace: [threads][vcap] checkpoints of the current photon
+    int vcap;
+    AdjVertex *pool;           // the batch's checkpoints, photon after photon
+    long long pool_cap;
+    unsigned long long *pool_next;
+    AdjPhoton *photons;        // per photon of the batch
     double *grad;              // dJ/dtheta (layout per field kind, see FieldAdj)
     unsigned long long *cnt;   // AdjCounter
 };
@@ -307,25 +342,35 @@ template <> struct FieldAdj<FK_SPLINE> {
 };
 
 // ---- replay hook: checkpoints (phase A), stop at a segment's end (phase B), splat capture ----------
-struct AdjHook {
+__device__ __forceinline__ float g_at(const AdjParams &A, int x, int y, int z) {
+    if (x < 0 || x >= A.X || y < 0 || y >= A.Y || z < 0 || z >= A.Z) return 0.0f;
+    return float(__ldg(A.G + (size_t(z) * A.Y + y) * A.X + x));
+}
+
+// dJ/dfilm at the four pixels a splat at sensor point p (path length pl) would touch; false when
+// the splat leaves the film's binned range or all four weights are zero.
+__device__ __forceinline__ bool splat_taps(const KParams &P, const AdjParams &A, float3 p, double pl, int depth,
+                                           int &ix, int &iy, float G[4]) {
+    int iz;
+    float fx, fy;
+    if (!splat_bin(P, A.X, p, pl, depth, ix, iy, iz, fx, fy)) return false;
+    G[0] = g_at(A, ix, iy, iz); G[1] = g_at(A, ix + 1, iy, iz);
+    G[2] = g_at(A, ix, iy + 1, iz); G[3] = g_at(A, ix + 1, iy + 1, iz);
+    return G[0] != 0.0f || G[1] != 0.0f || G[2] != 0.0f || G[3] != 0.0f;
+}
+
+// Checkpointing trace (first kernel): records the source and every scatter vertex of the photon in
+// this thread's buffer, marks which of them are followed by a splat that reaches the objective,
+// bounds the length of every move, and at the photon's end copies its checkpoints into the batch
+// pool. Never stops the events.
+struct AdjTraceHook {
     static constexpr bool on = true;
-    int record;                // phase A: record checkpoints, never stop
-    int stop_ev;               // phase B: stop at the entry of this event
+    const KParams *P;
+    const AdjParams *A;
     AdjVertex *v;              // this thread's checkpoints
     int nv, vcap, overflow;
-    int seg_len, max_seg;      // trajectory entries of the current segment / the longest move
-    int splat;                 // a splat happened in this segment
-    float3 sp;                 // its sensor point, path length, depth, value
-    double spl;
-    int sdepth;
-    float sval;
-    // a segment ends at each hook: the direct march at EV_SCATTER, a move at EV_VERTEX, a
-    // connection at EV_SCATTER_ONCE. A move too long for the buffer drops the photon (everything
-    // after it depends on it); a sensor march too long is skipped on its own.
-    __device__ void boundary(int ev) {
-        if (ev == EV_VERTEX) max_seg = max(max_seg, seg_len);
-        seg_len = 0;
-    }
+    int direct_hit;
+    unsigned long long nok, ndrop, nabort;
     __device__ void put(int k, const Lane &L) {
         AdjVertex &c = v[k];
         c.pos[0] = L.pos.x; c.pos[1] = L.pos.y; c.pos[2] = L.pos.z;
@@ -335,12 +380,13 @@ struct AdjHook {
         c.total = L.total;
         c.draws_v = L.draws; c.steps_v = L.steps;
         c.draws_so = L.draws; c.steps_so = L.steps;
+        c.hits = 0;
     }
+    __device__ void photon_begin(const Lane &) { nv = 0; overflow = 0; direct_hit = 0; }
     __device__ bool at(Lane &L, int ev) {
-        if (!record) return ev == stop_ev;
-        boundary(ev);
         if (ev == EV_SCATTER) {
             put(0, L);
+            v[0].hits = direct_hit ? 2 : 0;
             nv = 1;
         } else if (ev == EV_VERTEX) {
             if (nv < vcap) put(nv, L);
@@ -352,9 +398,70 @@ struct AdjHook {
         }
         return false;
     }
-    __device__ void splatted(const Lane &, float3 p, double pl, int depth, float val) {
-        splat = 1; sp = p; spl = pl; sdepth = depth; sval = val;
+    __device__ void splatted(const Lane &, float3 p, double pl, int depth, float) {
+        int ix, iy;
+        float G[4];
+        if (splat_taps(*P, *A, p, pl, depth, ix, iy, G)) {
+            if (nv == 0) direct_hit = 1;                      // before EV_SCATTER: the direct splat
+            else if (nv - 1 < vcap) v[nv - 1].hits |= 1;      // the connection from the last vertex
+        }
     }
+    __device__ void photon_end(const Lane &L) {
+        AdjPhoton r;
+        r.off = 0; r.nv = 0; r.hits = 0; r.s = L.s; r.tlen = 0; r.round = 0; r.last = 0; r.toff = 0; r.pad = 0;
+        if (L.end == SMP_END_STEP_CAP || L.end == SMP_END_NAN) { r.status = PH_ABORTED; ++nabort; }
+        else if (overflow) { r.status = PH_DROPPED; ++ndrop; }
+        else {
+            r.status = PH_OK;
+            // the segments the sweep needs: connections that reach dJ/dfilm, every move up to the
+            // last of them, the direct march if it does; a segment of n er_steps records at most
+            // 2n + 1 trajectory entries (its start, accepted steps, one marker per later march)
+            int hits = 0, last = 0;
+            long long tlen = 0;
+            for (int k = 0; k < nv; ++k) {
+                hits |= v[k].hits;
+                if (k >= 1 && (v[k].hits & 1)) last = k;
+            }
+            if (v[0].hits & 2) tlen += 2LL * v[0].steps_so + 1;
+            for (int k = 1; k < nv; ++k) {
+                if (k <= last) tlen += 2LL * (v[k].steps_v - v[k - 1].steps_so) + 1;
+                if (v[k].hits & 1) tlen += 2LL * (v[k].steps_so - v[k].steps_v) + 1;
+            }
+            r.hits = hits;
+            r.last = last;
+            r.tlen = int(min(tlen, 2147483647LL));
+            if (tlen > A->traj_cap) { r.status = PH_DROPPED; ++ndrop; hits = 0; r.hits = 0; }
+            if (hits && nv > 0) {
+                const unsigned long long off = atomicAdd(A->pool_next, (unsigned long long)nv);
+                if ((long long)(off + nv) > A->pool_cap) { r.status = PH_DROPPED; ++ndrop; }
+                else {
+                    r.off = int(off);
+                    r.nv = nv;
+                    for (int k = 0; k < nv; ++k) A->pool[off + k] = v[k];
+                }
+            }
+            if (r.status == PH_OK) ++nok;
+        }
+        A->photons[L.idx - P->first_photon] = r;
+    }
+};
+
+// Segment replay (sweep kernel): stops at the entry of the event that ends the segment and keeps
+// the segment's splat.
+struct AdjReplayHook {
+    static constexpr bool on = true;
+    int stop_ev;
+    int seg_len;               // trajectory entries of the current segment
+    int splat;                 // a splat happened in this segment
+    float3 sp;                 // its sensor point, path length, depth
+    double spl;
+    int sdepth;
+    __device__ bool at(Lane &, int ev) { return ev == stop_ev; }
+    __device__ void splatted(const Lane &, float3 p, double pl, int depth, float) {
+        splat = 1; sp = p; spl = pl; sdepth = depth;
+    }
+    __device__ void photon_begin(const Lane &) {}
+    __device__ void photon_end(const Lane &) {}
 };
 
 // Position the lane's Philox stream at draw index d (draw k uses word k % 4 of block k / 4).
@@ -365,42 +472,8 @@ __device__ __forceinline__ void rng_seek(Lane &L, const KParams &P, int d) {
     for (int i = 0; i < (d & 3); ++i) (void)draw(L, P);
 }
 
-__device__ __forceinline__ void traj_put(const AdjParams &A, int lane, int i, float4 e) {
-    if (i < A.tcap) A.traj[size_t(i) * A.lanes + lane] = e;
-}
-__device__ __forceinline__ float4 traj_get(const AdjParams &A, int lane, int i) {
-    return A.traj[size_t(i) * A.lanes + lane];
-}
-
-// Run the lane's events from `ev` and every march they start, until the hook stops them
-// (ST_HOOK) or the photon ends (ST_FETCH). With `rec`, the segment's points go to the trajectory
-// buffer: its start point, each accepted step's end point with its step size, and a marker at
-// every face reflection between two of its marches. h.seg_len counts the entries either way.
-template <int FK>
-__device__ __forceinline__ int replay(Lane &L, const KParams &P, int ev, AdjHook &h, const AdjParams &A, int lane,
-                                      bool rec, float3 &md_start, long long &steps) {
-    bool first = true;
-    for (;;) {
-        const int st = run_events<FK, AdjHook>(L, P, ev, &h);
-        if (st != ST_MARCH) return st;
-        if (rec) {
-            if (first) { traj_put(A, lane, h.seg_len, make_float4(L.mp.x, L.mp.y, L.mp.z, 0.0f)); md_start = L.md; }
-            else traj_put(A, lane, h.seg_len, make_float4(0.0f, 0.0f, 0.0f, -1.0f));
-        }
-        ++h.seg_len;
-        first = false;
-        for (;;) {
-            const float3 q = L.mp;
-            const bool end = march_step<FK>(L, P);
-            ++steps;
-            if (q.x != L.mp.x || q.y != L.mp.y || q.z != L.mp.z) {
-                if (rec) traj_put(A, lane, h.seg_len, make_float4(L.mp.x, L.mp.y, L.mp.z, L.cur));
-                ++h.seg_len;
-            }
-            if (end) break;
-        }
-        ev = EV_MARCH_END;
-    }
+__device__ __forceinline__ float4 traj_get(const AdjParams &A, long long base, int i) {
+    return A.traj[base + i];
 }
 
 __device__ __forceinline__ int face_axis(float3 nf) { return nf.x != 0.0f ? 0 : (nf.y != 0.0f ? 1 : 2); }
@@ -409,93 +482,100 @@ __device__ __forceinline__ void add_axis(float3 &v, int ax, float x) {
     if (ax == 0) v.x += x; else if (ax == 1) v.y += x; else v.z += x;
 }
 
-// Backward sweep over one recorded segment (entries [0, nent) of this thread's buffer).
-// In:  (Pa, Da) adjoints of the segment's end position and optical direction, a_end the adjoint of
-//      n at the end point, T the adjoint of each face crossing's arc-length shift, face_end whether
-//      the last march ends on a face (connections, direct) or at its sampled distance (moves;
-//      then T is derived here from the end adjoints), md_end the end direction.
-// Out: (P, D) adjoints of the start position (field terms included) and start direction, with the
-//      start point's parameter cotangent (a0, b0) left to the caller, and n, grad n there.
-struct SweepOut { float3 P, D, b0, g0; float a0, n0; };
+// Backward sweep over one recorded segment (entries [0, nent) of this thread's buffer), one step
+// per sweep_point call so that a warp's sweeping lanes advance together.
+// sweep_begin takes (Pa, Da), the adjoints of the segment's end position and optical direction,
+// a_end the adjoint of n at the end point, T the adjoint of each face crossing's arc-length shift
+// and face_end: the last march ends on a face (connections, direct) or at its sampled distance
+// (moves; T is then derived here from the end adjoints). When sweep_point returns 1 the state
+// holds the adjoints of the start position (Pa, field terms included) and start direction (Da),
+// the start point's parameter cotangent (a0, b0) left to the caller, and n, grad n there (n0, gk).
+struct Sweep {
+    int i;                     // entry whose step is undone next
+    float4 e;
+    float3 d, gk, Pa, Da, b0;
+    float T, a0, n0;
+};
 
 template <int FK>
-__device__ __forceinline__ SweepOut sweep(const KParams &P, const AdjParams &A, int lane, int nent, float3 md_end,
-                                          float3 Pa, float3 Da, float a_end, float T, bool face_end, float s,
-                                          typename FieldAdj<FK>::Acc &acc, long long &pts) {
+__device__ __forceinline__ void sweep_begin(Sweep &w, const KParams &P, const AdjParams &A, long long base, int nent,
+                                            float3 md_end, float3 Pa, float3 Da, float a_end, float T, bool face_end,
+                                            float s, typename FieldAdj<FK>::Acc &acc) {
     const FieldParams &F = P.field;
-    int i = nent - 1;
-    float4 e = traj_get(A, lane, i);
+    w.i = nent - 1;
+    w.e = traj_get(A, base, w.i);
+    const float3 pk = f3(w.e.x, w.e.y, w.e.z);
     float n_k, H[6];
     float3 g_k;
-    float3 d = md_end;
-    FieldAdj<FK>::eval_h(F, f3(e.x, e.y, e.z), s, n_k, g_k, H);
-    {
-        const float3 u = divs(d, n_k);
-        const float At = dot3(u, Pa) + dot3(g_k, Da) + dot3(g_k, u) * a_end;
-        if (face_end) {
-            const int ax = face_axis(face_normal(P, f3(e.x, e.y, e.z)));
-            add_axis(Pa, ax, -(At + T) / comp(u, ax));
-        } else {
-            T = -At;        // each earlier face crossing delays the sampled end by its own shift
-        }
+    FieldAdj<FK>::eval_h(F, pk, s, n_k, g_k, H);
+    const float3 u = divs(md_end, n_k);
+    const float At = dot3(u, Pa) + dot3(g_k, Da) + dot3(g_k, u) * a_end;
+    if (face_end) {
+        const int ax = face_axis(face_normal(P, pk));
+        add_axis(Pa, ax, -(At + T) / comp(u, ax));
+    } else {
+        T = -At;        // each earlier face crossing delays the sampled end by its own shift
     }
     // second kick of the last step, and the end point's own use of n
-    {
-        const float3 b = mul(Da, 0.5f * e.w);
-        Pa = add(Pa, add(mul(g_k, a_end), hmul(H, b)));
-        FieldAdj<FK>::theta(F, f3(e.x, e.y, e.z), s, a_end, b, acc, A);
+    const float3 b = mul(Da, 0.5f * w.e.w);
+    Pa = add(Pa, add(mul(g_k, a_end), hmul(H, b)));
+    FieldAdj<FK>::theta(F, pk, s, a_end, b, acc, A);
+    w.d = md_end; w.gk = g_k; w.Pa = Pa; w.Da = Da; w.T = T;
+}
+
+// Undo one step. 0: more to go; 1: the start point is reached (outputs in w); 2: malformed.
+template <int FK>
+__device__ __forceinline__ int sweep_point(Sweep &w, const KParams &P, const AdjParams &A, long long base, float s,
+                                           typename FieldAdj<FK>::Acc &acc) {
+    const FieldParams &F = P.field;
+    const float c = w.e.w, hh = 0.5f * c;
+    int j = w.i - 1;
+    if (j < 0) return 2;
+    float4 pe = traj_get(A, base, j);
+    const bool junction = pe.w < 0.0f;
+    if (junction) {
+        j -= 1;
+        if (j < 0) return 2;
+        pe = traj_get(A, base, j);
     }
-    SweepOut o;
-    for (;;) {
-        const float c = e.w, hh = 0.5f * c;
-        int j = i - 1;
-        if (j < 0) break;                       // no start entry: malformed segment, give up on it
-        float4 pe = traj_get(A, lane, j);
-        const bool junction = pe.w < 0.0f;
-        if (junction) {
-            j -= 1;
-            if (j < 0) break;
-            pe = traj_get(A, lane, j);
-        }
-        const float3 pp = f3(pe.x, pe.y, pe.z);
-        float n1;
-        float3 g1;
-        FieldAdj<FK>::eval_h(F, pp, s, n1, g1, H);
-        const float3 dh = sub(d, mul(g_k, hh));
-        const float3 dprev = sub(dh, mul(g1, hh));
-        const float q = c / n1;
-        const float3 Dh = add(Da, mul(Pa, q));
-        const float a1 = -(q / n1) * dot3(dh, Pa);
-        float3 b1 = mul(Dh, hh);
-        Pa = add(Pa, add(mul(g1, a1), hmul(H, b1)));
-        Da = Dh;
-        d = dprev;
-        g_k = g1;
-        ++pts;
-        if (junction) {
-            // the previous march ended on a face and reflected: undo the reflection, then the crossing
-            const float3 nf = face_normal(P, pp);
-            Da = reflect_n(Da, nf);
-            d = reflect_n(d, nf);
-            const float3 u = divs(d, n1);
-            const int ax = face_axis(nf);
-            const float At = dot3(u, Pa) + dot3(g1, Da) + T;
-            add_axis(Pa, ax, -At / comp(u, ax));
-        }
-        if (pe.w == 0.0f) {             // the segment's start point
-            o.P = Pa; o.D = Da; o.a0 = a1; o.b0 = b1; o.g0 = g1; o.n0 = n1;
-            return o;
-        }
-        // second kick of the previous step
-        const float3 b2 = mul(Da, 0.5f * pe.w);
-        Pa = add(Pa, hmul(H, b2));
-        b1 = add(b1, b2);
-        FieldAdj<FK>::theta(F, pp, s, a1, b1, acc, A);
-        i = j;
-        e = pe;
+    const float3 pp = f3(pe.x, pe.y, pe.z);
+    float n1, H[6];
+    float3 g1;
+    FieldAdj<FK>::eval_h(F, pp, s, n1, g1, H);
+    const float3 dh = sub(w.d, mul(w.gk, hh));
+    const float3 dprev = sub(dh, mul(g1, hh));
+    const float q = c / n1;
+    const float3 Dh = add(w.Da, mul(w.Pa, q));
+    const float a1 = -(q / n1) * dot3(dh, w.Pa);
+    float3 b1 = mul(Dh, hh);
+    float3 Pa = add(w.Pa, add(mul(g1, a1), hmul(H, b1)));
+    float3 Da = Dh;
+    float3 d = dprev;
+    if (junction) {
+        // the previous march ended on a face and reflected: undo the reflection, then the crossing
+        const float3 nf = face_normal(P, pp);
+        Da = reflect_n(Da, nf);
+        d = reflect_n(d, nf);
+        const float3 u = divs(d, n1);
+        const int ax = face_axis(nf);
+        const float At = dot3(u, Pa) + dot3(g1, Da) + w.T;
+        add_axis(Pa, ax, -At / comp(u, ax));
     }
-    o.P = f3(0.0f, 0.0f, 0.0f); o.D = o.P; o.b0 = o.P; o.g0 = o.P; o.a0 = 0.0f; o.n0 = 1.0f;
-    return o;
+    w.gk = g1;
+    w.d = d;
+    if (pe.w == 0.0f) {                // the segment's start point
+        w.Pa = Pa; w.Da = Da; w.a0 = a1; w.b0 = b1; w.n0 = n1;
+        return 1;
+    }
+    // second kick of the previous step
+    const float3 b2 = mul(Da, 0.5f * pe.w);
+    Pa = add(Pa, hmul(H, b2));
+    b1 = add(b1, b2);
+    FieldAdj<FK>::theta(F, pp, s, a1, b1, acc, A);
+    w.Pa = Pa; w.Da = Da;
+    w.i = j;
+    w.e = pe;
+    return 0;
 }
 
 // ---- the splat's value as a function of the march's end state --------------------------------------
@@ -579,11 +659,6 @@ __device__ __noinline__ float3 hg_vjp(float3 v, float cosT, float sinT, float cP
               Dout.x * ox.d[2] + Dout.y * oy.d[2] + Dout.z * oz.d[2]);
 }
 
-__device__ __forceinline__ float g_at(const AdjParams &A, int x, int y, int z) {
-    if (x < 0 || x >= A.X || y < 0 || y >= A.Y || z < 0 || z >= A.Z) return 0.0f;
-    return float(__ldg(A.G + (size_t(z) * A.Y + y) * A.X + x));
-}
-
 __device__ __forceinline__ void restore(Lane &L, const KParams &P, const AdjVertex &c, bool at_vertex) {
     L.pos = f3(c.pos[0], c.pos[1], c.pos[2]);
     L.dir = f3(c.dir[0], c.dir[1], c.dir[2]);
@@ -595,146 +670,234 @@ __device__ __forceinline__ void restore(Lane &L, const KParams &P, const AdjVert
     rng_seek(L, P, at_vertex ? c.draws_v : c.draws_so);
 }
 
-// Jobs of one photon's backward pass, in order: connection from vertex K, the move into vertex K,
-// ..., connection from vertex 1, the move into vertex 1 (from the source), the direct march, the
-// source direction n(p0) omega0.
-enum AdjJob : int { JOB_FWD = 0, JOB_CONN = 1, JOB_MOVE = 2, JOB_DIRECT = 3, JOB_SOURCE = 4, JOB_END = 5 };
 
-// One thread per photon at a time, photons from a global counter. P is the render's parameter
-// block with P.X = 0 (replays write no film); A carries the film shape, dJ/dfilm and the buffers.
+// Checkpointing trace: the render's persistent lane loop over the batch's photons with the
+// recording hook (no film is written: P.X = 0).
 template <int FK>
-__global__ void __launch_bounds__(128) adjoint_kernel(const __grid_constant__ KParams P, const __grid_constant__ AdjParams A) {
-    const int lane = blockIdx.x * blockDim.x + threadIdx.x;
-    if (lane >= A.lanes) return;
-    const FieldParams &F = P.field;
-    AdjHook h;
-    h.v = A.verts + size_t(lane) * A.vcap;
+__global__ void __launch_bounds__(128, 4) adjoint_trace_kernel(const __grid_constant__ KParams P,
+                                                               const __grid_constant__ AdjParams A) {
+    const int lane = threadIdx.x & 31;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    Lane L;
+    L.end = 0;
+    L.idx = 0;
+    L.tab = nullptr;
+    L.inst = nullptr;
+    L.s = 0.0f;
+    AdjTraceHook h;
+    h.P = &P;
+    h.A = &A;
+    h.v = A.tverts + size_t(t) * A.vcap;
     h.vcap = A.vcap;
+    h.nok = h.ndrop = h.nabort = 0;
+    h.photon_begin(L);
+    LaneStats S;
+    lane_loop<FK, AdjTraceHook>(L, ST_FETCH, P, S, lane, &h);
+    flush_stats(S, P, lane);
+    atomicAdd(A.cnt + ADJ_PHOTONS, h.nok);
+    atomicAdd(A.cnt + ADJ_DROPPED, h.ndrop);
+    atomicAdd(A.cnt + ADJ_ABORTED, h.nabort);
+}
+
+// Segment c of a photon is needed by the sweep: the direct march if its splat reaches dJ/dfilm,
+// a connection if its splat does, a move if a later connection does.
+__device__ __forceinline__ bool seg_needed(const AdjPhoton &r, const AdjVertex *V, int c) {
+    if (c == 0) return (V[0].hits & 2) != 0;
+    const int k = (c + 1) >> 1;
+    return (c & 1) ? k <= r.last : (V[k].hits & 1) != 0;
+}
+
+// Discrete work, marching and sweeping lanes (see the two kernels below).
+enum AdjMode : int { M_DISC = 0, M_MARCH = 1, M_SWEEP = 2, M_EXIT = 3 };
+
+// Replay kernel: for each photon of this round, every segment the sweep needs, replayed forward from
+// its checkpoint with the trajectory written to traj[toff ..] and the end state to its AdjSeg.
+// Lanes run their discrete work (photon fetch, restore, events) one by one and then march together
+// until a quarter of the live lanes wait, as the render's lane loop does. A photon whose entries
+// no longer fit this round's trajectory buffer waits for the next round.
+template <int FK>
+__global__ void __launch_bounds__(128, 3) adjoint_replay_kernel(const __grid_constant__ KParams P,
+                                                                const __grid_constant__ AdjParams A, int round) {
+    const FieldParams &F = P.field;
+    AdjReplayHook h;
     Lane L;
     L.tab = nullptr;
     L.inst = nullptr;
     L.s = 0.0f;
-    long long fsteps = 0, rsteps = 0, pts = 0;
-    unsigned long long nph = 0, ndrop = 0, nabort = 0, nspl = 0, nskip = 0;
-    const float albedo = P.albedo;
-    const int rr_draw = (albedo > 0.0f && albedo < 1.0f) ? 1 : 0;
+    long long rsteps = 0;
+    unsigned long long nmis = 0;
+    const AdjVertex *V = A.pool;
+    AdjSeg *segs = A.segs;
+    AdjPhoton r;
+    r.last = 0; r.nv = 0;
+    int mode = M_DISC, c = 0, K = -1, ev = EV_NEW;
+    bool in_seg = false, first = true, trunc = false;
+    long long base = 0, pos = 0, pend = 0;          // pend: end of the photon's reserved entries
+    float3 md0 = f3(0.0f, 0.0f, 0.0f);
+
     for (;;) {
-        const long long k = (long long)atomicAdd(A.cnt + ADJ_NEXT, 1ull);
-        if (k >= P.n_photons) break;
-        const long long idx = P.first_photon + k;
-        typename FieldAdj<FK>::Acc acc;
-        FieldAdj<FK>::clear(acc);
-        float3 lp = f3(0.0f, 0.0f, 0.0f), ld = f3(0.0f, 0.0f, 0.0f);   // adjoint of (pos, dir) at vertex kv
-        int job = JOB_FWD, kv = 0, K = 0;
-        float s = 0.0f;
-        while (job != JOB_END) {
-            // ---- set up the segment ----
-            int ev = EV_NEW;
-            bool rec = true;
-            h.seg_len = 0;
-            h.splat = 0;
-            h.record = 0;
-            if (job == JOB_FWD) {
-                L.idx = idx;
-                L.end = 0;                          // run_events tests the end code before EV_NEW
-                h.record = 1; h.nv = 0; h.overflow = 0; h.max_seg = 0;
-                rec = false;
-            } else if (job == JOB_CONN) {
-                const AdjVertex &c = h.v[kv];
-                restore(L, P, c, true);
-                L.mp = L.pos;
-                Field<FK>::eval(F, L.tab, L.mp, s, L.mn, L.mg);
-                ev = EV_VERTEX;
-                h.stop_ev = EV_SCATTER_ONCE;
-            } else if (job == JOB_MOVE) {
-                if (lp.x == 0.0f && lp.y == 0.0f && lp.z == 0.0f && ld.x == 0.0f && ld.y == 0.0f && ld.z == 0.0f) {
-                    // nothing downstream of this move depends on it
-                    if (kv == 1) job = P.use_direct ? JOB_DIRECT : JOB_SOURCE;
-                    else { --kv; job = JOB_CONN; }
+        while (mode == M_DISC) {
+            if (!in_seg) {
+                // the photon's next needed segment, or the next photon
+                ++c;
+                while (c <= 2 * K && !seg_needed(r, V, c)) ++c;
+                if (c > 2 * K) {
+                    const long long k = (long long)atomicAdd(A.cnt + ADJ_NEXT, 1ull);
+                    if (k >= P.n_photons) { mode = M_EXIT; break; }
+                    r = A.photons[k];
+                    K = -1;
+                    if (r.status != PH_OK || !r.hits || r.round != 0) continue;
+                    const unsigned long long off = atomicAdd(A.traj_next, (unsigned long long)r.tlen);
+                    if ((long long)(off + r.tlen) > A.traj_cap) { atomicExch(A.pending, 1); continue; }
+                    A.photons[k].round = round;
+                    A.photons[k].toff = (long long)off;
+                    L.idx = P.first_photon + k;         // keys the photon's Philox stream
+                    L.s = r.s;
+                    V = A.pool + r.off;
+                    segs = A.segs + 2LL * r.off;
+                    K = r.nv - 1;
+                    pos = (long long)off;
+                    pend = (long long)off + r.tlen;
+                    c = -1;
                     continue;
                 }
-                restore(L, P, h.v[kv - 1], false);
-                ev = kv == 1 ? EV_SCATTER : EV_SCATTER_ONCE;
-                h.stop_ev = EV_VERTEX;
-            } else if (job == JOB_DIRECT) {
-                L.idx = idx;
-                L.end = 0;
-                h.stop_ev = EV_SCATTER;
+                const int k = (c + 1) >> 1;
+                h.seg_len = 0;
+                h.splat = 0;
+                if (c == 0) {                           // the direct march, from the photon's start
+                    L.end = 0;                          // run_events tests the end code before EV_NEW
+                    ev = EV_NEW;
+                    h.stop_ev = EV_SCATTER;
+                } else if (c & 1) {                     // the move into vertex k
+                    restore(L, P, V[k - 1], false);
+                    ev = k == 1 ? EV_SCATTER : EV_SCATTER_ONCE;
+                    h.stop_ev = EV_VERTEX;
+                } else {                                // the connection from vertex k
+                    restore(L, P, V[k], true);
+                    L.mp = L.pos;
+                    Field<FK>::eval(F, L.tab, L.mp, L.s, L.mn, L.mg);
+                    ev = EV_VERTEX;
+                    h.stop_ev = EV_SCATTER_ONCE;
+                }
+                base = pos;
+                first = true;
+                trunc = false;
+                in_seg = true;
             }
-            float3 md0 = f3(0.0f, 0.0f, 0.0f);
-            int st = ST_FETCH;
-            if (job != JOB_SOURCE) st = replay<FK>(L, P, ev, h, A, lane, rec, md0, job == JOB_FWD ? fsteps : rsteps);
-
-            // ---- differentiate it ----
-            if (job == JOB_FWD) {
-                if (L.end == SMP_END_STEP_CAP || L.end == SMP_END_NAN) { ++nabort; break; }
-                if (h.overflow || h.max_seg > A.tcap) { ++ndrop; break; }
-                ++nph;
-                s = L.s;
-                K = h.nv - 1;
-                if (h.nv == 0) break;                       // never reached the scatter stage
-                if (K >= 1) { kv = K; job = JOB_CONN; }
-                else job = P.use_direct ? JOB_DIRECT : JOB_SOURCE;
-                continue;
-            }
-            if (job != JOB_SOURCE && st != ST_HOOK) {
-                atomicAdd(A.cnt + ADJ_MISMATCH, 1ull);
-                atomicAdd(A.cnt + (job == JOB_CONN ? ADJ_MIS_CONN : job == JOB_MOVE ? ADJ_MIS_MOVE : ADJ_MIS_DIRECT), 1ull);
+            const int st = run_events<FK, AdjReplayHook>(L, P, ev, &h);
+            if (st == ST_MARCH) {
+                if (base + h.seg_len < pend)
+                    A.traj[base + h.seg_len] = first ? make_float4(L.mp.x, L.mp.y, L.mp.z, 0.0f)
+                                                     : make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+                else trunc = true;
+                if (first) md0 = L.md;
+                first = false;
+                ++h.seg_len;
+                mode = M_MARCH;
                 break;
             }
-            if (job == JOB_MOVE) {
-                const AdjVertex &c = h.v[kv];
-                const bool pos_ok = L.pos.x == c.pos[0] && L.pos.y == c.pos[1] && L.pos.z == c.pos[2];
-                const bool dir_ok = L.dir.x == c.dir[0] && L.dir.y == c.dir[1] && L.dir.z == c.dir[2];
-                if (!pos_ok || !dir_ok) {
-                    atomicAdd(A.cnt + ADJ_MISMATCH, 1ull);
-                    atomicAdd(A.cnt + (pos_ok ? ADJ_MIS_DIR : ADJ_MIS_POS), 1ull);
-                    break;
-                }
+            // the segment has ended: check it against the checkpoint it leads to, record its end
+            const int k = (c + 1) >> 1;
+            bool ok = st == ST_HOOK && !trunc;
+            if (ok && (c & 1)) {
+                const AdjVertex &cv = V[k];
+                ok = L.pos.x == cv.pos[0] && L.pos.y == cv.pos[1] && L.pos.z == cv.pos[2] &&
+                     L.dir.x == cv.dir[0] && L.dir.y == cv.dir[1] && L.dir.z == cv.dir[2];
             }
-            bool do_sweep = false, face_end = true;
-            float3 Pa = f3(0.0f, 0.0f, 0.0f), Da = Pa, Ddir = Pa;
-            float a_end = 0.0f, T = 0.0f;
-            if ((job == JOB_CONN || job == JOB_DIRECT) && h.splat) {
-                int ix, iy, iz;
-                float fx, fy;
-                if (splat_bin(P, A.X, h.sp, h.spl, h.sdepth, ix, iy, iz, fx, fy)) {
-                    const float G00 = g_at(A, ix, iy, iz), G10 = g_at(A, ix + 1, iy, iz);
-                    const float G01 = g_at(A, ix, iy + 1, iz), G11 = g_at(A, ix + 1, iy + 1, iz);
-                    if (G00 != 0.0f || G10 != 0.0f || G01 != 0.0f || G11 != 0.0f) {
-                        float gr[11];
-                        sensor_grad(P, A.X, P.weight, P.sigma_t, P.g, job == JOB_CONN, L.mp, L.md, L.mn, L.d2s, L.dir,
-                                    ix, iy, G00, G10, G01, G11, gr);
-                        Pa = f3(gr[0], gr[1], gr[2]);
-                        Da = f3(gr[3], gr[4], gr[5]);
-                        a_end = gr[6];
-                        T = gr[7];
-                        Ddir = f3(gr[8], gr[9], gr[10]);
-                        do_sweep = true;
-                        ++nspl;
+            if (!ok) ++nmis;
+            AdjSeg &g = segs[c];
+            g.off = base;
+            g.len = int(min((long long)h.seg_len, pend - base));
+            g.ok = ok && ((c & 1) || h.splat);
+            g.mp[0] = L.mp.x; g.mp[1] = L.mp.y; g.mp[2] = L.mp.z;
+            g.md[0] = L.md.x; g.md[1] = L.md.y; g.md[2] = L.md.z;
+            g.mn = L.mn;
+            g.d2s = L.d2s;
+            g.dir[0] = L.dir.x; g.dir[1] = L.dir.y; g.dir[2] = L.dir.z;
+            g.md0[0] = md0.x; g.md0[1] = md0.y; g.md0[2] = md0.z;
+            g.sp[0] = h.sp.x; g.sp[1] = h.sp.y; g.sp[2] = h.sp.z;
+            g.sdepth = h.sdepth;
+            g.spl = h.spl;
+            pos = min(base + h.seg_len, pend);
+            in_seg = false;
+        }
+
+        const unsigned live = __ballot_sync(kFull, mode != M_EXIT);
+        if (live == 0) break;
+        const int thr = max(1, (__popc(live) + 2) >> 2);
+        if (__any_sync(kFull, mode == M_MARCH)) {
+            for (;;) {
+                if (mode == M_MARCH) {
+                    for (int t = 0; t < 2; ++t) {
+                        const float3 q = L.mp;
+                        const bool end = march_step<FK>(L, P);
+                        ++rsteps;
+                        if (q.x != L.mp.x || q.y != L.mp.y || q.z != L.mp.z) {
+                            if (base + h.seg_len < pend) A.traj[base + h.seg_len] = make_float4(L.mp.x, L.mp.y, L.mp.z, L.cur);
+                            else trunc = true;
+                            ++h.seg_len;
+                        }
+                        if (end) { mode = M_DISC; ev = EV_MARCH_END; break; }
                     }
                 }
-            } else if (job == JOB_MOVE) {
-                Pa = lp; Da = ld;
-                face_end = false;
-                do_sweep = true;
+                const unsigned waiting = __ballot_sync(kFull, mode == M_DISC);
+                if (__popc(waiting) >= thr || !__any_sync(kFull, mode == M_MARCH)) break;
             }
-            if (do_sweep && h.seg_len >= 2 && h.seg_len <= A.tcap) {
-                const SweepOut o = sweep<FK>(P, A, lane, h.seg_len, L.md, Pa, Da, a_end, T, face_end, s, acc, pts);
-                const float4 e0 = traj_get(A, lane, 0);
+        }
+    }
+    atomicAdd(A.cnt + ADJ_STEPS_REPLAY, (unsigned long long)rsteps);
+    if (nmis) atomicAdd(A.cnt + ADJ_MISMATCH, nmis);
+}
+
+// Sweep kernel: for each photon of this round, the jobs of its backward pass over the recorded
+// segments -- the connection from vertex K, the move into vertex K, ..., the move into vertex 1,
+// the direct march, the source direction n(p0) omega0 -- each a backward sweep (sweep_begin, then
+// sweep_point per recorded step). Lanes run their discrete work one by one and then sweep together
+// until few lanes are left sweeping.
+enum AdjJob : int { JOB_CONN = 1, JOB_MOVE = 2, JOB_DIRECT = 3, JOB_SOURCE = 4 };
+
+template <int FK>
+__global__ void __launch_bounds__(128) adjoint_sweep_kernel(const __grid_constant__ KParams P,
+                                                            const __grid_constant__ AdjParams A, int round) {
+    const FieldParams &F = P.field;
+    Lane L;                                     // Philox draws of the HG rotation
+    L.tab = nullptr;
+    L.inst = nullptr;
+    long long pts = 0;
+    unsigned long long nspl = 0, nskip = 0;
+    const float albedo = P.albedo;
+    const int rr_draw = (albedo > 0.0f && albedo < 1.0f) ? 1 : 0;
+    const AdjVertex *V = A.pool;
+    const AdjSeg *segs = A.segs;
+    int mode = M_DISC, job = 0, kv = 0;
+    bool busy = false;                          // a photon is in progress
+    float s = 0.0f;
+    float3 lp = f3(0.0f, 0.0f, 0.0f), ld = lp, Ddir = lp;
+    long long sbase = 0;
+    typename FieldAdj<FK>::Acc acc;
+    FieldAdj<FK>::clear(acc);
+    Sweep w;
+    bool after = false;                         // a sweep just finished: its job's start handling is due
+
+    for (;;) {
+        while (mode == M_DISC) {
+            if (after) {
+                after = false;
+                const float4 e0 = traj_get(A, sbase, 0);
                 const float3 p0 = f3(e0.x, e0.y, e0.z);
+                const AdjSeg &g = segs[job == JOB_DIRECT ? 0 : (job == JOB_MOVE ? 2 * kv - 1 : 2 * kv)];
                 if (job == JOB_CONN) {
                     // md0 = omega n(pos): the start direction's dependence on n at the vertex
-                    const float as = dot3(md0, o.D) / o.n0;
-                    lp = add(lp, add(o.P, mul(o.g0, as)));
+                    const float as = (g.md0[0] * w.Da.x + g.md0[1] * w.Da.y + g.md0[2] * w.Da.z) / w.n0;
+                    lp = add(lp, add(w.Pa, mul(w.gk, as)));
                     ld = add(ld, Ddir);
-                    FieldAdj<FK>::theta(F, p0, s, o.a0 + as, o.b0, acc, A);
+                    FieldAdj<FK>::theta(F, p0, s, w.a0 + as, w.b0, acc, A);
                 } else if (job == JOB_MOVE) {
-                    FieldAdj<FK>::theta(F, p0, s, o.a0, o.b0, acc, A);
-                    lp = o.P;
+                    FieldAdj<FK>::theta(F, p0, s, w.a0, w.b0, acc, A);
+                    lp = w.Pa;
                     if (kv >= 2) {
                         // the move began with v' = |v| HG(v / |v|) at vertex kv - 1
-                        const AdjVertex &c = h.v[kv - 1];
+                        const AdjVertex &c = V[kv - 1];
                         rng_seek(L, P, c.draws_so + rr_draw);
                         const float u1 = draw(L, P), u2 = draw(L, P);
                         const float gg = P.g;
@@ -747,44 +910,120 @@ __global__ void __launch_bounds__(128) adjoint_kernel(const __grid_constant__ KP
                         const float sinT = sqrtf(fmaxf(0.0f, 1.0f - cosT * cosT));
                         float sP, cP;
                         sincos_red(6.28318548202514648f * u2, sP, cP);
-                        ld = hg_vjp(f3(c.dir[0], c.dir[1], c.dir[2]), cosT, sinT, cP, sP, o.D);
+                        ld = hg_vjp(f3(c.dir[0], c.dir[1], c.dir[2]), cosT, sinT, cP, sP, w.Da);
                     } else {
-                        ld = o.D;
+                        ld = w.Da;
                     }
-                } else {   // JOB_DIRECT: starts from the source state, as the first move does
-                    lp = add(lp, o.P);
-                    ld = add(ld, o.D);
-                    FieldAdj<FK>::theta(F, p0, s, o.a0, o.b0, acc, A);
+                } else {                            // JOB_DIRECT: starts from the source state
+                    lp = add(lp, w.Pa);
+                    ld = add(ld, w.Da);
+                    FieldAdj<FK>::theta(F, p0, s, w.a0, w.b0, acc, A);
                 }
-            } else if (do_sweep) {
-                ++nskip;                                // a sensor march longer than the buffer
+                // the next job
+                if (job == JOB_CONN) job = JOB_MOVE;
+                else if (job == JOB_MOVE) {
+                    if (kv == 1) job = JOB_DIRECT;
+                    else { --kv; job = JOB_CONN; }
+                } else job = JOB_SOURCE;
             }
+            if (!busy) {
+                const long long k = (long long)atomicAdd(A.cnt + ADJ_NEXT, 1ull);
+                if (k >= P.n_photons) { mode = M_EXIT; break; }
+                const AdjPhoton r = A.photons[k];
+                if (r.round != round) continue;
+                L.idx = P.first_photon + k;
+                s = r.s;
+                V = A.pool + r.off;
+                segs = A.segs + 2LL * r.off;
+                FieldAdj<FK>::clear(acc);
+                lp = f3(0.0f, 0.0f, 0.0f); ld = lp;
+                kv = r.nv - 1;
+                job = kv >= 1 ? JOB_CONN : JOB_DIRECT;
+                busy = true;
+            }
+            // set up the current job's sweep, skipping jobs with nothing to carry
             if (job == JOB_SOURCE) {
                 // dir0 = n(p0) omega0 (photon.cpp:329)
-                const AdjVertex &c = h.v[0];
-                const float3 p0 = f3(c.pos[0], c.pos[1], c.pos[2]);
-                float n0, H[6];
-                float3 g0;
-                FieldAdj<FK>::eval_h(F, p0, s, n0, g0, H);
-                const float as = (c.dir[0] * ld.x + c.dir[1] * ld.y + c.dir[2] * ld.z) / n0;
-                FieldAdj<FK>::theta(F, p0, s, as, f3(0.0f, 0.0f, 0.0f), acc, A);
-                job = JOB_END;
-            } else if (job == JOB_CONN) {
-                job = JOB_MOVE;
-            } else if (job == JOB_MOVE) {
-                if (kv == 1) job = P.use_direct ? JOB_DIRECT : JOB_SOURCE;
+                if (ld.x != 0.0f || ld.y != 0.0f || ld.z != 0.0f) {
+                    const AdjVertex &c = V[0];
+                    const float3 p0 = f3(c.pos[0], c.pos[1], c.pos[2]);
+                    float n0, H[6];
+                    float3 g0;
+                    FieldAdj<FK>::eval_h(F, p0, s, n0, g0, H);
+                    const float as = (c.dir[0] * ld.x + c.dir[1] * ld.y + c.dir[2] * ld.z) / n0;
+                    FieldAdj<FK>::theta(F, p0, s, as, f3(0.0f, 0.0f, 0.0f), acc, A);
+                }
+                FieldAdj<FK>::flush(acc, F, A);
+                busy = false;
+                continue;
+            }
+            const int c = job == JOB_DIRECT ? 0 : (job == JOB_MOVE ? 2 * kv - 1 : 2 * kv);
+            bool run = false, face_end = true;
+            float3 Pa = f3(0.0f, 0.0f, 0.0f), Da = Pa;
+            float a_end = 0.0f, T = 0.0f;
+            Ddir = Pa;
+            if (job == JOB_MOVE) {
+                run = !(lp.x == 0.0f && lp.y == 0.0f && lp.z == 0.0f && ld.x == 0.0f && ld.y == 0.0f && ld.z == 0.0f);
+                Pa = lp; Da = ld;
+                face_end = false;
+            } else if (job == JOB_CONN ? (V[kv].hits & 1) : (V[0].hits & 2)) {
+                const AdjSeg &g = segs[c];
+                int ix, iy;
+                float Gt[4];
+                if (g.ok && splat_taps(P, A, f3(g.sp[0], g.sp[1], g.sp[2]), g.spl, g.sdepth, ix, iy, Gt)) {
+                    float gr[11];
+                    sensor_grad(P, A.X, P.weight, P.sigma_t, P.g, job == JOB_CONN, f3(g.mp[0], g.mp[1], g.mp[2]),
+                                f3(g.md[0], g.md[1], g.md[2]), g.mn, g.d2s, f3(g.dir[0], g.dir[1], g.dir[2]),
+                                ix, iy, Gt[0], Gt[1], Gt[2], Gt[3], gr);
+                    Pa = f3(gr[0], gr[1], gr[2]);
+                    Da = f3(gr[3], gr[4], gr[5]);
+                    a_end = gr[6];
+                    T = gr[7];
+                    Ddir = f3(gr[8], gr[9], gr[10]);
+                    run = true;
+                    ++nspl;
+                }
+            }
+            if (run && segs[c].len >= 2 && (job != JOB_MOVE || segs[c].ok)) {
+                const AdjSeg &g = segs[c];
+                sbase = g.off;
+                sweep_begin<FK>(w, P, A, sbase, g.len, f3(g.md[0], g.md[1], g.md[2]), Pa, Da, a_end, T, face_end, s, acc);
+                mode = M_SWEEP;
+                break;
+            }
+            if (run) ++nskip;
+            // nothing to sweep: the next job, with the adjoint carried as it is
+            if (job == JOB_CONN) job = JOB_MOVE;
+            else if (job == JOB_MOVE) {
+                if (kv == 1) job = JOB_DIRECT;
                 else { --kv; job = JOB_CONN; }
-            } else {
-                job = JOB_SOURCE;
+            } else job = JOB_SOURCE;
+        }
+
+        const unsigned live = __ballot_sync(kFull, mode != M_EXIT);
+        if (live == 0) break;
+        const int thr = max(1, (__popc(live) + 2) >> 2);
+        if (__any_sync(kFull, mode == M_SWEEP)) {
+            for (;;) {
+                if (mode == M_SWEEP) {
+                    const int rr = sweep_point<FK>(w, P, A, sbase, s, acc);
+                    ++pts;
+                    if (rr == 1) { mode = M_DISC; after = true; }
+                    else if (rr == 2) {
+                        mode = M_DISC;
+                        ++nskip;
+                        if (job == JOB_CONN) job = JOB_MOVE;
+                        else if (job == JOB_MOVE) {
+                            if (kv == 1) job = JOB_DIRECT;
+                            else { --kv; job = JOB_CONN; }
+                        } else job = JOB_SOURCE;
+                    }
+                }
+                const unsigned idle = __ballot_sync(kFull, mode == M_DISC);
+                if (__popc(idle) >= thr || !__any_sync(kFull, mode == M_SWEEP)) break;
             }
         }
-        FieldAdj<FK>::flush(acc, F, A);
     }
-    atomicAdd(A.cnt + ADJ_PHOTONS, nph);
-    atomicAdd(A.cnt + ADJ_DROPPED, ndrop);
-    atomicAdd(A.cnt + ADJ_ABORTED, nabort);
-    atomicAdd(A.cnt + ADJ_STEPS_FWD, (unsigned long long)fsteps);
-    atomicAdd(A.cnt + ADJ_STEPS_REPLAY, (unsigned long long)rsteps);
     atomicAdd(A.cnt + ADJ_POINTS, (unsigned long long)pts);
     atomicAdd(A.cnt + ADJ_SPLATS, nspl);
     atomicAdd(A.cnt + ADJ_SKIPPED, nskip);

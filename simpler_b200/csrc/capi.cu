@@ -430,6 +430,9 @@ struct smp_plan {
     long long graph_march_launches = 0;
     double tune_rate[4] = {0, 0, 0, 0};
     int tune_n[4] = {0, 0, 0, 0};
+    // adjoint buffers (smp_plan_adjoint), kept for the plan's life and grown on demand
+    void *adj_buf = nullptr;
+    size_t adj_bytes = 0;
     std::vector<cudaEvent_t> march_ev;   // event pairs around march-kernel launches (a reused pool)
     size_t march_ev_used = 0;            // since the last clear
     long long n_launched = 0;            // kernels launched since the last clear
@@ -452,6 +455,7 @@ static void plan_free(smp_plan *p) {
     cudaFree(p->d_film);
     cudaFree(p->d_counters);
     cudaFree(p->d_wave);
+    cudaFree(p->adj_buf);
     if (p->h_live) cudaFreeHost(p->h_live);
     for (int i = 0; i < 2; ++i) {
         if (p->live_ev[i]) cudaEventDestroy(p->live_ev[i]);
@@ -1320,10 +1324,25 @@ int64_t smp_adjoint_param_count(const smp_field_desc *f) {
 }
 
 typedef void (*AdjFn)(KParams, AdjParams);
-static AdjFn adjoint_fn(int fk) {
+typedef void (*AdjRoundFn)(KParams, AdjParams, int);
+static AdjFn adjoint_trace_fn(int fk) {
     switch (fk) {
-        case FK_PLANEWAVE: return adjoint_kernel<FK_PLANEWAVE>;
-        case FK_SPLINE: return adjoint_kernel<FK_SPLINE>;
+        case FK_PLANEWAVE: return adjoint_trace_kernel<FK_PLANEWAVE>;
+        case FK_SPLINE: return adjoint_trace_kernel<FK_SPLINE>;
+        default: return nullptr;
+    }
+}
+static AdjRoundFn adjoint_replay_fn(int fk) {
+    switch (fk) {
+        case FK_PLANEWAVE: return adjoint_replay_kernel<FK_PLANEWAVE>;
+        case FK_SPLINE: return adjoint_replay_kernel<FK_SPLINE>;
+        default: return nullptr;
+    }
+}
+static AdjRoundFn adjoint_sweep_fn(int fk) {
+    switch (fk) {
+        case FK_PLANEWAVE: return adjoint_sweep_kernel<FK_PLANEWAVE>;
+        case FK_SPLINE: return adjoint_sweep_kernel<FK_SPLINE>;
         default: return nullptr;
     }
 }
@@ -1334,6 +1353,19 @@ static int env_int(const char *name, int def, int lo, int hi) {
     return std::max(lo, std::min(hi, std::atoi(v)));
 }
 
+static int grid_of(const void *fn, int dev) {
+    int sms = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0) != cudaSuccess) return 0;
+    return sms * std::max(per_sm, 1);
+}
+
+// Photons are differentiated in batches. Per batch: the checkpointing trace (one checkpoint per
+// scatter vertex into the batch pool), then rounds of replay (every segment the sweep needs,
+// written to the trajectory buffer, as many photons as fit) and sweep (the backward pass over
+// them). Buffers, one allocation kept in the plan: dJ/dfilm, gradient, counters; per trace thread
+// vcap checkpoints; the pool (batch x pool_per_photon checkpoints), two segment records per
+// checkpoint, one AdjPhoton per photon of the batch; the trajectory buffer.
 int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, int64_t weight_photons,
                      const double *dJ_dfilm, double *grad_out, smp_adjoint_stats *stats_out) {
     if (!plan || !dJ_dfilm || !grad_out || n_photons < 0 || first_photon < 0)
@@ -1341,61 +1373,110 @@ int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, in
     if (weight_photons <= 0) return set_error(SMP_ERR_BAD_ARG, "weight_photons must be positive");
     const int64_t np = smp_adjoint_param_count(&plan->field);
     if (np < 0) return int(np);
-    AdjFn fn = adjoint_fn(plan->fk);
-    if (!fn) return set_error(SMP_ERR_UNSUPPORTED, "no adjoint for field kind %d", plan->fk);
+    AdjFn fa = adjoint_trace_fn(plan->fk);
+    AdjRoundFn fr = adjoint_replay_fn(plan->fk), fs = adjoint_sweep_fn(plan->fk);
+    if (!fa || !fr || !fs) return set_error(SMP_ERR_UNSUPPORTED, "no adjoint for field kind %d", plan->fk);
     if (plan->kp.rng != SMP_RNG_PHILOX) return set_error(SMP_ERR_UNSUPPORTED, "the adjoint replays Philox streams only");
     if (plan->kp.src_lens_active || plan->kp.cam_lens_active)
         return set_error(SMP_ERR_UNSUPPORTED, "the adjoint is built for scenes without lenses");
     SMP_CUDA(cudaSetDevice(plan->device));
-    int sms = 0, per_sm = 0;
-    SMP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, plan->device));
-    SMP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0));
-    // per-thread buffers: trajectory entries of one segment (16 B each) and vertex checkpoints
-    per_sm = env_int("SMP_ADJ_BLOCKS", std::max(per_sm, 1), 1, 64);
-    const int grid = sms * per_sm;
+    const int grid_a = grid_of(reinterpret_cast<const void *>(fa), plan->device);
+    const int grid_r = grid_of(reinterpret_cast<const void *>(fr), plan->device);
+    const int grid_s = grid_of(reinterpret_cast<const void *>(fs), plan->device);
+    if (!grid_a || !grid_r || !grid_s) return set_error(SMP_ERR_CUDA, "adjoint occupancy query failed");
     AdjParams a;
     std::memset(&a, 0, sizeof(a));
     a.X = plan->kp.X; a.Y = plan->kp.Y; a.Z = plan->kp.Z;
-    a.lanes = grid * kBlock;
-    a.tcap = env_int("SMP_ADJ_TCAP", 8192, 16, 1 << 24);
     a.vcap = env_int("SMP_ADJ_VCAP", 256, 2, 1 << 20);
+    const long long batch = env_int("SMP_ADJ_BATCH", 1 << 19, 1024, 1 << 30);
+    const long long per_photon = env_int("SMP_ADJ_POOL_PER_PHOTON", 16, 1, 4096);
+    a.pool_cap = batch * per_photon;
+    a.traj_cap = (long long)env_int("SMP_ADJ_TRAJ_MB", 8192, 16, 1 << 20) * (1LL << 20) / (long long)sizeof(float4);
     const size_t film = size_t(a.X) * a.Y * a.Z;
-    double *d_G = nullptr, *d_grad = nullptr;
-    float4 *d_traj = nullptr;
-    AdjVertex *d_verts = nullptr;
-    unsigned long long *d_cnt = nullptr;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    const int ncnt = ADJ_COUNT + CNT_COUNT + 3;          // + pool_next, traj_next, pending
+    auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t bG = up(film * sizeof(double)), bgrad = up(size_t(np) * sizeof(double));
+    const size_t bcnt = up(ncnt * sizeof(unsigned long long));
+    const size_t btv = up(size_t(a.vcap) * grid_a * kBlock * sizeof(AdjVertex));
+    const size_t bpool = up(size_t(a.pool_cap) * sizeof(AdjVertex));
+    const size_t bsegs = up(2 * size_t(a.pool_cap) * sizeof(AdjSeg));
+    const size_t bph = up(size_t(batch) * sizeof(AdjPhoton));
+    const size_t btraj = size_t(a.traj_cap) * sizeof(float4);
+    const size_t need = bG + bgrad + bcnt + btv + bpool + bsegs + bph + btraj;
+    if (plan->adj_bytes < need) {
+        cudaFree(plan->adj_buf);
+        plan->adj_buf = nullptr;
+        plan->adj_bytes = 0;
+        cudaError_t ea = cudaMalloc(&plan->adj_buf, need);
+        if (ea != cudaSuccess)
+            return set_error(ea == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "adjoint buffers (%zu bytes): %s",
+                             need, cudaGetErrorString(ea));
+        plan->adj_bytes = need;
+    }
+    char *base = static_cast<char *>(plan->adj_buf);
+    double *d_G = reinterpret_cast<double *>(base); base += bG;
+    double *d_grad = reinterpret_cast<double *>(base); base += bgrad;
+    unsigned long long *d_cnt = reinterpret_cast<unsigned long long *>(base); base += bcnt;
+    a.tverts = reinterpret_cast<AdjVertex *>(base); base += btv;
+    a.pool = reinterpret_cast<AdjVertex *>(base); base += bpool;
+    a.segs = reinterpret_cast<AdjSeg *>(base); base += bsegs;
+    a.photons = reinterpret_cast<AdjPhoton *>(base); base += bph;
+    a.traj = reinterpret_cast<float4 *>(base);
+    a.G = d_G; a.grad = d_grad; a.cnt = d_cnt;
+    unsigned long long *d_kcnt = d_cnt + ADJ_COUNT;
+    a.pool_next = d_kcnt + CNT_COUNT;
+    a.traj_next = a.pool_next + 1;
+    a.pending = reinterpret_cast<int *>(a.pool_next + 2);
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int rc = SMP_OK;
-    cudaError_t e = cudaMalloc(&d_G, film * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&d_grad, size_t(np) * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&d_traj, size_t(a.tcap) * a.lanes * sizeof(float4));
-    if (e == cudaSuccess) e = cudaMalloc(&d_verts, size_t(a.vcap) * a.lanes * sizeof(AdjVertex));
-    if (e == cudaSuccess) e = cudaMalloc(&d_cnt, ADJ_COUNT * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMemcpy(d_G, dJ_dfilm, film * sizeof(double), cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpy(d_G, dJ_dfilm, film * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(d_grad, 0, size_t(np) * sizeof(double));
-    if (e == cudaSuccess) e = cudaMemset(d_cnt, 0, ADJ_COUNT * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaEventCreate(&e0);
-    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaMemset(d_cnt, 0, ncnt * sizeof(unsigned long long));
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&ev[i]);
     unsigned long long c[ADJ_COUNT] = {0};
+    unsigned long long fwd_steps = 0;
     float ms = 0.0f;
+    double trace_ms = 0.0;
     if (e != cudaSuccess) {
-        rc = set_error(e == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "adjoint setup: %s", cudaGetErrorString(e));
+        rc = set_error(SMP_ERR_CUDA, "adjoint setup: %s", cudaGetErrorString(e));
     } else if (n_photons > 0) {
-        a.G = d_G; a.grad = d_grad; a.traj = d_traj; a.verts = d_verts; a.cnt = d_cnt;
         KParams k = plan->kp;
         k.weight = photon_weight(plan->scene, weight_photons);
-        k.first_photon = first_photon;
-        k.n_photons = n_photons;
         k.records = nullptr;
         k.stream = nullptr;
         k.offsets = nullptr;
+        k.counters = d_kcnt;
+        k.event_batch = plan->event_batch;
         k.X = 0;                          // replays add nothing to any film
-        cudaEventRecord(e0, 0);
-        fn<<<grid, kBlock>>>(k, a);
-        e = cudaGetLastError();
-        cudaEventRecord(e1, 0);
+        cudaEventRecord(ev[0], 0);
+        for (long long done = 0; done < n_photons && e == cudaSuccess; done += batch) {
+            k.first_photon = first_photon + done;
+            k.n_photons = std::min<long long>(batch, n_photons - done);
+            e = cudaMemsetAsync(d_kcnt, 0, (CNT_COUNT + 1) * sizeof(unsigned long long), 0);
+            cudaEventRecord(ev[2], 0);
+            if (e == cudaSuccess) fa<<<grid_a, kBlock>>>(k, a);
+            cudaEventRecord(ev[3], 0);
+            for (int round = 1; e == cudaSuccess; ++round) {
+                e = cudaMemsetAsync(a.traj_next, 0, 2 * sizeof(unsigned long long), 0);
+                if (e == cudaSuccess) e = cudaMemsetAsync(d_cnt + ADJ_NEXT, 0, sizeof(unsigned long long), 0);
+                if (e == cudaSuccess) fr<<<grid_r, kBlock>>>(k, a, round);
+                if (e == cudaSuccess) e = cudaMemsetAsync(d_cnt + ADJ_NEXT, 0, sizeof(unsigned long long), 0);
+                if (e == cudaSuccess) fs<<<grid_s, kBlock>>>(k, a, round);
+                if (e == cudaSuccess) e = cudaGetLastError();
+                int pending = 0;
+                if (e == cudaSuccess) e = cudaMemcpy(&pending, a.pending, sizeof(int), cudaMemcpyDeviceToHost);
+                if (!pending) break;
+            }
+            unsigned long long steps = 0;
+            if (e == cudaSuccess) e = cudaMemcpy(&steps, d_kcnt + CNT_STEPS, sizeof(steps), cudaMemcpyDeviceToHost);
+            float tms = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&tms, ev[2], ev[3]);
+            trace_ms += tms;
+            fwd_steps += steps;
+        }
+        cudaEventRecord(ev[1], 0);
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
-        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[0], ev[1]);
         if (e == cudaSuccess) e = cudaMemcpy(grad_out, d_grad, size_t(np) * sizeof(double), cudaMemcpyDeviceToHost);
         if (e == cudaSuccess) e = cudaMemcpy(c, d_cnt, sizeof(c), cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) rc = set_error(SMP_ERR_CUDA, "adjoint: %s", cudaGetErrorString(e));
@@ -1408,23 +1489,16 @@ int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, in
         stats_out->skipped = (int64_t)c[ADJ_SKIPPED];
         stats_out->aborted = (int64_t)c[ADJ_ABORTED];
         stats_out->replay_mismatch = (int64_t)c[ADJ_MISMATCH];
-        stats_out->er_steps_forward = (int64_t)c[ADJ_STEPS_FWD];
+        stats_out->er_steps_forward = (int64_t)fwd_steps;
         stats_out->er_steps_replay = (int64_t)c[ADJ_STEPS_REPLAY];
         stats_out->points = (int64_t)c[ADJ_POINTS];
         stats_out->splats = (int64_t)c[ADJ_SPLATS];
         stats_out->kernel_ms = ms;
+        stats_out->trace_ms = trace_ms;
     }
-    if (e0) cudaEventDestroy(e0);
-    if (e1) cudaEventDestroy(e1);
-    cudaFree(d_G);
-    cudaFree(d_grad);
-    cudaFree(d_traj);
-    cudaFree(d_verts);
-    cudaFree(d_cnt);
+    for (int i = 0; i < 4; ++i) if (ev[i]) cudaEventDestroy(ev[i]);
     if (!rc && c[ADJ_MISMATCH])
-        rc = set_error(SMP_ERR_CUDA, "internal: %llu segment replay(s) diverged from their checkpoint "
-                       "(connection %llu, move %llu, direct %llu, position %llu, direction %llu)",
-                       c[ADJ_MISMATCH], c[ADJ_MIS_CONN], c[ADJ_MIS_MOVE], c[ADJ_MIS_DIRECT], c[ADJ_MIS_POS], c[ADJ_MIS_DIR]);
+        rc = set_error(SMP_ERR_CUDA, "internal: %llu segment replay(s) diverged from their checkpoint", c[ADJ_MISMATCH]);
     return rc;
 }
 

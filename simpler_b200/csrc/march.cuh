@@ -414,6 +414,8 @@ struct NoHook {
     static constexpr bool on = false;
     __device__ bool at(Lane &, int) { return false; }
     __device__ void splatted(const Lane &, float3, double, int, float) {}
+    __device__ void photon_begin(const Lane &) {}
+    __device__ void photon_end(const Lane &) {}
 };
 
 // Runs the lane's events until it starts a march (returns ST_MARCH) or its photon ends
@@ -722,8 +724,10 @@ __device__ __noinline__ bool stage_to_shared(void *dst, const void *src, unsigne
 // from the global counter, one atomic per warp) alternating with the march phase (two ER steps per
 // vote until event_batch lanes, scaled by the live lanes, wait for events). A lane enters with
 // `st` = ST_FETCH (no photon) or ST_MARCH (a photon loaded mid-march). All 32 lanes call it.
-template <int FK>
-__device__ __forceinline__ void lane_loop(Lane &L, int st, const KParams &P, LaneStats &S, int lane) {
+// A hook (adjoint.cuh's checkpointing trace) also sees each photon's start and end; the render
+// kernels use NoHook.
+template <int FK, class H = NoHook>
+__device__ __forceinline__ void lane_loop(Lane &L, int st, const KParams &P, LaneStats &S, int lane, H *h = nullptr) {
     int pending_ev = EV_NEW;
     for (;;) {
         for (;;) {
@@ -740,14 +744,18 @@ __device__ __forceinline__ void lane_loop(Lane &L, int st, const KParams &P, Lan
                         L.end = 0;                       // the previous photon's end code
                         st = ST_EVENT;
                         pending_ev = EV_NEW;
+                        if (H::on) h->photon_begin(L);
                     } else {
                         st = ST_DONE;
                     }
                 }
             }
             if (st == ST_EVENT) {
-                st = run_events<FK>(L, P, pending_ev);
-                if (st == ST_FETCH) finish_photon_stats<FK>(L, S);
+                st = run_events<FK, H>(L, P, pending_ev, h);
+                if (st == ST_FETCH) {
+                    finish_photon_stats<FK>(L, S);
+                    if (H::on) h->photon_end(L);
+                }
             }
             if (!__any_sync(kFull, st == ST_FETCH)) break;
         }

@@ -20,6 +20,16 @@ add/sub/mul/div/sqrt and one per transcendental call (jn, atan2, sin, cos):
                        accumulation (11) (spline.h:415-448, separable)                          = 400
                        scale of the gradient (3) + base (1)                                      = 4
                        479, 513 FLOP/step
+
+The adjoint's backward sweep visits every recorded point once (adjoint.cuh): n, grad n and the
+Hessian there, the parameter vector-Jacobian product, and the step's own adjoint algebra
+(dh, d_prev, Dh, a, b, P += a g + H b for both kicks, about 80 FLOP):
+  plane waves (each)   phase (7) + sin, cos (2) + n (2) + grad (7) + Hessian (13)                 = 31
+                       parameter product: phase (7) + sin, cos (2) + k.b (5) + two sums (7)      = 21
+  tricubic spline      weights of three orders on three axes (72), 16 rows x (three 4-tap sums
+                       (21) + ten accumulations (20) + products (3)) (704), scaling (15)        = 791
+                       parameter product: weights (72) + 16 rows x (row factors (10) + 4 taps
+                       (12)) (352)                                                              = 424
 """
 
 FLOP_LEAPFROG = 24
@@ -47,3 +57,16 @@ def flop_per_step(setup) -> int:
     if setup.field_type == L.FIELD_SPLINE:
         return flop_per_step_spline()
     return flop_per_step_bessel(setup.mode)
+
+
+FLOP_ADJ_STEP = 80
+
+
+def flop_per_point_adjoint(setup) -> int:
+    """FLOP per point of the adjoint's backward sweep."""
+    from . import _lib as L
+    if setup.field_type == L.FIELD_PLANEWAVE:
+        return FLOP_ADJ_STEP + (31 + 21) * len(setup.wave_amp)
+    if setup.field_type == L.FIELD_SPLINE:
+        return FLOP_ADJ_STEP + 791 + 424
+    raise ValueError("the adjoint is built for plane-wave and spline fields")

@@ -111,7 +111,7 @@ def test_param_layout():
 
 
 def test_adjoint_stats_layout():
-    assert sb.check_layout()["smp_adjoint_stats"][0] == 80
+    assert sb.check_layout()["smp_adjoint_stats"][0] == 88
 
 
 # ---- GPU -----------------------------------------------------------------------------------------
