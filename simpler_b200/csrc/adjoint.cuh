@@ -125,6 +125,8 @@ struct AdjVertex {             // a checkpoint (source: index 0, scatter vertex 
     int draws_so, steps_so;    // the same at EV_SCATTER_ONCE (source: at EV_SCATTER)
     int hits;                  // the splat that follows lands where dJ/dfilm is nonzero: bit 0 the
                                // connection from this vertex, bit 1 (source) the direct splat
+    int len_in;                // trajectory entries of the move into this vertex (source: the direct march)
+    int len_conn;              // trajectory entries of the connection from this vertex
     int pad;
     double total;              // optical path length
 };
@@ -207,6 +209,7 @@ template <int FK> struct FieldAdj;
 // for the cotangent (a, b) of (n, grad n). Gradient layout: a_0..a_{W-1}, phase_0..phase_{W-1}.
 template <> struct FieldAdj<FK_PLANEWAVE> {
     struct Acc { float ga[SMP_MAX_WAVES], gp[SMP_MAX_WAVES]; };
+    struct Cache { float sn[SMP_MAX_WAVES], cs[SMP_MAX_WAVES]; int gap; };   // eval_h -> theta_c at one point
     static __device__ __forceinline__ void clear(Acc &c) {
 #pragma unroll
         for (int i = 0; i < SMP_MAX_WAVES; ++i) { c.ga[i] = 0.0f; c.gp[i] = 0.0f; }
@@ -245,6 +248,42 @@ template <> struct FieldAdj<FK_PLANEWAVE> {
             }
         }
     }
+    // the same pair with the sines and cosines computed once
+    static __device__ __forceinline__ void eval_h(const FieldParams &F, float3 p, float tau, float &n, float3 &g, float H[6],
+                                                  Cache &k) {
+#pragma unroll
+        for (int j = 0; j < 6; ++j) H[j] = 0.0f;
+        n = F.n_o;
+        g = f3(0.0f, 0.0f, 0.0f);
+        k.gap = in_gap(F, p);
+        if (k.gap) return;
+#pragma unroll
+        for (int i = 0; i < SMP_MAX_WAVES; ++i) {
+            if (i < F.n_waves) {
+                const float kx = F.wk[i][0], ky = F.wk[i][1], kz = F.wk[i][2];
+                float sn, cs;
+                sincos_red(kx * p.x + ky * p.y + kz * p.z - tau + F.wphase[i], sn, cs);
+                k.sn[i] = sn; k.cs[i] = cs;
+                n += F.wamp[i] * sn;
+                const float ac = F.wamp[i] * cs, as = -F.wamp[i] * sn;
+                g.x += ac * kx; g.y += ac * ky; g.z += ac * kz;
+                H[0] += as * kx * kx; H[1] += as * ky * ky; H[2] += as * kz * kz;
+                H[3] += as * kx * ky; H[4] += as * kx * kz; H[5] += as * ky * kz;
+            }
+        }
+    }
+    static __device__ __forceinline__ void theta_c(const FieldParams &F, float3, float, float a, float3 b, Acc &c,
+                                                   const AdjParams &, const Cache &k) {
+        if (k.gap) return;
+#pragma unroll
+        for (int i = 0; i < SMP_MAX_WAVES; ++i) {
+            if (i < F.n_waves) {
+                const float kb = F.wk[i][0] * b.x + F.wk[i][1] * b.y + F.wk[i][2] * b.z;
+                c.ga[i] += a * k.sn[i] + k.cs[i] * kb;
+                c.gp[i] += F.wamp[i] * (a * k.cs[i] - k.sn[i] * kb);
+            }
+        }
+    }
     static __device__ __forceinline__ void flush(const Acc &c, const FieldParams &F, const AdjParams &A) {
 #pragma unroll
         for (int i = 0; i < SMP_MAX_WAVES; ++i) {
@@ -270,6 +309,7 @@ __device__ __forceinline__ void bspline_dd(float t, float dd[4]) {
 }
 template <> struct FieldAdj<FK_SPLINE> {
     struct Acc {};
+    struct Cache {};
     static __device__ __forceinline__ void clear(Acc &) {}
     static __device__ __forceinline__ void taps(const FieldParams &F, float3 p, float wx[4], float wy[4], float wz[4],
                                                 float dx[4], float dy[4], float dz[4], float ddx[4], float ddy[4],
@@ -338,6 +378,14 @@ template <> struct FieldAdj<FK_SPLINE> {
             }
         }
     }
+    static __device__ __forceinline__ void eval_h(const FieldParams &F, float3 p, float s, float &n, float3 &g, float H[6],
+                                                  Cache &) {
+        eval_h(F, p, s, n, g, H);
+    }
+    static __device__ __forceinline__ void theta_c(const FieldParams &F, float3 p, float s, float a, float3 b, Acc &c,
+                                                   const AdjParams &A, const Cache &) {
+        theta(F, p, s, a, b, c, A);
+    }
     static __device__ __forceinline__ void flush(const Acc &, const FieldParams &, const AdjParams &) {}
 };
 
@@ -370,6 +418,8 @@ struct AdjTraceHook {
     AdjVertex *v;              // this thread's checkpoints
     int nv, vcap, overflow;
     int direct_hit;
+    int seg_entries;           // trajectory entries of the current segment: its start, one marker per
+                               // later march, one per accepted step
     unsigned long long nok, ndrop, nabort;
     __device__ void put(int k, const Lane &L) {
         AdjVertex &c = v[k];
@@ -381,8 +431,14 @@ struct AdjTraceHook {
         c.draws_v = L.draws; c.steps_v = L.steps;
         c.draws_so = L.draws; c.steps_so = L.steps;
         c.hits = 0;
+        c.len_in = seg_entries;
+        c.len_conn = 0;
     }
-    __device__ void photon_begin(const Lane &) { nv = 0; overflow = 0; direct_hit = 0; }
+    __device__ void photon_begin(const Lane &) { nv = 0; overflow = 0; direct_hit = 0; seg_entries = 0; }
+    __device__ void march_begin() { ++seg_entries; }
+    __device__ void accepted() { ++seg_entries; }
+    // each hook ends a segment: the direct march at EV_SCATTER, a move at EV_VERTEX, a connection
+    // at EV_SCATTER_ONCE
     __device__ bool at(Lane &L, int ev) {
         if (ev == EV_SCATTER) {
             put(0, L);
@@ -395,7 +451,9 @@ struct AdjTraceHook {
         } else if (ev == EV_SCATTER_ONCE && nv - 1 < vcap && nv >= 1) {
             v[nv - 1].draws_so = L.draws;
             v[nv - 1].steps_so = L.steps;
+            v[nv - 1].len_conn = seg_entries;
         }
+        seg_entries = 0;
         return false;
     }
     __device__ void splatted(const Lane &, float3 p, double pl, int depth, float) {
@@ -413,19 +471,18 @@ struct AdjTraceHook {
         else if (overflow) { r.status = PH_DROPPED; ++ndrop; }
         else {
             r.status = PH_OK;
-            // the segments the sweep needs: connections that reach dJ/dfilm, every move up to the
-            // last of them, the direct march if it does; a segment of n er_steps records at most
-            // 2n + 1 trajectory entries (its start, accepted steps, one marker per later march)
+            // the segments the sweep needs, with their exact trajectory entries: connections that
+            // reach dJ/dfilm, every move up to the last of them, the direct march if it does
             int hits = 0, last = 0;
             long long tlen = 0;
             for (int k = 0; k < nv; ++k) {
                 hits |= v[k].hits;
                 if (k >= 1 && (v[k].hits & 1)) last = k;
             }
-            if (v[0].hits & 2) tlen += 2LL * v[0].steps_so + 1;
+            if (v[0].hits & 2) tlen += v[0].len_in;
             for (int k = 1; k < nv; ++k) {
-                if (k <= last) tlen += 2LL * (v[k].steps_v - v[k - 1].steps_so) + 1;
-                if (v[k].hits & 1) tlen += 2LL * (v[k].steps_so - v[k].steps_v) + 1;
+                if (k <= last) tlen += v[k].len_in;
+                if (v[k].hits & 1) tlen += v[k].len_conn;
             }
             r.hits = hits;
             r.last = last;
@@ -507,7 +564,8 @@ __device__ __forceinline__ void sweep_begin(Sweep &w, const KParams &P, const Ad
     const float3 pk = f3(w.e.x, w.e.y, w.e.z);
     float n_k, H[6];
     float3 g_k;
-    FieldAdj<FK>::eval_h(F, pk, s, n_k, g_k, H);
+    typename FieldAdj<FK>::Cache kc;
+    FieldAdj<FK>::eval_h(F, pk, s, n_k, g_k, H, kc);
     const float3 u = divs(md_end, n_k);
     const float At = dot3(u, Pa) + dot3(g_k, Da) + dot3(g_k, u) * a_end;
     if (face_end) {
@@ -519,7 +577,7 @@ __device__ __forceinline__ void sweep_begin(Sweep &w, const KParams &P, const Ad
     // second kick of the last step, and the end point's own use of n
     const float3 b = mul(Da, 0.5f * w.e.w);
     Pa = add(Pa, add(mul(g_k, a_end), hmul(H, b)));
-    FieldAdj<FK>::theta(F, pk, s, a_end, b, acc, A);
+    FieldAdj<FK>::theta_c(F, pk, s, a_end, b, acc, A, kc);
     w.d = md_end; w.gk = g_k; w.Pa = Pa; w.Da = Da; w.T = T;
 }
 
@@ -541,7 +599,8 @@ __device__ __forceinline__ int sweep_point(Sweep &w, const KParams &P, const Adj
     const float3 pp = f3(pe.x, pe.y, pe.z);
     float n1, H[6];
     float3 g1;
-    FieldAdj<FK>::eval_h(F, pp, s, n1, g1, H);
+    typename FieldAdj<FK>::Cache kc;
+    FieldAdj<FK>::eval_h(F, pp, s, n1, g1, H, kc);
     const float3 dh = sub(w.d, mul(w.gk, hh));
     const float3 dprev = sub(dh, mul(g1, hh));
     const float q = c / n1;
@@ -571,7 +630,7 @@ __device__ __forceinline__ int sweep_point(Sweep &w, const KParams &P, const Adj
     const float3 b2 = mul(Da, 0.5f * pe.w);
     Pa = add(Pa, hmul(H, b2));
     b1 = add(b1, b2);
-    FieldAdj<FK>::theta(F, pp, s, a1, b1, acc, A);
+    FieldAdj<FK>::theta_c(F, pp, s, a1, b1, acc, A, kc);
     w.Pa = Pa; w.Da = Da;
     w.i = j;
     w.e = pe;
@@ -585,7 +644,7 @@ __device__ __forceinline__ int sweep_point(Sweep &w, const KParams &P, const Adj
 // (directTracing photon.cpp:41-87; addEnergyInParticle scene.cpp:866-946; propagate_till_sensor
 // camera.cpp:54-75 without a lens) and the bilinear split of addEnergyToImage with the base
 // pixel (ix, iy) held fixed. Returns dJ/d(inputs) for J = value * sum_taps G w.
-__device__ __noinline__ void sensor_grad(const KParams &P, int X, float weight, float sigma_t, float g, bool connect,
+static __device__ __noinline__ void sensor_grad(const KParams &P, int X, float weight, float sigma_t, float g, bool connect,
                                          float3 p, float3 md, float n, float d2s, float3 dv, int ix, int iy,
                                          float G00, float G10, float G01, float G11, float *out) {
     typedef Dual<11> D;
@@ -635,7 +694,7 @@ __device__ __noinline__ void sensor_grad(const KParams &P, int X, float weight, 
 
 // Jacobian^T of the scatterOnce direction update (photon.cpp:20-38: v' = |v| HG(v/|v|), the HG
 // sample drawn in the frame of util::coordinateSystem, util.h:17-27) applied to D.
-__device__ __noinline__ float3 hg_vjp(float3 v, float cosT, float sinT, float cP, float sP, float3 Dout) {
+static __device__ __noinline__ float3 hg_vjp(float3 v, float cosT, float sinT, float cP, float sP, float3 Dout) {
     typedef Dual<3> D;
     D x = dvar<3>(v.x, 0), y = dvar<3>(v.y, 1), z = dvar<3>(v.z, 2);
     D mag = dsqrt(x * x + y * y + z * z);
@@ -856,8 +915,11 @@ __global__ void __launch_bounds__(128, 3) adjoint_replay_kernel(const __grid_con
 // until few lanes are left sweeping.
 enum AdjJob : int { JOB_CONN = 1, JOB_MOVE = 2, JOB_DIRECT = 3, JOB_SOURCE = 4 };
 
+typedef void (*AdjRoundFn)(KParams, AdjParams, int);
+AdjRoundFn adjoint_sweep_fn(int fk);     // adjoint_sweep.cu
+
 template <int FK>
-__global__ void __launch_bounds__(128) adjoint_sweep_kernel(const __grid_constant__ KParams P,
+__global__ void __launch_bounds__(128, 3) adjoint_sweep_kernel(const __grid_constant__ KParams P,
                                                             const __grid_constant__ AdjParams A, int round) {
     const FieldParams &F = P.field;
     Lane L;                                     // Philox draws of the HG rotation

@@ -1324,7 +1324,6 @@ int64_t smp_adjoint_param_count(const smp_field_desc *f) {
 }
 
 typedef void (*AdjFn)(KParams, AdjParams);
-typedef void (*AdjRoundFn)(KParams, AdjParams, int);
 static AdjFn adjoint_trace_fn(int fk) {
     switch (fk) {
         case FK_PLANEWAVE: return adjoint_trace_kernel<FK_PLANEWAVE>;
@@ -1336,13 +1335,6 @@ static AdjRoundFn adjoint_replay_fn(int fk) {
     switch (fk) {
         case FK_PLANEWAVE: return adjoint_replay_kernel<FK_PLANEWAVE>;
         case FK_SPLINE: return adjoint_replay_kernel<FK_SPLINE>;
-        default: return nullptr;
-    }
-}
-static AdjRoundFn adjoint_sweep_fn(int fk) {
-    switch (fk) {
-        case FK_PLANEWAVE: return adjoint_sweep_kernel<FK_PLANEWAVE>;
-        case FK_SPLINE: return adjoint_sweep_kernel<FK_SPLINE>;
         default: return nullptr;
     }
 }
@@ -1388,7 +1380,7 @@ int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, in
     std::memset(&a, 0, sizeof(a));
     a.X = plan->kp.X; a.Y = plan->kp.Y; a.Z = plan->kp.Z;
     a.vcap = env_int("SMP_ADJ_VCAP", 256, 2, 1 << 20);
-    const long long batch = env_int("SMP_ADJ_BATCH", 1 << 19, 1024, 1 << 30);
+    const long long batch = env_int("SMP_ADJ_BATCH", 1 << 21, 1024, 1 << 30);
     const long long per_photon = env_int("SMP_ADJ_POOL_PER_PHOTON", 16, 1, 4096);
     a.pool_cap = batch * per_photon;
     a.traj_cap = (long long)env_int("SMP_ADJ_TRAJ_MB", 8192, 16, 1 << 20) * (1LL << 20) / (long long)sizeof(float4);

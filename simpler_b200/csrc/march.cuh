@@ -96,7 +96,7 @@ __device__ __forceinline__ void philox_block(unsigned &c0, unsigned &c1, unsigne
 }
 
 // one Philox block, kept out of line: draw() is called from many places in the event code
-__device__ __noinline__ uint4 philox_refill(unsigned blk, unsigned ph_lo, unsigned ph_hi, unsigned k0, unsigned k1) {
+static __device__ __noinline__ uint4 philox_refill(unsigned blk, unsigned ph_lo, unsigned ph_hi, unsigned k0, unsigned k1) {
     unsigned c0 = blk, c1 = 0u, c2 = ph_lo, c3 = ph_hi;
     philox_block(c0, c1, c2, c3, k0, k1);
     return make_uint4(c0, c1, c2, c3);
@@ -416,6 +416,8 @@ struct NoHook {
     __device__ void splatted(const Lane &, float3, double, int, float) {}
     __device__ void photon_begin(const Lane &) {}
     __device__ void photon_end(const Lane &) {}
+    __device__ void march_begin() {}
+    __device__ void accepted() {}
 };
 
 // Runs the lane's events until it starts a march (returns ST_MARCH) or its photon ends
@@ -695,7 +697,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity,
     }
     return false;
 }
-__device__ __noinline__ bool stage_to_shared(void *dst, const void *src, unsigned bytes, unsigned long long *err) {
+static __device__ __noinline__ bool stage_to_shared(void *dst, const void *src, unsigned bytes, unsigned long long *err) {
     __shared__ __align__(8) unsigned long long bar;
     const unsigned b = smem_u32(&bar);
     if (threadIdx.x == 0) {
@@ -756,6 +758,7 @@ __device__ __forceinline__ void lane_loop(Lane &L, int st, const KParams &P, Lan
                     finish_photon_stats<FK>(L, S);
                     if (H::on) h->photon_end(L);
                 }
+                if (H::on && st == ST_MARCH) h->march_begin();
             }
             if (!__any_sync(kFull, st == ST_FETCH)) break;
         }
@@ -764,9 +767,19 @@ __device__ __forceinline__ void lane_loop(Lane &L, int st, const KParams &P, Lan
         const int thr = max(1, (P.event_batch * __popc(alive) + 16) >> 5);
         for (;;) {
             // two steps per vote; a lane whose march ends on the first skips the second
-            if (st == ST_MARCH && (march_step<FK>(L, P) || march_step<FK>(L, P))) {
-                st = ST_EVENT;
-                pending_ev = EV_MARCH_END;
+            if (!H::on) {
+                if (st == ST_MARCH && (march_step<FK>(L, P) || march_step<FK>(L, P))) {
+                    st = ST_EVENT;
+                    pending_ev = EV_MARCH_END;
+                }
+            } else if (st == ST_MARCH) {
+                // the same two steps, telling the hook which ones were accepted
+                for (int t = 0; t < 2; ++t) {
+                    const float3 q = L.mp;
+                    const bool end = march_step<FK>(L, P);
+                    if (q.x != L.mp.x || q.y != L.mp.y || q.z != L.mp.z) h->accepted();
+                    if (end) { st = ST_EVENT; pending_ev = EV_MARCH_END; break; }
+                }
             }
             const unsigned waiting = __ballot_sync(kFull, st == ST_EVENT);
             if (__popc(waiting) >= thr || !__any_sync(kFull, st == ST_MARCH)) break;
