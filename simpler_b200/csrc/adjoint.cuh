@@ -338,12 +338,20 @@ template <> struct FieldAdj<FK_SPLINE> {
         taps(F, p, wx, wy, wz, dx, dy, dz, ddx, ddy, ddz, ix, iy, iz);
         float v = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
         float hxx = 0.0f, hyy = 0.0f, hzz = 0.0f, hxy = 0.0f, hxz = 0.0f, hyz = 0.0f;
+        const int fx = int(floorf((p.x - F.xmin[0]) * F.xres[0]));
+        const bool quad = F.coeff4 != nullptr && unsigned(fx) < unsigned(F.N[0]);
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
-                const float *row = F.coeff + iz[c] + iy[b];
-                const float r0 = __ldg(row + ix[0]), r1 = __ldg(row + ix[1]), r2 = __ldg(row + ix[2]), r3 = __ldg(row + ix[3]);
+                float r0, r1, r2, r3;
+                if (quad) {
+                    const float4 q = __ldg(F.coeff4 + (iz[c] + iy[b] + fx));
+                    r0 = q.x; r1 = q.y; r2 = q.z; r3 = q.w;
+                } else {
+                    const float *row = F.coeff + iz[c] + iy[b];
+                    r0 = __ldg(row + ix[0]); r1 = __ldg(row + ix[1]); r2 = __ldg(row + ix[2]); r3 = __ldg(row + ix[3]);
+                }
                 const float sv = r0 * wx[0] + r1 * wx[1] + r2 * wx[2] + r3 * wx[3];
                 const float sd = r0 * dx[0] + r1 * dx[1] + r2 * dx[2] + r3 * dx[3];
                 const float sdd = r0 * ddx[0] + r1 * ddx[1] + r2 * ddx[2] + r3 * ddx[3];

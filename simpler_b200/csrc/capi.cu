@@ -121,6 +121,24 @@ static void source_centres(const smp_field_desc &f, std::vector<float4> &out) {
     }
 }
 
+// The offsets as x-tap quads (FieldParams.coeff4): entry row * N0 + x holds the offsets at the
+// mirrored x - 1, x, x + 1, x + 2 of that row, the four taps of a point with floor(t_x) = x.
+static int spline_mirror(int i, int n) {
+    int m = 2 * n - 2, w = i % m;
+    if (w < 0) w += m;
+    return w >= n ? m - w : w;
+}
+static void spline_quads(const int N[3], const std::vector<float> &delta, std::vector<float4> &quads) {
+    const size_t rows = size_t(N[1]) * N[2];
+    quads.resize(rows * N[0]);
+    for (size_t r = 0; r < rows; ++r)
+        for (int x = 0; x < N[0]; ++x) {
+            const float *row = delta.data() + r * N[0];
+            quads[r * N[0] + x] = make_float4(row[spline_mirror(x - 1, N[0])], row[x], row[spline_mirror(x + 1, N[0])],
+                                              row[spline_mirror(x + 2, N[0])]);
+        }
+}
+
 // Spline coefficients as float offsets from their mean (see spline_field in dev_field.cuh).
 static float spline_offsets(const smp_field_desc &f, std::vector<float> &delta) {
     size_t n = size_t(f.grid_n[0]) * f.grid_n[1] * f.grid_n[2];
@@ -399,6 +417,7 @@ struct smp_plan {
     float *d_cdf = nullptr;
     float4 *d_centers = nullptr;
     float *d_coeff = nullptr;
+    float4 *d_coeff4 = nullptr;
     float4 *d_btab = nullptr;
     size_t smem_bytes = 0;
     int event_batch = 8;
@@ -451,6 +470,7 @@ static void plan_free(smp_plan *p) {
     cudaFree(p->d_cdf);
     cudaFree(p->d_centers);
     cudaFree(p->d_coeff);
+    cudaFree(p->d_coeff4);
     cudaFree(p->d_btab);
     cudaFree(p->d_film);
     cudaFree(p->d_counters);
@@ -504,6 +524,13 @@ static int plan_setup_field(smp_plan *p, const smp_field_desc &f) {
         SMP_CUDA(cudaMalloc(&p->d_coeff, delta.size() * sizeof(float)));
         SMP_CUDA(cudaMemcpy(p->d_coeff, delta.data(), delta.size() * sizeof(float), cudaMemcpyHostToDevice));
         p->kp.field.coeff = p->d_coeff;
+        std::vector<float4> quads;
+        spline_quads(f.grid_n, delta, quads);
+        cudaFree(p->d_coeff4);
+        p->d_coeff4 = nullptr;
+        SMP_CUDA(cudaMalloc(&p->d_coeff4, quads.size() * sizeof(float4)));
+        SMP_CUDA(cudaMemcpy(p->d_coeff4, quads.data(), quads.size() * sizeof(float4), cudaMemcpyHostToDevice));
+        p->kp.field.coeff4 = p->d_coeff4;
     }
     p->smem_bytes = 0;
     if (p->fk <= FK_BESSEL2) {

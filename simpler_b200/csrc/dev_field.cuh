@@ -162,6 +162,7 @@ __device__ __forceinline__ void sources_field(const FieldParams &F, float3 p, fl
 // n = base + sum(delta w), grad n = sum(delta w'). Summing the raw coefficients (~1.33) in FP32,
 // as the reference does, cancels about four digits of a 1e-3 gradient signal.
 __device__ __forceinline__ int spline_wrap(int i, int n) {
+    if (unsigned(i) < unsigned(n)) return i;     // inside the grid: the common case
     int m = 2 * n - 2;
     int w = i % m;
     if (w < 0) w += m;
@@ -202,12 +203,21 @@ __device__ __forceinline__ void spline_field(const FieldParams &F, float3 p, flo
         iz[a] = spline_wrap(bz + a, N2) * N0 * N1;
     }
     float v = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f;
+    // x-tap quads: one 16-byte load per row when floor(t_x) lies on the grid (same values, same
+    // sums as the four single loads)
+    const bool quad = F.coeff4 != nullptr && unsigned(bx + 1) < unsigned(N0);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
-            const float *row = F.coeff + iz[c] + iy[b];
-            float r0 = __ldg(row + ix[0]), r1 = __ldg(row + ix[1]), r2 = __ldg(row + ix[2]), r3 = __ldg(row + ix[3]);
+            float r0, r1, r2, r3;
+            if (quad) {
+                const float4 q = __ldg(F.coeff4 + (iz[c] + iy[b] + bx + 1));
+                r0 = q.x; r1 = q.y; r2 = q.z; r3 = q.w;
+            } else {
+                const float *row = F.coeff + iz[c] + iy[b];
+                r0 = __ldg(row + ix[0]); r1 = __ldg(row + ix[1]); r2 = __ldg(row + ix[2]); r3 = __ldg(row + ix[3]);
+            }
             float sv = r0 * wx[0] + r1 * wx[1] + r2 * wx[2] + r3 * wx[3];
             float sd = r0 * dx[0] + r1 * dx[1] + r2 * dx[2] + r3 * dx[3];
             float wyz = wy[b] * wz[c];

@@ -44,6 +44,9 @@ struct FieldParams {
     float xmin[3], xres[3];
     float spline_base;      // coefficients are stored as offsets from this value
     const float *coeff;
+    const float4 *coeff4;   // the same offsets as x-tap quads: coeff4[row * N0 + x] holds the
+                            // coefficients at mirrored x-1, x, x+1, x+2 of that (y, z) row (NULL:
+                            // read coeff tap by tap)
     // Bessel table: for interval i of width bh, btab[2i] / btab[2i+1] hold the cubics of J_m /
     // J_m+1 in f = x/bh - i; bint intervals, bnodes = 2 * bint float4 entries
     const float4 *btab;
