@@ -190,14 +190,19 @@ def cpu_trace(n: int, first: int, threads: int) -> float:
 
 
 def cpu_baseline(target_s: float = 12.0) -> dict:
-    """Trace batches of the workload on all host threads until about target_s of wall time."""
+    """Trace batches of the workload on all host threads until about target_s of wall time: one
+    photon per thread first, then batches doubling while the next one fits in the time left (a
+    photon of the point-source field costs seconds on the CPU)."""
     threads = os.cpu_count() or 1
-    batch = max(threads * 16, 64)
+    batch = threads
     done, dt, first = 0, 0.0, 0
     while dt < target_s and done < 2_000_000:
-        dt += cpu_trace(batch, first, threads)
+        t = cpu_trace(batch, first, threads)
+        dt += t
         done += batch
         first += batch
+        if 2.0 * t < target_s - dt:
+            batch *= 2
     return {"value": done / dt, "unit": METRIC, "cores": threads, "kind": "port",
             "sample": f"photons 0..{done} of the same workload ({done} photon paths) in {dt:.1f} s on all "
                       f"{threads} host threads, CPU restatement built with the reference's -O3 -ffast-math "
@@ -300,7 +305,7 @@ def run_ours(args):
         # this stream inside the library, and it counts the steps it executes
         n_march = max(1, st1.march_launches - st0.march_launches)
         achieved = fps * march_steps / (march_ms / 1e3) / 1e12
-        kname = {L.FIELD_PLANEWAVE: "FK_PLANEWAVE", L.FIELD_SPLINE: "FK_SPLINE"}.get(
+        kname = {L.FIELD_PLANEWAVE: "FK_PLANEWAVE", L.FIELD_SPLINE: "FK_SPLINE", L.FIELD_SOURCES: "FK_SOURCES"}.get(
             setup.field_type, f"FK_BESSEL{setup.mode}")
         form = "fp64 path length" if setup.precision_mode == L.PREC_MIXED else "fp32"
         roof = {"bound": "fp32", "kernel": f"wf_march_kernel<{kname}, {form}>",

@@ -49,9 +49,20 @@ def flop_per_step_spline() -> int:
     return FLOP_LEAPFROG + FLOP_BOOKKEEPING + 75 + 400 + 4
 
 
+def flop_per_step_sources(n_coeff: int, n_sources: int, arcs: int) -> int:
+    """Point sources (scene.cpp:139-195): per source and harmonic, offset (3), squared distance
+    (5), 1/r and r (2), k r c (2), phase + sin, cos (3), value sum (2), radial factor (5),
+    gradient sums (6) = 28; per harmonic its weight and the two sums (10); n and the scaled
+    gradient (5)."""
+    return FLOP_LEAPFROG + FLOP_BOOKKEEPING + n_coeff * (28 * arcs * n_sources + 10) + 5
+
+
 def flop_per_step(setup) -> int:
     """FLOP per ER step of a Setup's field."""
     from . import _lib as L
+    if setup.field_type == L.FIELD_SOURCES:
+        arcs = int(bool(setup.active1)) + int(bool(setup.active2))
+        return flop_per_step_sources(setup.n_coeff, setup.theta_sources * setup.trans_z_sources, arcs)
     if setup.field_type == L.FIELD_PLANEWAVE:
         return flop_per_step_planewave(len(setup.wave_amp))
     if setup.field_type == L.FIELD_SPLINE:

@@ -239,6 +239,17 @@ def config_planewave(**kw) -> Setup:
     return s
 
 
+def config_sources(**kw) -> Setup:
+    """The focused-ultrasound point-source field (rif_sources) with the reference's source layout:
+    two arcs of radius 2 in with a 0.5 in chord, 100 x 501 point sources each, centred 2 in behind
+    the medium on the -x axis, first harmonic, n_scaling 5e-5; medium, beam and film of
+    config_plain_small."""
+    s = Setup(field_type=L.FIELD_SOURCES)
+    for kk, v in kw.items():
+        setattr(s, kk, v)
+    return s
+
+
 def config_batch_sweep(n_inst: int = 256, seed: int = 2, scale: float = 1.0, **kw):
     """The batched sweep: n_inst cylindrical-transducer instances over the plain small scene
     (medium, optics and 128x128 x 32 film of config_plain_small), with amplitude n_max ~ U[0, 2e-3],
