@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--photons-per-step", type=int, default=PHOTONS_PER_STEP)
-    ap.add_argument("--workload", choices=["precision", "sweep", "plain", "planewave", "spline", "adjoint",
+    ap.add_argument("--workload", choices=["precision", "sweep", "plain", "planewave", "spline", "sources", "adjoint",
                                            "adjoint-spline"], default="precision",
                     help="precision: the headline line (default); sweep: the batched 256-instance sweep "
                          "against the same instances rendered one by one; adjoint / adjoint-spline: gradients "
@@ -64,6 +64,10 @@ OTHER = {
     "planewave": (lambda d: sb.config_planewave(device=d), 10_000_000, 10_000_000,
                   "two plane waves a = 1e-3 at 1 MHz along +y and +z, phases U[0, 2 pi) (seed 3), "
                   "sigma_s 0.5/mm, albedo 0.9, g 0.9, 128x128 x 32 bins, fp32, 1e7 photons"),
+    "sources": (lambda d: _sources_grid(d), 2_000_000, 10_000_000,
+                "focused-ultrasound point sources (two 2 in arcs of 100 x 501 sources, first harmonic) sampled "
+                "once on a 96^3 tricubic grid (sources_to_spline, grad n within 7e-4 of the direct sum), medium "
+                "and 128x128 x 32 film of the plain small configuration, fp32; 2e6-photon steps"),
     "spline": (lambda d: sb.config_spline(device=d), 10_000_000, 1_000_000_000,
                "tricubic spline 64^3 over the 10 mm cube (Gaussian-filtered noise, max dn 1e-3, seed 4), "
                "sigma_s 1/mm, albedo 0.95, g 0.8, 256x256 x 64 bins, fp32; 1e7-photon steps of a "
@@ -85,6 +89,14 @@ ADJOINT = {
 }
 
 _ARGS = None           # the parsed command line (set in main)
+_GRIDS = {}
+
+
+def _sources_grid(device: int) -> sb.Setup:
+    """The point-source workload's field on its 96^3 grid, sampled once per device."""
+    if device not in _GRIDS:
+        _GRIDS[device] = sb.sources_to_spline(sb.config_sources(device=device), 96)
+    return _GRIDS[device]
 
 
 def workload(args=None, device: int = 0) -> sb.Setup:

@@ -103,6 +103,10 @@ typedef struct smp_field_desc {
        used when theta_max > theta_min, else derived from chordlength as
        renderer3d_sample.cpp:136-140 does (theta = -+asin(chord/2r), trans_z = -+chord/2) */
     double  theta_min, theta_max, trans_z_min, trans_z_max;
+    /* spline: a value added to every grid_coeff entry (in double), so that a grid of a small
+       field on a large background (n_o + dn, dn ~ 1e-5) keeps dn's full float precision; 0 for the
+       reference's absolute grids */
+    double  grid_offset;
 } smp_field_desc;
 
 /* ---- scene: medium box, textured collimated source, sensor --------------------------------- */

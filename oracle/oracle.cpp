@@ -152,9 +152,9 @@ template <typename R> struct Field {
             double mean = 0.0;
             for (size_t i = 0; i < n; ++i) mean += coeff[i];
             mean /= double(n);
-            base = R(float(mean));
+            base = R(float(f.grid_offset + mean));
             delta.resize(n);
-            for (size_t i = 0; i < n; ++i) delta[i] = R(double(coeff[i]) - double(float(mean)));
+            for (size_t i = 0; i < n; ++i) delta[i] = R(double(coeff[i]) + f.grid_offset - double(float(f.grid_offset + mean)));
         }
     }
 

@@ -59,6 +59,7 @@ class FieldDesc(C.Structure):
         ("grid_coeff", C.POINTER(C.c_float)),
         ("theta_min", C.c_double), ("theta_max", C.c_double),
         ("trans_z_min", C.c_double), ("trans_z_max", C.c_double),
+        ("grid_offset", C.c_double),
     ]
 
 

@@ -145,9 +145,9 @@ static float spline_offsets(const smp_field_desc &f, std::vector<float> &delta) 
     double mean = 0.0;
     for (size_t i = 0; i < n; ++i) mean += f.grid_coeff[i];
     mean /= double(n);
-    float base = float(mean);
+    float base = float(f.grid_offset + mean);
     delta.resize(n);
-    for (size_t i = 0; i < n; ++i) delta[i] = float(double(f.grid_coeff[i]) - double(base));
+    for (size_t i = 0; i < n; ++i) delta[i] = float(double(f.grid_coeff[i]) + f.grid_offset - double(base));
     return base;
 }
 

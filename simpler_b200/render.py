@@ -228,3 +228,35 @@ def adjoint(setup: Setup, n_photons: int, dJ_dfilm: np.ndarray) -> tuple[np.ndar
     L.check(lib.smp_render_adjoint(C.byref(sc), C.byref(md), C.byref(fd), C.byref(op), int(n_photons), _ptr(g),
                                    _ptr(grad), C.byref(st)))
     return grad, st
+
+
+# ---- static fields as a tricubic grid ---------------------------------------------------------
+def sources_to_spline(setup: Setup, n: int = 96, margin: int = 6) -> Setup:
+    """The point-source field of `setup` sampled on an n^3 grid of nodes (with the march's own field
+    code, on the GPU), prefiltered into tricubic B-spline coefficients (smp_spline_prefilter, the
+    reference's Spline<3>::build3d), returned as a spline-field setup: the reference's
+    rif_interpolated route for a field that is fixed in time. Every evaluation then reads 64
+    coefficients instead of summing every point source (1e5 for the reference's arcs). The grid
+    reaches `margin` node spacings beyond the medium box on every side, because the prefilter's
+    mirror boundary flattens the field's normal derivative over the last few nodes. The gaps stay
+    those of `setup`. For the reference's default arcs (1 MHz-scale wavelengths of 1.8 mm in a
+    10 mm box) a 96^3 grid reproduces grad n to 7e-4 and a 128^3 grid to 3e-4 of its largest value;
+    n to the float resolution of n itself."""
+    if setup.field_type != L.FIELD_SOURCES:
+        raise ValueError("sources_to_spline takes a point-source setup")
+    lo = np.asarray(setup.medium_l, dtype=np.float64)
+    hi = np.asarray(setup.medium_r, dtype=np.float64)
+    h = (hi - lo) / (n - 1 - 2 * margin)
+    lo, hi = lo - margin * h, hi + margin * h
+    axes = [np.linspace(lo[i], hi[i], n) for i in range(3)]
+    z, y, x = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    pts = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    # dn = n - n_o at the nodes (n_o = 0 keeps dn's own float precision), no gating at the nodes
+    probe = dataclasses.replace(setup, n_o=0.0, emitter_gap=-1e-3, sensor_gap=-1e-3)
+    vals, _ = field_eval(probe, 0.0, pts)
+    samples = np.ascontiguousarray(vals.reshape(n, n, n), dtype=np.float32)
+    coeff = np.zeros_like(samples)
+    dims = np.array([n, n, n], dtype=np.int32)
+    L.check(L.load().smp_spline_prefilter(_ptr(samples), _ptr(dims), _ptr(coeff)))
+    return dataclasses.replace(setup, field_type=L.FIELD_SPLINE, grid_coeff=coeff, grid_offset=float(setup.n_o),
+                               grid_min=tuple(float(v) for v in lo), grid_max=tuple(float(v) for v in hi))

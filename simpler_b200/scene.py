@@ -98,6 +98,7 @@ class Setup:
     grid_coeff: np.ndarray | None = None
     grid_min: tuple = (0.0, 0.0, 0.0)
     grid_max: tuple = (1.0, 1.0, 1.0)
+    grid_offset: float = 0.0        # added to every coefficient in double (small fields on n_o)
     # renderer
     max_depth: int = -1
     max_pathlength: float = -1.0
@@ -182,6 +183,7 @@ class Setup:
             f.grid_min[:] = self.grid_min
             f.grid_max[:] = self.grid_max
             f.grid_coeff = g.ctypes.data_as(C.POINTER(C.c_float))
+            f.grid_offset = float(self.grid_offset)
         return f
 
     def opts(self) -> L.RenderOpts:
