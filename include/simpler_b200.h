@@ -336,8 +336,9 @@ typedef struct smp_adjoint_stats {
     double  trace_ms;             /* of which the checkpointing trace                               */
 } smp_adjoint_stats;
 /* Number of parameters smp_render_adjoint returns for this field, or a negative smp_status:
-   plane waves 2*n_waves (amplitudes a_0..a_{W-1}, then phases phase_0..phase_{W-1});
-   spline grid_n[0]*grid_n[1]*grid_n[2] coefficients in grid_coeff's order. */
+   Bessel modes 0-2: 3 (n_max, phi_min, phi_max); plane waves 2*n_waves (amplitudes
+   a_0..a_{W-1}, then phases phase_0..phase_{W-1}); spline grid_n[0]*grid_n[1]*grid_n[2]
+   coefficients in grid_coeff's order. */
 int64_t smp_adjoint_param_count(const smp_field_desc *field);
 /* Gradient of J = sum_pixels dJ_dfilm[pixel] * film[pixel] with respect to the field parameters,
    where film is the image smp_render would produce for photons [first_photon, first_photon +
@@ -345,8 +346,8 @@ int64_t smp_adjoint_param_count(const smp_field_desc *field);
    It is the pathwise derivative of that estimator: per photon, random numbers, discrete events
    and ER step sequences are held fixed, and marches ending on a face end on the face plane.
    dJ_dfilm: host, X*Y*Z doubles (Image3 layout); grad_out: host, smp_adjoint_param_count doubles,
-   overwritten. Plane-wave and spline fields, Philox streams, no lenses; others return
-   SMP_ERR_UNSUPPORTED. Synchronous. */
+   overwritten. Bessel (modes 0-2), plane-wave and spline fields, Philox streams, no lenses; others
+   return SMP_ERR_UNSUPPORTED. Synchronous. */
 int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, int64_t weight_photons,
                      const double *dJ_dfilm, double *grad_out, smp_adjoint_stats *stats_out);
 int smp_render_adjoint(const smp_scene_desc *scene, const smp_medium_desc *medium,

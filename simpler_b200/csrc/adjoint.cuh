@@ -1,5 +1,6 @@
 // adjoint.cuh -- reverse-mode derivative of a render's sensor objective with respect to the
-// refractive-index field's parameters (plane-wave amplitudes and phases, spline coefficients).
+// refractive-index field's parameters (Bessel amplitude and phase window, plane-wave amplitudes and phases,
+// spline coefficients).
 //
 // Objective: J = sum_pixels G[pixel] * film[pixel] for a caller-given weight image G (dJ/dfilm;
 // a region-of-interest mask gives ROI throughput). The film is the render's own estimator
@@ -193,6 +194,14 @@ struct AdjParams {
     unsigned long long *cnt;   // AdjCounter
 };
 
+// Position the lane's Philox stream at draw index d (draw k uses word k % 4 of block k / 4).
+__device__ __forceinline__ void rng_seek(Lane &L, const KParams &P, int d) {
+    L.rblk = unsigned(d >> 2);
+    L.rhave = 0;
+    L.draws = d & ~3;
+    for (int i = 0; i < (d & 3); ++i) (void)draw(L, P);
+}
+
 // ---- field: n, grad n, Hessian, and the parameter vector-Jacobian product -------------------------
 // H = (xx, yy, zz, xy, xz, yz).
 __device__ __forceinline__ float3 hmul(const float H[6], float3 b) {
@@ -210,6 +219,7 @@ template <int FK> struct FieldAdj;
 template <> struct FieldAdj<FK_PLANEWAVE> {
     struct Acc { float ga[SMP_MAX_WAVES], gp[SMP_MAX_WAVES]; };
     struct Cache { float sn[SMP_MAX_WAVES], cs[SMP_MAX_WAVES]; int gap; };   // eval_h -> theta_c at one point
+    static __device__ __forceinline__ void begin(Acc &, Lane &, const KParams &, float) {}
     static __device__ __forceinline__ void clear(Acc &c) {
 #pragma unroll
         for (int i = 0; i < SMP_MAX_WAVES; ++i) { c.ga[i] = 0.0f; c.gp[i] = 0.0f; }
@@ -310,6 +320,7 @@ __device__ __forceinline__ void bspline_dd(float t, float dd[4]) {
 template <> struct FieldAdj<FK_SPLINE> {
     struct Acc {};
     struct Cache {};
+    static __device__ __forceinline__ void begin(Acc &, Lane &, const KParams &, float) {}
     static __device__ __forceinline__ void clear(Acc &) {}
     static __device__ __forceinline__ void taps(const FieldParams &F, float3 p, float wx[4], float wy[4], float wz[4],
                                                 float dx[4], float dy[4], float dz[4], float ddx[4], float ddy[4],
@@ -398,6 +409,101 @@ template <> struct FieldAdj<FK_SPLINE> {
 };
 
 // ---- replay hook: checkpoints (phase A), stop at a segment's end (phase B), splat capture ----------
+// Cylindrical Bessel mode m = 0, 1, 2 (scene.cpp:205-257): n = n_o + A f, A = n_max s, f = J_m(k r)
+// cos(m phi), phi = atan2(y, z). In polar form, with e_r = (y, z)/r, e_phi = (z, -y)/r and
+// J'' = -J'/x - (1 - m^2/x^2) J (Bessel's equation):
+//   grad f = f_r e_r + f_phi/r e_phi,
+//   H = f_rr e_r e_r^T + (f_r/r + f_phiphi/r^2) e_phi e_phi^T + (f_rphi/r - f_phi/r^2)(e_r e_phi^T + e_phi e_r^T),
+// with f_r = k J' cos, f_phi = -m J sin, f_rr = k^2 J'' cos, f_rphi = -m k J' sin, f_phiphi = -m^2 J cos.
+// Parameters: n_max, phi_min, phi_max. Per photon the sum dJ/dA = sum (a f + b . grad f) is taken;
+// with the scaling s = sin(psi), psi = phi_min + (phi_max - phi_min) u, unclamped, dJ/dn_max = s dJ/dA
+// and dJ/dpsi = n_max cos(psi) dJ/dA; a clamped s (|sin psi| >= n_clip/n_max) makes A = +-n_clip,
+// which depends on neither. Within M_EPSILON of the axis the Hessian is taken as zero.
+template <int M> struct FieldAdjBessel {
+    struct Acc { float dA, s, u; };
+    struct Cache { float f; float3 gf; int gap; };
+    static __device__ __forceinline__ void clear(Acc &c) { c.dA = 0.0f; c.s = 0.0f; c.u = 0.0f; }
+    static __device__ __forceinline__ void parts(const FieldParams &F, float3 p, float &f, float3 &gf, float H[6]) {
+#pragma unroll
+        for (int j = 0; j < 6; ++j) H[j] = 0.0f;
+        const float y = p.y, z = p.z;
+        const float r2 = y * y + z * z;
+        const float r = sqrtf(r2);
+        const float rr = fmaxf(r, kEps);
+        float jm, jm1;
+        bessel_pair_table_t<M>(F.btab, F.bint, F.kb * rr, F.k_r * rr, jm, jm1);
+        const float c = r > 0.0f ? z / r : 1.0f, sn = r > 0.0f ? y / r : 0.0f;
+        float cm = 1.0f, sm = 0.0f;
+        if (M == 1) { cm = c; sm = sn; }
+        else if (M == 2) { cm = c * c - sn * sn; sm = 2.0f * c * sn; }
+        const float x = F.k_r * rr, k = F.k_r, m = float(M);
+        const float dj = m / x * jm - jm1;
+        const float ddj = -dj / x - (1.0f - m * m / (x * x)) * jm;
+        f = jm * cm;
+        const float fr = k * dj * cm, fp = -m * jm * sm;
+        // e_r = (sn, c), e_phi = (c, -sn) in (y, z)
+        gf = f3(0.0f, fr * sn + fp / rr * c, fr * c - fp / rr * sn);
+        if (r < kEps) return;
+        const float frr = k * k * ddj * cm, frp = -m * k * dj * sm, fpp = -m * m * jm * cm;
+        const float app = fr / r + fpp / r2, arp = frp / r - fp / r2;
+        // H in (y, z): frr er er^T + app ep ep^T + arp (er ep^T + ep er^T)
+        H[1] = frr * sn * sn + app * c * c + 2.0f * arp * sn * c;                 // yy
+        H[2] = frr * c * c + app * sn * sn - 2.0f * arp * c * sn;                 // zz
+        H[5] = frr * sn * c - app * c * sn + arp * (c * c - sn * sn);             // yz
+    }
+    static __device__ __forceinline__ void eval_h(const FieldParams &F, float3 p, float s, float &n, float3 &g, float H[6],
+                                                  Cache &k) {
+        k.gap = in_gap(F, p);
+        if (k.gap) {
+#pragma unroll
+            for (int j = 0; j < 6; ++j) H[j] = 0.0f;
+            n = F.n_o; g = f3(0.0f, 0.0f, 0.0f); k.f = 0.0f; k.gf = g;
+            return;
+        }
+        parts(F, p, k.f, k.gf, H);
+        const float A = F.amp * s;
+        n = fmaf(A, k.f, F.n_o);
+        g = mul(k.gf, A);
+#pragma unroll
+        for (int j = 0; j < 6; ++j) H[j] *= A;
+    }
+    static __device__ __forceinline__ void eval_h(const FieldParams &F, float3 p, float s, float &n, float3 &g, float H[6]) {
+        Cache k;
+        eval_h(F, p, s, n, g, H, k);
+    }
+    static __device__ __forceinline__ void theta_c(const FieldParams &, float3, float, float a, float3 b, Acc &c,
+                                                   const AdjParams &, const Cache &k) {
+        if (k.gap) return;
+        c.dA += a * k.f + dot3(b, k.gf);
+    }
+    static __device__ __forceinline__ void theta(const FieldParams &F, float3 p, float s, float a, float3 b, Acc &c,
+                                                 const AdjParams &A) {
+        float n, H[6];
+        float3 g;
+        Cache k;
+        eval_h(F, p, s, n, g, H, k);
+        theta_c(F, p, s, a, b, c, A, k);
+    }
+    // the photon's scaling draw (the sixth uniform: five for genRay, scene.cpp:107-137)
+    static __device__ __forceinline__ void begin(Acc &c, Lane &L, const KParams &P, float s) {
+        rng_seek(L, P, 5);
+        c.u = draw(L, P);
+        c.s = s;
+    }
+    static __device__ __forceinline__ void flush(const Acc &c, const FieldParams &F, const AdjParams &A) {
+        float sn, cs;
+        sincos_red(F.phi_min + F.phi_range * c.u, sn, cs);
+        if (!(sn < F.max_scaling && sn > -F.max_scaling)) return;      // clamped: A = +-n_clip
+        atomicAdd(A.grad + 0, double(c.s * c.dA));
+        const float dpsi = F.amp * cs * c.dA;
+        atomicAdd(A.grad + 1, double(dpsi * (1.0f - c.u)));
+        atomicAdd(A.grad + 2, double(dpsi * c.u));
+    }
+};
+template <> struct FieldAdj<FK_BESSEL0> : FieldAdjBessel<0> {};
+template <> struct FieldAdj<FK_BESSEL1> : FieldAdjBessel<1> {};
+template <> struct FieldAdj<FK_BESSEL2> : FieldAdjBessel<2> {};
+
 __device__ __forceinline__ float g_at(const AdjParams &A, int x, int y, int z) {
     if (x < 0 || x >= A.X || y < 0 || y >= A.Y || z < 0 || z >= A.Z) return 0.0f;
     return float(__ldg(A.G + (size_t(z) * A.Y + y) * A.X + x));
@@ -528,14 +634,6 @@ struct AdjReplayHook {
     __device__ void photon_begin(const Lane &) {}
     __device__ void photon_end(const Lane &) {}
 };
-
-// Position the lane's Philox stream at draw index d (draw k uses word k % 4 of block k / 4).
-__device__ __forceinline__ void rng_seek(Lane &L, const KParams &P, int d) {
-    L.rblk = unsigned(d >> 2);
-    L.rhave = 0;
-    L.draws = d & ~3;
-    for (int i = 0; i < (d & 3); ++i) (void)draw(L, P);
-}
 
 __device__ __forceinline__ float4 traj_get(const AdjParams &A, long long base, int i) {
     return A.traj[base + i];
@@ -748,7 +846,7 @@ __global__ void __launch_bounds__(128, 4) adjoint_trace_kernel(const __grid_cons
     Lane L;
     L.end = 0;
     L.idx = 0;
-    L.tab = nullptr;
+    L.tab = P.field.btab;                       // Bessel table (global memory); NULL for other fields
     L.inst = nullptr;
     L.s = 0.0f;
     AdjTraceHook h;
@@ -788,7 +886,7 @@ __global__ void __launch_bounds__(128, 3) adjoint_replay_kernel(const __grid_con
     const FieldParams &F = P.field;
     AdjReplayHook h;
     Lane L;
-    L.tab = nullptr;
+    L.tab = P.field.btab;                       // Bessel table (global memory); NULL for other fields
     L.inst = nullptr;
     L.s = 0.0f;
     long long rsteps = 0;
@@ -931,7 +1029,7 @@ __global__ void __launch_bounds__(128, 3) adjoint_sweep_kernel(const __grid_cons
                                                             const __grid_constant__ AdjParams A, int round) {
     const FieldParams &F = P.field;
     Lane L;                                     // Philox draws of the HG rotation
-    L.tab = nullptr;
+    L.tab = P.field.btab;                       // Bessel table (global memory); NULL for other fields
     L.inst = nullptr;
     long long pts = 0;
     unsigned long long nspl = 0, nskip = 0;
@@ -1006,6 +1104,7 @@ __global__ void __launch_bounds__(128, 3) adjoint_sweep_kernel(const __grid_cons
                 V = A.pool + r.off;
                 segs = A.segs + 2LL * r.off;
                 FieldAdj<FK>::clear(acc);
+                FieldAdj<FK>::begin(acc, L, P, s);
                 lp = f3(0.0f, 0.0f, 0.0f); ld = lp;
                 kv = r.nv - 1;
                 job = kv >= 1 ? JOB_CONN : JOB_DIRECT;

@@ -10,6 +10,9 @@ namespace smp {
 
 AdjRoundFn adjoint_sweep_fn(int fk) {
     switch (fk) {
+        case FK_BESSEL0: return adjoint_sweep_kernel<FK_BESSEL0>;
+        case FK_BESSEL1: return adjoint_sweep_kernel<FK_BESSEL1>;
+        case FK_BESSEL2: return adjoint_sweep_kernel<FK_BESSEL2>;
         case FK_PLANEWAVE: return adjoint_sweep_kernel<FK_PLANEWAVE>;
         case FK_SPLINE: return adjoint_sweep_kernel<FK_SPLINE>;
         default: return nullptr;

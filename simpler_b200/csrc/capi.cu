@@ -1347,12 +1347,19 @@ int64_t smp_adjoint_param_count(const smp_field_desc *f) {
         if (f->grid_n[0] < 2 || f->grid_n[1] < 2 || f->grid_n[2] < 2) return set_error(SMP_ERR_BAD_ARG, "bad spline grid");
         return int64_t(f->grid_n[0]) * f->grid_n[1] * f->grid_n[2];
     }
-    return set_error(SMP_ERR_UNSUPPORTED, "the adjoint is built for plane-wave and spline fields");
+    if (f->type == SMP_FIELD_BESSEL) {
+        if (f->mode < 0 || f->mode > 2) return set_error(SMP_ERR_UNSUPPORTED, "the Bessel adjoint is built for modes 0-2");
+        return 3;
+    }
+    return set_error(SMP_ERR_UNSUPPORTED, "the adjoint is built for Bessel (modes 0-2), plane-wave and spline fields");
 }
 
 typedef void (*AdjFn)(KParams, AdjParams);
 static AdjFn adjoint_trace_fn(int fk) {
     switch (fk) {
+        case FK_BESSEL0: return adjoint_trace_kernel<FK_BESSEL0>;
+        case FK_BESSEL1: return adjoint_trace_kernel<FK_BESSEL1>;
+        case FK_BESSEL2: return adjoint_trace_kernel<FK_BESSEL2>;
         case FK_PLANEWAVE: return adjoint_trace_kernel<FK_PLANEWAVE>;
         case FK_SPLINE: return adjoint_trace_kernel<FK_SPLINE>;
         default: return nullptr;
@@ -1360,6 +1367,9 @@ static AdjFn adjoint_trace_fn(int fk) {
 }
 static AdjRoundFn adjoint_replay_fn(int fk) {
     switch (fk) {
+        case FK_BESSEL0: return adjoint_replay_kernel<FK_BESSEL0>;
+        case FK_BESSEL1: return adjoint_replay_kernel<FK_BESSEL1>;
+        case FK_BESSEL2: return adjoint_replay_kernel<FK_BESSEL2>;
         case FK_PLANEWAVE: return adjoint_replay_kernel<FK_PLANEWAVE>;
         case FK_SPLINE: return adjoint_replay_kernel<FK_SPLINE>;
         default: return nullptr;

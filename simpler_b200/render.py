@@ -177,8 +177,8 @@ def records_to_arrays(recs) -> dict:
 
 # ---- field parameters of the adjoint -------------------------------------------------------------
 def param_count(setup: Setup) -> int:
-    """Length of the parameter vector `adjoint` differentiates (plane waves: amplitudes then
-    phases; spline: the coefficient grid, x fastest)."""
+    """Length of the parameter vector `adjoint` differentiates (Bessel: n_max, phi_min, phi_max;
+    plane waves: amplitudes then phases; spline: the coefficient grid, x fastest)."""
     fd = setup.field_desc()
     n = L.load().smp_adjoint_param_count(C.byref(fd))
     if n < 0:
@@ -192,7 +192,9 @@ def field_params(setup: Setup) -> np.ndarray:
         return np.concatenate([np.asarray(setup.wave_amp, np.float64), np.asarray(setup.wave_phase, np.float64)])
     if setup.field_type == L.FIELD_SPLINE:
         return np.asarray(setup.grid_coeff, np.float64).ravel().copy()
-    raise ValueError("the adjoint is built for plane-wave and spline fields")
+    if setup.field_type == L.FIELD_BESSEL:
+        return np.array([setup.n_max, setup.phi_min, setup.phi_max], dtype=np.float64)
+    raise ValueError("the adjoint is built for Bessel, plane-wave and spline fields")
 
 
 def with_field_params(setup: Setup, theta) -> Setup:
@@ -204,7 +206,9 @@ def with_field_params(setup: Setup, theta) -> Setup:
                                    wave_phase=tuple(float(x) for x in theta[w:2 * w]))
     if setup.field_type == L.FIELD_SPLINE:
         return dataclasses.replace(setup, grid_coeff=theta.reshape(np.shape(setup.grid_coeff)).astype(np.float32))
-    raise ValueError("the adjoint is built for plane-wave and spline fields")
+    if setup.field_type == L.FIELD_BESSEL:
+        return dataclasses.replace(setup, n_max=float(theta[0]), phi_min=float(theta[1]), phi_max=float(theta[2]))
+    raise ValueError("the adjoint is built for Bessel, plane-wave and spline fields")
 
 
 def roi_weights(setup: Setup, size: int = 32) -> np.ndarray:

@@ -104,8 +104,11 @@ def test_param_layout():
     assert sb.param_count(sp) == 8 ** 3
     c = sb.field_params(sp)
     np.testing.assert_array_equal(sb.with_field_params(sp, c).grid_coeff, sp.grid_coeff)
+    assert sb.param_count(sb.config_plain_small()) == 3   # Bessel: n_max, phi_min, phi_max
     with pytest.raises(L.SmpError):
-        sb.param_count(sb.config_plain_small())          # Bessel: no adjoint built
+        sb.param_count(sb.config_plain_small(mode=3))    # orders above 2: no adjoint built
+    with pytest.raises(L.SmpError):
+        sb.param_count(sb.config_sources())
     g = sb.roi_weights(pw, 32)
     assert g.shape == pw.film_shape() and g.sum() == 32 * 32 * pw.path_length_bins
 
@@ -117,7 +120,7 @@ def test_adjoint_stats_layout():
 # ---- GPU -----------------------------------------------------------------------------------------
 @pytest.mark.gpu
 def test_planewave_direct_light_fd():
-    s = sb.config_planewave(albedo=0.0)
+    s = sb.config_planewave(albedo=0.0, precision_mode=L.PREC_MIXED)      # FP64 film (see the Bessel test)
     G = smooth_weights(s)
     n = 200_000
     grad, st = sb.adjoint(s, n, G)
@@ -150,10 +153,52 @@ def test_planewave_scattering_matched_fd():
 
 
 @pytest.mark.gpu
+def test_bessel_direct_light_fd():
+    """Bessel mode 1 at a fixed phase (s = sin 1 for every photon; n_clip = 2 n_max, so no photon is
+    clamped on either side of the step): amplitude, and the phase window moved as a whole. (Mode 0
+    is a poor finite-difference case: its radially symmetric focusing gives photons on opposite
+    sides of the axis contributions of opposite sign that cancel to about 1 % of their size.)"""
+    # FP64 film: direct light lands in a single path-length bin, where FP32 film atomics (thousands
+    # per pixel, in no fixed order) would round away the difference being measured
+    s = sb.config_plain_small(albedo=0.0, mode=1, n_max=2e-3, n_clip=4e-3, phi_min=1.0, phi_max=1.0,
+                              precision_mode=L.PREC_MIXED)
+    G = smooth_weights(s)
+    n = 1_000_000
+    grad, st = sb.adjoint(s, n, G)
+    assert st.replay_mismatch == 0 and st.dropped == 0
+    th = sb.field_params(s)
+    # amplitude (a 5 % step: smaller ones are dominated by the march's FP32 rounding at this signal)
+    tp, tm, dh = stepped(th, 0, 1e-4)
+    fd = float(((sb.render(sb.with_field_params(s, tp), n)[0] - sb.render(sb.with_field_params(s, tm), n)[0]) * G).sum()) / dh
+    assert abs(grad[0] - fd) <= 2e-2 * abs(fd), (grad[0], fd)
+    # the phase window shifted as a whole: d/dphi_min + d/dphi_max
+    tp, tm = th.copy(), th.copy()
+    tp[1:] += 0.05
+    tm[1:] -= 0.05
+    fd = float(((sb.render(sb.with_field_params(s, tp), n)[0] - sb.render(sb.with_field_params(s, tm), n)[0]) * G).sum()) / 0.1
+    assert abs(grad[1] + grad[2] - fd) <= 3e-2 * abs(fd), (grad[1] + grad[2], fd)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [0, 1])
+def test_bessel_scattering_matched_fd(mode):
+    s = sb.config_plain_small(mode=mode, n_max=2e-3, n_clip=4e-3, max_depth=7)
+    G = sb.roi_weights(s, 32)
+    n = 300_000
+    grad, st = sb.adjoint(s, n, G)
+    assert st.replay_mismatch == 0 and st.dropped == 0
+    tp, tm, dh = stepped(sb.field_params(s), 0, 2e-5)
+    fd, frac = matched_fd(s, sb.with_field_params(s, tp), sb.with_field_params(s, tm), n, G)
+    assert frac > 0.99
+    fd /= dh
+    assert abs(grad[0] - fd) <= 3e-2 * abs(fd), (grad[0], fd)
+
+
+@pytest.mark.gpu
 def test_spline_direction_fd():
     """All 262144 coefficients at once: the gradient dotted with a random perturbation."""
     n = 100_000
-    s = sb.config_spline(albedo=0.0)
+    s = sb.config_spline(albedo=0.0, precision_mode=L.PREC_MIXED)
     G = smooth_weights(s)
     grad, st = sb.adjoint(s, n, G)
     assert st.replay_mismatch == 0 and st.dropped == 0
