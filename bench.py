@@ -227,7 +227,9 @@ def run_reference(args):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    per_step = max(threads * 4, 32)
+    # 64 photons per thread: a step waits for its slowest photon, so small steps understate the
+    # CPU's throughput
+    per_step = max(threads * 64, 1024)
     for i in range(args.warmup):
         cpu_trace(per_step, i * per_step, threads)
     times = []
