@@ -17,18 +17,21 @@
 // path), which shifts the arc length (exp(-sigma_t d) of connections; the remaining distance of
 // a move after a reflection).
 //
-// Path replay with checkpointed scatter vertices, one photon per thread:
-//   phase A  trace the photon (run_events + march_step, the render's own code) and record a
-//            checkpoint at the source and at every scatter vertex: position, optical direction,
-//            path length, step count and the Philox draw index (draw k of photon i is a pure
-//            function of (seed, i, k), so any segment can be replayed from its checkpoint);
-//   phase B  walk the vertices backwards. For each segment (connection from vertex k, move from
-//            vertex k-1 to k, the direct march), replay it forward from its checkpoint writing the
-//            accepted ER-step positions to this thread's trajectory buffer, then sweep the buffer
-//            backwards: the adjoint of kick-drift-kick (scene.cpp:323-330)
+// Path replay with checkpointed scatter vertices, in batches of photons, three kernels per batch:
+//   adjoint_trace_kernel   traces every photon with the render's own lane loop (march.cuh) and a
+//            hook that records a checkpoint at the source and at every scatter vertex: position,
+//            optical direction, path length, step count and the Philox draw index (draw k of
+//            photon i is a pure function of (seed, i, k), so any segment can be replayed from its
+//            checkpoint); it marks the splats that reach dJ/dfilm and counts the trajectory
+//            entries of every segment the backward pass will need;
+//   adjoint_replay_kernel  replays those segments forward from their checkpoints, writing each
+//            accepted ER step's position and step size to the trajectory buffer (rounds: photons
+//            that do not fit wait for the next one);
+//   adjoint_sweep_kernel   (adjoint_sweep.cu) walks each photon's vertices backwards and sweeps
+//            every recorded segment with the adjoint of kick-drift-kick (scene.cpp:323-330)
 //              dh = d + h/2 g(p),  p' = p + dh h/n(p),  d' = dh + h/2 g(p')
-//            needs n, grad n and the Hessian of n at every point, and accumulates
-//            dJ/dtheta through dn/dtheta and dgrad n/dtheta at every point.
+//            which needs n, grad n and the Hessian of n at every point, and accumulates dJ/dtheta
+//            through dn/dtheta and dgrad n/dtheta at every point.
 // The splat's value (Fresnel exit, foreshortening, Henyey-Greenstein, exp(-sigma_t d), bilinear
 // weights) and the HG frame rotation at a vertex are differentiated with forward-mode dual numbers.
 #pragma once
@@ -138,7 +141,7 @@ enum AdjCounter : int {
     ADJ_DROPPED = 2,       // photons left out: more vertices than checkpoints, pool or trajectory buffer full
     ADJ_ABORTED = 3,       // photons left out: step cap or non-finite state in the forward trace
     ADJ_MISMATCH = 4,      // replays whose end state differed from the checkpoint (a defect)
-    ADJ_STEPS_FWD = 5,     // (unused: the trace counts its steps in KParams.counters)
+    ADJ_RESERVED = 5,      // (the trace counts its ER steps in KParams.counters)
     ADJ_STEPS_REPLAY = 6,  // er_step evaluations of the replays
     ADJ_POINTS = 7,        // trajectory points swept backwards
     ADJ_SPLATS = 8,        // splats differentiated
