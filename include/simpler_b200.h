@@ -222,7 +222,7 @@ typedef struct smp_photon_record {
     smp_splat_record splats[SMP_TRACE_MAX_SPLATS];
 } smp_photon_record;
 
-/* ---- batched sweep (north-star form 2) ----------------------------------------------------- */
+/* ---- batched sweep: many field / medium configurations in one launch --------------------- */
 typedef struct smp_instance_desc {
     smp_field_desc  field;        /* per-instance field (Bessel / plane wave)                       */
     smp_medium_desc medium;

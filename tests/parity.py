@@ -3,7 +3,7 @@ from __future__ import annotations
 
 import numpy as np
 
-# positions within 1e-4 mm, directions within 1e-5 rad
+# acceptance bounds of the path: positions within 1e-4 mm, directions within 1e-5 rad
 POS_TOL_M = 1e-7
 DIR_TOL_RAD = 1e-5
 PATH_TOL_M = 1e-7

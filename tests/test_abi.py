@@ -60,6 +60,16 @@ def test_bad_arguments_are_rejected_before_any_device_work():
     assert rc in (L.SMP_ERR_UNSUPPORTED, L.SMP_ERR_NO_DEVICE)
     assert lib.smp_texture_cdf(None, 4, 4, None) == L.SMP_ERR_BAD_ARG
     assert lib.smp_spline_prefilter(None, None, None) == L.SMP_ERR_BAD_ARG
+    # the adjoint's entry points check their arguments before touching a device
+    g = np.zeros(4)
+    assert lib.smp_plan_adjoint(None, 0, 10, 10, C.c_void_p(img.ctypes.data), C.c_void_p(g.ctypes.data), None) == L.SMP_ERR_BAD_ARG
+    sc, md, fd, op = s.descs()
+    sc.x_res = 0
+    assert lib.smp_render_adjoint(C.byref(sc), C.byref(md), C.byref(fd), C.byref(op), 10, C.c_void_p(img.ctypes.data),
+                                  C.c_void_p(g.ctypes.data), None) == L.SMP_ERR_BAD_ARG
+    sc, md, fd, op = sb.config_sources().descs()
+    assert lib.smp_adjoint_param_count(C.byref(fd)) == L.SMP_ERR_UNSUPPORTED
+    assert lib.smp_adjoint_param_count(None) == L.SMP_ERR_BAD_ARG
 
 
 def test_sizeof_unknown_is_zero():

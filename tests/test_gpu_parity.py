@@ -2,7 +2,7 @@
 
 Each photon i draws from SFMT-19937 seeded with i (renderer/src/photon.cpp:313); the streams are
 generated by the oracle's SFMT restatement (pinned to the reference engine in test_oracle.py)
-and injected into both implementations. Tolerances (north star): positions 1e-4 mm, directions
+and injected into both implementations. Tolerances (the acceptance bounds of this path): positions 1e-4 mm, directions
 1e-5 rad; splat values 1e-4 relative. Photons whose discrete events differ (a Fresnel coin flip
 or a refinement decision within an FP32 rounding of its threshold) are counted, not hidden.
 """
