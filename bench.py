@@ -425,11 +425,14 @@ def run_sweep(args):
 
 
 def run_adjoint(args):
-    """Gradients of the central 32x32 px ROI throughput per second. Each step differentiates its own
+    """Gradients of the central 32x32 px ROI throughput per second, on one GPU (under torchrun only
+    rank 0 runs it). Each step differentiates its own
     photon range (photons [i N, (i+1) N)); device time from CUDA events around the adjoint launch.
     Beside it: the forward render of the same photons, and central finite differences, which cost
     two forward renders per parameter."""
     import torch
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
     torch.cuda.set_device(0)
     make, n, desc = ADJOINT[args.workload]
     setup = make(0)
@@ -441,7 +444,7 @@ def run_adjoint(args):
     clocks = ClockSampler(0)
     clocks.start()
     ms, tot = [], {k: 0 for k in ("er_steps_forward", "er_steps_replay", "points", "splats", "dropped", "skipped",
-                                  "replay_mismatch", "photons", "trace_ms")}
+                                  "replay_mismatch", "photons", "trace_ms", "launches")}
     for i in range(args.steps):
         _, st = plan.adjoint(G, (args.warmup + i) * n, n, n)
         ms.append(st.kernel_ms)
@@ -486,7 +489,7 @@ def run_adjoint(args):
         "e2e": {"value": 1.0 / e2e_s, "unit": "gradients/s", "h2d_bytes_per_step": G.nbytes + 4096,
                 "d2h_bytes_per_step": npar * 8 + 80, "call": "smp_render_adjoint (one-shot plan, host dJ/dfilm "
                                                             "and gradient), wall clock"},
-        "gpu_launches": args.steps, "clocks": clk,
+        "gpu_launches": int(tot["launches"]), "clocks": clk,
     }
     print(json.dumps(out), flush=True)
 

@@ -1464,6 +1464,7 @@ int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, in
     for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&ev[i]);
     unsigned long long c[ADJ_COUNT] = {0};
     unsigned long long fwd_steps = 0;
+    long long launches = 0;
     float ms = 0.0f;
     double trace_ms = 0.0;
     if (e != cudaSuccess) {
@@ -1483,14 +1484,14 @@ int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, in
             k.n_photons = std::min<long long>(batch, n_photons - done);
             e = cudaMemsetAsync(d_kcnt, 0, (CNT_COUNT + 1) * sizeof(unsigned long long), 0);
             cudaEventRecord(ev[2], 0);
-            if (e == cudaSuccess) fa<<<grid_a, kBlock>>>(k, a);
+            if (e == cudaSuccess) { fa<<<grid_a, kBlock>>>(k, a); ++launches; }
             cudaEventRecord(ev[3], 0);
             for (int round = 1; e == cudaSuccess; ++round) {
                 e = cudaMemsetAsync(a.traj_next, 0, 2 * sizeof(unsigned long long), 0);
                 if (e == cudaSuccess) e = cudaMemsetAsync(d_cnt + ADJ_NEXT, 0, sizeof(unsigned long long), 0);
-                if (e == cudaSuccess) fr<<<grid_r, kBlock>>>(k, a, round);
+                if (e == cudaSuccess) { fr<<<grid_r, kBlock>>>(k, a, round); ++launches; }
                 if (e == cudaSuccess) e = cudaMemsetAsync(d_cnt + ADJ_NEXT, 0, sizeof(unsigned long long), 0);
-                if (e == cudaSuccess) fs<<<grid_s, kBlock>>>(k, a, round);
+                if (e == cudaSuccess) { fs<<<grid_s, kBlock>>>(k, a, round); ++launches; }
                 if (e == cudaSuccess) e = cudaGetLastError();
                 int pending = 0;
                 if (e == cudaSuccess) e = cudaMemcpy(&pending, a.pending, sizeof(int), cudaMemcpyDeviceToHost);
@@ -1524,6 +1525,7 @@ int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, in
         stats_out->splats = (int64_t)c[ADJ_SPLATS];
         stats_out->kernel_ms = ms;
         stats_out->trace_ms = trace_ms;
+        stats_out->launches = launches;
     }
     for (int i = 0; i < 4; ++i) if (ev[i]) cudaEventDestroy(ev[i]);
     if (!rc && c[ADJ_MISMATCH])

@@ -114,7 +114,7 @@ def test_param_layout():
 
 
 def test_adjoint_stats_layout():
-    assert sb.check_layout()["smp_adjoint_stats"][0] == 88
+    assert sb.check_layout()["smp_adjoint_stats"][0] == 96
 
 
 # ---- GPU -----------------------------------------------------------------------------------------
