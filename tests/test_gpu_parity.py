@@ -123,6 +123,21 @@ def test_plan_render_film_matches_oracle_same_streams():
     assert abs(img.sum() / rimg.sum() - 1.0) < 1e-3
 
 
+@pytest.mark.gpu
+def test_fp32_march_image_against_fp64_oracle():
+    """The precision form (FP32 march, FP64 path length and film) against the FP64 restatement on
+    the same Philox photons: relative image RMSE within 1 %."""
+    s = sb.config_plain_small(rng=L.RNG_PHILOX, seed=5, spatial_x=32, spatial_y=32, path_length_bins=8,
+                              precision_mode=L.PREC_MIXED)
+    n = 20_000
+    img, st = sb.render(s, n)
+    assert st.photons == n
+    _, ref = ob.oracle_trace(s, 0, n, n, records=False, real_bits=64)
+    rmse = np.sqrt(((img - ref) ** 2).sum() / (ref ** 2).sum())
+    print(f"relative image RMSE against the FP64 oracle: {rmse:.3e}")
+    assert rmse < 1e-2, rmse
+
+
 def test_field_probe_matches_oracle():
     rng = np.random.default_rng(0)
     pts = rng.uniform(-0.005, 0.005, size=(4000, 3))
