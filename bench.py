@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--photons-per-step", type=int, default=PHOTONS_PER_STEP)
     ap.add_argument("--workload", choices=["precision", "sweep", "plain", "planewave", "spline", "sources", "adjoint",
-                                           "adjoint-spline"], default="precision",
+                                           "adjoint-spline", "adjoint-bessel"], default="precision",
                     help="precision: the headline line (default); sweep: the batched 256-instance sweep "
                          "against the same instances rendered one by one; adjoint / adjoint-spline: gradients "
                          "of the central 32x32 px ROI throughput")
@@ -81,6 +81,10 @@ ADJOINT = {
                 "traveling-wave adjoint: two plane waves a = 1e-3 at 1 MHz along +y and +z, phases U[0, 2 pi) "
                 "(seed 3), sigma_s 0.5/mm, albedo 0.9, g 0.9, 128x128 x 32 bins, fp32, 1e7 photons; gradient "
                 "of the central 32x32 px ROI throughput w.r.t. (a_i, phase_i)"),
+    "adjoint-bessel": (lambda d: sb.config_plain_small(device=d, n_clip=2e-3), 1_000_000,
+                       "transducer adjoint: Bessel mode 0, n_max 1e-3 (n_clip 2e-3: no scaling clamped) at 848 kHz, "
+                       "sigma_s 0.1/mm, albedo 0.9, g 0.9, 128x128 x 32 bins, fp32, 1e6 photons; gradient of the "
+                       "central 32x32 px ROI throughput w.r.t. (n_max, phi_min, phi_max)"),
     "adjoint-spline": (lambda d: sb.config_spline(device=d), 1_000_000,
                        "spline adjoint: 64^3 tricubic coefficients over the 10 mm cube (Gaussian-filtered noise, "
                        "max dn 1e-3, seed 4), sigma_s 1/mm, albedo 0.95, g 0.8, 256x256 x 64 bins, fp32; "
@@ -479,7 +483,9 @@ def run_adjoint(args):
         "forward_ms": fwd_ms, "cost_vs_forward": adj_ms / fwd_ms,
         "finite_differences": {"renders": 2 * npar, "ms": 2 * npar * fwd_ms,
                                "speedup_of_adjoint": 2 * npar * fwd_ms / adj_ms},
-        "roofline": {"bound": "fp32", "kernel": f"adjoint_kernel<{'FK_PLANEWAVE' if npar < 100 else 'FK_SPLINE'}>",
+        "roofline": {"bound": "fp32", "kernel": "adjoint_{trace,replay,sweep}_kernel<"
+                     + {L.FIELD_PLANEWAVE: "FK_PLANEWAVE", L.FIELD_SPLINE: "FK_SPLINE"}.get(
+                         setup.field_type, f"FK_BESSEL{setup.mode}") + ">",
                      "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s", "frac": achieved / peak.value,
                      "traffic": None,
                      "flop_model": "er_steps (checkpointing trace + replays) x flop_per_step + swept points x "

@@ -30,6 +30,10 @@ Hessian there, the parameter vector-Jacobian product, and the step's own adjoint
                        (21) + ten accumulations (20) + products (3)) (704), scaling (15)        = 791
                        parameter product: weights (72) + 16 rows x (row factors (10) + 4 taps
                        (12)) (352)                                                              = 424
+  Bessel m <= 2        r, 1/r (3) + J_m, J_m+1 (2) + cos, sin of m phi (4) + J', J'' (9) + f and
+                       the polar derivatives (9) + grad f (8) + Hessian in y, z (21) + scaling
+                       by A (8)                                                                  = 64
+                       parameter product a f + b . grad f (6)                                    = 6
 """
 
 FLOP_LEAPFROG = 24
@@ -80,4 +84,6 @@ def flop_per_point_adjoint(setup) -> int:
         return FLOP_ADJ_STEP + (31 + 21) * len(setup.wave_amp)
     if setup.field_type == L.FIELD_SPLINE:
         return FLOP_ADJ_STEP + 791 + 424
-    raise ValueError("the adjoint is built for plane-wave and spline fields")
+    if setup.field_type == L.FIELD_BESSEL:
+        return FLOP_ADJ_STEP + 64 + 6
+    raise ValueError("the adjoint is built for Bessel, plane-wave and spline fields")
