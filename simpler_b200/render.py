@@ -220,6 +220,24 @@ def roi_weights(setup: Setup, size: int = 32) -> np.ndarray:
     return g
 
 
+def adjoint_sharded(plan, dJ_dfilm: np.ndarray, n_photons: int, rank: int = 0, world: int = 1,
+                    all_reduce=None) -> np.ndarray:
+    """The gradient of the n_photons render over `world` processes (one GPU each): this rank
+    differentiates its contiguous photon range -- photon k draws Philox stream (seed, k) on any
+    rank, so the ranges add up to the single-process gradient -- and `all_reduce` (a callable that
+    sums a float64 array over the ranks in place and returns it, e.g. over torch.distributed)
+    combines them. `plan` is this rank's Plan (anything with Plan.adjoint's signature)."""
+    per = -(-int(n_photons) // int(world))
+    first = int(rank) * per
+    n = max(0, min(per, int(n_photons) - first))
+    if n > 0:
+        grad, _ = plan.adjoint(dJ_dfilm, first, n, int(n_photons))
+        grad = np.asarray(grad, dtype=np.float64)
+    else:
+        grad = np.zeros(param_count(plan.setup), dtype=np.float64)
+    return all_reduce(grad) if all_reduce is not None else grad
+
+
 def adjoint(setup: Setup, n_photons: int, dJ_dfilm: np.ndarray) -> tuple[np.ndarray, L.AdjointStats]:
     """One-shot gradient of sum(dJ_dfilm * film) for the n_photons render of `setup`."""
     lib = L.load()

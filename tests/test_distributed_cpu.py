@@ -44,3 +44,45 @@ def test_two_rank_photon_sharding_matches_single_process(tmp_path):
     sharded = np.load(out)
     _, single = ob.oracle_trace(_setup(), 0, N, N, records=False, threads=2)
     assert np.allclose(sharded, single, rtol=1e-12, atol=1e-15)
+
+
+class _AdditivePlan:
+    """Stands in for a Plan: its 'gradient' of photons [first, first + n) is additive over photon
+    ranges, as Plan.adjoint's is (tests/test_adjoint.py checks that on the GPU)."""
+    setup = sb.config_planewave()
+
+    def adjoint(self, G, first, n, weight):
+        k = np.arange(first, first + n, dtype=np.float64)
+        return np.array([k.sum(), (k * k).sum(), np.sin(k).sum(), float(n)]) / weight, None
+
+
+def _adjoint_rank(rank, world, port, out, n_photons):
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+
+    def all_reduce(a):
+        t = torch.from_numpy(a)
+        dist.all_reduce(t)
+        return t.numpy()
+
+    g = sb.adjoint_sharded(_AdditivePlan(), None, n_photons, rank, world, all_reduce)
+    if rank == 0:
+        np.save(out, g)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_adjoint_sharding_matches_single_process(tmp_path):
+    n_photons = 1001                      # not a multiple of the world size
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    out = str(tmp_path / "grad.npy")
+    mp.spawn(_adjoint_rank, args=(2, port, out, n_photons), nprocs=2, join=True)
+    sharded = np.load(out)
+    single = sb.adjoint_sharded(_AdditivePlan(), None, n_photons)
+    assert np.allclose(sharded, single, rtol=1e-12)
+    assert single[3] * n_photons == n_photons          # every photon exactly once
