@@ -88,6 +88,21 @@ def oracle_trace(setup, first: int, n: int, weight_photons: int, uniforms=None, 
     return (records_to_arrays(recs) if recs is not None else None), img
 
 
+def oracle_fd_gradient(setup, index: int, h: float, n: int, G: np.ndarray, threads: int = 0) -> float:
+    """FP64 reference gradient: the central difference of sum(G * film) in field parameter `index`
+    (simpler_b200.field_params order) with the FP64 restatement on common random numbers (the same
+    Philox photons 0..n-1 on both sides). Parameters enter the FP64 arithmetic unrounded, so the
+    step is exactly 2h."""
+    import simpler_b200 as sb
+    th = sb.field_params(setup)
+    tp, tm = th.copy(), th.copy()
+    tp[index] += h
+    tm[index] -= h
+    _, ip = oracle_trace(sb.with_field_params(setup, tp), 0, n, n, records=False, real_bits=64, threads=threads)
+    _, im = oracle_trace(sb.with_field_params(setup, tm), 0, n, n, records=False, real_bits=64, threads=threads)
+    return float(((ip - im) * G).sum()) / (2.0 * h)
+
+
 def oracle_field(setup, scaling: float, points: np.ndarray, real_bits: int = 64):
     return oracle_field_desc(setup.field_desc(), scaling, points, real_bits)
 

@@ -113,6 +113,18 @@ def test_param_layout():
     assert g.shape == pw.film_shape() and g.sum() == 32 * 32 * pw.path_length_bins
 
 
+def test_fp64_reference_gradient_is_stable():
+    """The FP64 reference gradient (central differences of the FP64 restatement on the same photons)
+    does not depend on its step: direct light, plane-wave amplitude and phase."""
+    import oracle_bridge as ob
+    s = sb.config_planewave(albedo=0.0, precision_mode=L.PREC_MIXED, spatial_x=64, spatial_y=64, path_length_bins=8)
+    G = smooth_weights(s)
+    a1, a2 = (ob.oracle_fd_gradient(s, 0, h, 400, G) for h in (1e-6, 2e-6))
+    assert abs(a1 - a2) <= 1e-4 * abs(a1), (a1, a2)
+    p1, p2 = (ob.oracle_fd_gradient(s, 2, h, 400, G) for h in (2e-4, 4e-4))
+    assert abs(p1 - p2) <= 1e-2 * abs(p1), (p1, p2)
+
+
 def test_adjoint_stats_layout():
     assert sb.check_layout()["smp_adjoint_stats"][0] == 96
 
