@@ -183,8 +183,8 @@ class ClockSampler:
 
 
 # ---- CPU baseline: the oracle port on the host cores ----------------------------------------------
-def _oracle_lib():
-    lib = C.CDLL(os.path.join(ROOT, "oracle", "liboracle_fast.so"))
+def _oracle_lib(fast: bool = True):
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "liboracle_fast.so" if fast else "liboracle.so"))
     P = C.POINTER
     vp = C.c_void_p
     lib.orc_render.argtypes = [P(L.SceneDesc), P(L.MediumDesc), P(L.FieldDesc), P(L.RenderOpts), C.c_int, C.c_int,
@@ -223,6 +223,58 @@ def cpu_baseline(target_s: float = 12.0) -> dict:
             "sample": f"photons 0..{done} of the same workload ({done} photon paths) in {dt:.1f} s on all "
                       f"{threads} host threads, CPU restatement built with the reference's -O3 -ffast-math "
                       f"flags, film accumulation skipped"}
+
+
+def image_check(setup: sb.Setup, n: int, threads: int = 8) -> dict:
+    """The cpu_baseline leg's check of the image error (the oracle as the checker): photons 0..n-1 of
+    the workload on the same Philox streams, rendered by this library's default path (FP32 march,
+    the workload's precision form) and by the plain kernel in the reference GPU's FP32 form (FP32
+    path length and float film), each against the FP64 restatement on the CPU; beside them the FP32
+    restatement on the CPU against the same FP64 one, the error that FP32 marching itself makes.
+    Relative RMSE sqrt(sum (film - ref)^2 / sum ref^2) at the workload's film and with bins merged
+    4x4x4 and 16x16x16; and the fraction of photons whose discrete events (end, draws, depth, splat
+    count) are the same in the FP32 GPU march and the FP64 oracle."""
+    import dataclasses
+    lib = _oracle_lib(fast=False)
+    ours, _ = sb.render(setup, n)
+    plain_setup = dataclasses.replace(setup, kernel=L.KERNEL_PLAIN, precision_mode=L.PREC_FP32)
+    plain, _ = sb.render(plain_setup, n)
+    recs, _ = sb.trace_photons(setup, 0, n, n, with_image=False)
+    recs = sb.records_to_arrays(recs)
+    sc, md, fd, op = setup.descs()
+
+    def oracle(bits):
+        img = np.zeros(setup.film_shape(), dtype=np.float64)
+        rr = (L.PhotonRecord * n)()
+        t0 = time.perf_counter()
+        rc = lib.orc_render(C.byref(sc), C.byref(md), C.byref(fd), C.byref(op), bits, threads, 0, n, n, None, None,
+                            C.cast(rr, C.c_void_p), C.c_void_p(img.ctypes.data))
+        assert rc == 0
+        return img, sb.records_to_arrays(rr), time.perf_counter() - t0
+
+    ref, orecs, dt = oracle(64)
+    cpu32, _, _ = oracle(32)
+    same = ((recs["end"] == orecs["end"]) & (recs["draws"] == orecs["draws"]) & (recs["depth"] == orecs["depth"])
+            & (recs["n_splats"] == orecs["n_splats"]))
+
+    def binned(a, f):
+        z, y, x = a.shape
+        fz, fy, fx = min(f, z), min(f, y), min(f, x)
+        return a.reshape(z // fz, fz, y // fy, fy, x // fx, fx).sum(axis=(1, 3, 5))
+
+    def rmse(a, f):
+        a, b = binned(a, f), binned(ref, f)
+        return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+
+    out = {"photons": n, "film": [setup.spatial_x, setup.spatial_y, setup.path_length_bins],
+           "same_events_fraction": float(same.mean()),
+           "reference": f"FP64 CPU restatement (oracle/liboracle.so, {threads} threads, {dt:.1f} s), same Philox photons"}
+    for f in (1, 4, 16):
+        key = "" if f == 1 else f"_binned_{f}x{f}x{f}"
+        out["ours" + key] = rmse(ours, f)
+        out["plain_fp32" + key] = rmse(plain, f)
+        out["cpu_fp32_restatement" + key] = rmse(cpu32, f)
+    return out
 
 
 # ---- reference arm ---------------------------------------------------------------------------------
@@ -343,11 +395,49 @@ def run_ours(args):
             "er_steps_per_s": steps_timed * world / (ms / 1e3),
         }
     plan.close()
+    if rank == 0:
+        # the plain GPU kernel (one thread per photon, FP32 form) on the same workload and step size
+        plain = run_plain(args, setup, per_step, local, first_step=args.warmup + args.steps)
+        out["plain"] = plain
+        out["speedup_vs_plain"] = value / world / plain["value"]
+        if world == 1 and args.workload in ("precision", "plain"):
+            out["image_rmse_vs_fp64"] = image_check(setup, 20_000 if args.workload == "precision" else 100_000)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if out is not None:
         print(json.dumps(out), flush=True)
+
+
+def run_plain(args, setup, per_step: int, device: int, first_step: int, steps: int = 2) -> dict:
+    """The plain kernel (the reference GPU renderer's structure: one thread per photon, one launch,
+    no regeneration, float atomics; this library's per-photon arithmetic) in the reference GPU's FP32
+    form on the same workload, device-timed over `steps` steps of per_step photons after one
+    warm-up step."""
+    import dataclasses
+    import torch
+    ps = dataclasses.replace(setup, kernel=L.KERNEL_PLAIN, precision_mode=L.PREC_FP32)
+    plan = sb.Plan(ps)
+    stream = torch.cuda.current_stream()
+    h = stream.cuda_stream
+    plan.clear(h)
+    plan.trace(first_step * per_step, per_step, render_photons(args), stream=h)
+    torch.cuda.synchronize()
+    st0 = plan.stats()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(steps):
+        plan.trace((first_step + 1 + i) * per_step, per_step, render_photons(args), stream=h)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    st = plan.stats()
+    plan.close()
+    return {"value": per_step * steps / (ms / 1e3), "unit": METRIC, "ms_per_step": ms / steps, "steps": steps,
+            "kernel": "plain_kernel: one thread per photon, one launch per step (cuda_renderer.cu:681-725 structure)",
+            "precision": "fp32 march, fp32 path length, fp32 film atomics",
+            "er_steps_per_s": (st.er_steps - st0.er_steps) / (ms / 1e3)}
 
 
 def _profile_traffic():
@@ -410,6 +500,14 @@ def run_sweep(args):
         img, _ = sb.render(dataclasses.replace(setup, **over), inst["n_photons"])
         serial_sum += float(img.sum())
     t_serial = time.perf_counter() - t0
+    # the plain kernel (one thread per photon, FP32) over every 8th instance, one render each
+    t0 = time.perf_counter()
+    plain_photons = 0
+    for i, inst in enumerate(insts[::8]):
+        over = {k: v for k, v in inst.items() if k != "n_photons"}
+        sb.render(dataclasses.replace(setup, kernel=L.KERNEL_PLAIN, **over), inst["n_photons"])
+        plain_photons += inst["n_photons"]
+    t_plain = time.perf_counter() - t0
     clk = clocks.stop()
     out = {
         "metric": METRIC, "value": total / t_batch, "unit": METRIC, "n_gpus": 1, "steps": 1, "warmup": 1,
@@ -422,6 +520,10 @@ def run_sweep(args):
         "serial": {"value": total / t_serial, "unit": METRIC, "seconds": t_serial,
                    "call": "one smp_render per instance, host film"},
         "batch_seconds": t_batch, "speedup_vs_serial": t_serial / t_batch,
+        "plain": {"value": plain_photons / t_plain, "unit": METRIC, "seconds": t_plain, "photons": plain_photons,
+                  "call": "one smp_render per instance with the plain kernel (one thread per photon, fp32), every "
+                          "8th instance (32 of 256)"},
+        "speedup_vs_plain": (total / t_batch) / (plain_photons / t_plain),
         "film_sum_relative_difference": abs(float(films.sum()) - serial_sum) / max(serial_sum, 1e-300),
         "er_steps_per_s": st.er_steps / t_batch, "gpu_launches": st.launches, "clocks": clk,
     }

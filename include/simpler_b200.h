@@ -76,7 +76,8 @@ typedef struct smp_field_desc {
     double  rr_weight;            /* carried; unused on the path                                    */
     int32_t use_initialization_hack; /* carried; unused on the path                                 */
     /* Bessel (rif_analytical.h:168-175) */
-    int32_t mode;                 /* Bessel order m >= 0                                            */
+    int32_t mode;                 /* Bessel order 0 <= m <= 64 (orders above 2 need k r <= 128 over
+                                     the medium box)                                                */
     double  n_max, n_clip, phi_min, phi_max;
     /* FUS point sources (rif_sources.h:18-45) */
     int32_t n_coeff;              /* triangle-wave harmonics                                        */
@@ -172,7 +173,20 @@ typedef struct smp_render_opts {
        march's contribution weight*exp(-sigma_t*d) is exactly 0 in FP32, so a photon trapped by
        total internal reflection stops there instead of marching 1e4 m. */
     double   sensor_march_max;
+    int32_t  kernel;              /* smp_kernel: which kernel traces the photons (0 = the default)   */
+    int32_t  _pad0;
 } smp_render_opts;
+
+/* Kernels that trace a plan's photons. All three run the same per-photon arithmetic, so their
+   photons are identical; they differ in scheduling. */
+typedef enum smp_kernel {
+    SMP_KERNEL_POOL       = 0,    /* the default: march and event kernels alternating over a
+                                     resident pool of photon slots, with a persistent tail kernel  */
+    SMP_KERNEL_PERSISTENT = 1,    /* one persistent launch; each lane runs its photons to the end
+                                     and takes the next index from a global counter                */
+    SMP_KERNEL_PLAIN      = 2     /* one thread per photon in one launch, no regeneration: the
+                                     reference GPU renderer's structure (cuda_renderer.cu:681-725) */
+} smp_kernel;
 
 typedef struct smp_stats {
     int64_t photons;              /* photons traced                                                 */
@@ -310,9 +324,12 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
    loading this library holds until the process exits. Limits: texture CDF + Bessel table within the 1 MiB (a 501x501 texture fits);
    Bessel fields of order 0-2 and plane-wave fields; larger inputs are rejected with
    SMP_ERR_BAD_ARG / SMP_ERR_UNSUPPORTED. All calls on a device share that array and each call
-   overwrites what the last one left there; calls whose GPU work overlaps race on it. The first
-   call on each device looks up the array's device address, so make it before any stream capture.
-   stats_out (may be NULL) receives photon, step and splat counts; kernel_ms is not measured. */
+   overwrites what the last one left there. Calls whose GPU work overlapped would race on it, so
+   each call holds a process-wide lock until its own GPU work has finished: calls from several
+   threads or streams run one after another. The first call on each device looks up the array's
+   device address, so make it before any stream capture. The caller's current device is restored
+   on return. stats_out (may be NULL) receives photon, step and splat counts; kernel_ms is not
+   measured. */
 int smp_render_noalloc(const smp_scene_desc *scene, const smp_medium_desc *medium,
                        const smp_field_desc *field, const smp_render_opts *opts,
                        int64_t first_photon, int64_t n_photons, int64_t weight_photons,

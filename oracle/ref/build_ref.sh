@@ -3,9 +3,10 @@
 # smooth dielectric BSDF, thin lens) from their sources in place under the reference checkout,
 # together with ref_shim.cpp, into oracle/_ref/libref_prims.so. Test infrastructure only: the
 # library pins the oracle's restatements. Flags follow the reference's own optimised build
-# (CMakeLists.txt:110-116). Usage: build_ref.sh [reference-root]
+# (CMakeLists.txt:110-116). Usage: build_ref.sh [reference-root]; without the argument the checkout
+# is $SIMPLER_REFERENCE_ROOT, else /root/reference.
 set -e
-REF=${1:-/root/reference}
+REF=${1:-${SIMPLER_REFERENCE_ROOT:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/../_ref"
 mkdir -p "$OUT"

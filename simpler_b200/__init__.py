@@ -6,7 +6,7 @@ if it is missing: there is no CPU fallback.
 """
 from . import _lib
 from ._lib import SmpError, check_layout, load
-from .render import (Plan, adjoint, adjoint_sharded, field_eval, field_params, param_count, records_to_arrays, render, render_batch,
+from .render import (Plan, adjoint, adjoint_sharded, field_eval, render_sharded, shard_range, field_params, param_count, records_to_arrays, render, render_batch,
                      roi_weights, sources_to_spline, trace_photons, with_field_params)
 from .scene import (Setup, bernoulli_texture, config_batch_sweep, config_planewave, config_plain_small, config_sources, config_spline,
                     config_precision, disk_texture)
@@ -14,6 +14,6 @@ from .scene import (Setup, bernoulli_texture, config_batch_sweep, config_planewa
 __all__ = [
     "SmpError", "check_layout", "load", "Plan", "field_eval", "records_to_arrays", "render", "render_batch",
     "trace_photons", "config_batch_sweep", "config_spline", "config_sources", "adjoint", "field_params", "param_count",
-    "roi_weights", "with_field_params", "sources_to_spline", "adjoint_sharded",
+    "roi_weights", "with_field_params", "sources_to_spline", "adjoint_sharded", "render_sharded", "shard_range",
     "Setup", "bernoulli_texture", "config_planewave", "config_plain_small", "config_precision", "disk_texture",
 ]

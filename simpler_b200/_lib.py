@@ -28,6 +28,7 @@ SMP_ERR_UNSUPPORTED = -8
 FIELD_BESSEL, FIELD_SOURCES, FIELD_PLANEWAVE, FIELD_SPLINE = 0, 1, 2, 3
 RNG_SFMT, RNG_PHILOX, RNG_STREAM = 0, 1, 2
 PREC_FP32, PREC_MIXED = 0, 1
+KERNEL_POOL, KERNEL_PERSISTENT, KERNEL_PLAIN = 0, 1, 2
 
 END_NAMES = {1: "GENRAY_FAIL", 2: "NO_SCATTER", 3: "ESCAPED", 4: "ABSORBED", 5: "MAX_DEPTH",
              6: "STEP_CAP", 7: "NAN", 8: "STREAM"}
@@ -101,6 +102,7 @@ class RenderOpts(C.Structure):
         ("step_cap", C.c_int64),
         ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32),
         ("sensor_march_max", C.c_double),
+        ("kernel", C.c_int32), ("_pad0", C.c_int32),
     ]
 
 

@@ -3,8 +3,8 @@
 // The reference's GPU seam, cuda::CudaRenderer::renderImage (renderer/src/cuda_renderer.cu:710-742),
 // deep-copies the scene with ~30 small cudaMalloc/cudaMemcpy calls per render, runs one thread per
 // photon, and copies a float film back. Here a plan uploads the scene once (texture CDF, source
-// table, spline coefficients, film) and each render is one persistent launch over all SMs on the
-// caller's stream, so renders can be batched and captured in CUDA graphs.
+// table, spline coefficients, film) and each render runs asynchronously on the caller's stream (the
+// slot-pool march of wavefront.cuh by default), so renders of one plan can be queued back to back.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -20,6 +20,7 @@
 #include "kparams.h"
 #include "march.cuh"
 #include "wavefront.cuh"
+#include "plain.cuh"
 #include "adjoint.cuh"
 
 using namespace smp;
@@ -158,6 +159,9 @@ static float spline_offsets(const smp_field_desc &f, std::vector<float> &delta) 
 //   p(f) = J_0 + h J_0' f + (3 (J_1 - J_0) - h (2 J_0' + J_1')) f^2 + (2 (J_0 - J_1) + h (J_0' + J_1')) f^3
 static const double kBesselH = 1.0 / 16.0;
 static const double kBesselMaxX = 128.0;
+// Orders above 2 read J_m and J_m+1 from the table alone (no closed form beyond it), so their plans
+// need the box's largest k r within kBesselMaxX; cos(m phi) takes m - 1 complex products.
+static const int kBesselMaxOrder = 64;
 static int bessel_intervals(double x_max) {
     x_max = std::min(std::max(x_max, 1.0), kBesselMaxX);
     return int(std::ceil(x_max / kBesselH)) + 1;
@@ -206,9 +210,9 @@ static float fresnel_host(float cosI, float cosT, float eta) {
 static int field_kind(const smp_field_desc &f, int *fk) {
     switch (f.type) {
         case SMP_FIELD_BESSEL:
-            if (f.mode < 0 || f.mode > 2)
-                return set_error(SMP_ERR_UNSUPPORTED, "Bessel mode %d: orders 0..2 are built", f.mode);
-            *fk = FK_BESSEL0 + f.mode;
+            if (f.mode < 0 || f.mode > kBesselMaxOrder)
+                return set_error(SMP_ERR_UNSUPPORTED, "Bessel mode %d: orders 0..%d are built", f.mode, kBesselMaxOrder);
+            *fk = f.mode <= 2 ? FK_BESSEL0 + f.mode : FK_BESSELN;
             return SMP_OK;
         case SMP_FIELD_PLANEWAVE:
             if (f.n_waves < 0 || f.n_waves > SMP_MAX_WAVES) return set_error(SMP_ERR_BAD_ARG, "n_waves out of range");
@@ -342,6 +346,7 @@ static MarchFn march_fn(int fk) {
         case FK_BESSEL0: return march_kernel<FK_BESSEL0>;
         case FK_BESSEL1: return march_kernel<FK_BESSEL1>;
         case FK_BESSEL2: return march_kernel<FK_BESSEL2>;
+        case FK_BESSELN: return march_kernel<FK_BESSELN>;
         case FK_PLANEWAVE: return march_kernel<FK_PLANEWAVE>;
         case FK_SOURCES: return march_kernel<FK_SOURCES>;
         case FK_SPLINE: return march_kernel<FK_SPLINE>;
@@ -358,6 +363,7 @@ static WaveFn wf_march_fn(int fk, bool fp64) {
         case FK_BESSEL0: return fp64 ? wf_march_kernel<FK_BESSEL0, 1> : wf_march_kernel<FK_BESSEL0, 0>;
         case FK_BESSEL1: return fp64 ? wf_march_kernel<FK_BESSEL1, 1> : wf_march_kernel<FK_BESSEL1, 0>;
         case FK_BESSEL2: return fp64 ? wf_march_kernel<FK_BESSEL2, 1> : wf_march_kernel<FK_BESSEL2, 0>;
+        case FK_BESSELN: return fp64 ? wf_march_kernel<FK_BESSELN, 1> : wf_march_kernel<FK_BESSELN, 0>;
         case FK_PLANEWAVE: return fp64 ? wf_march_kernel<FK_PLANEWAVE, 1> : wf_march_kernel<FK_PLANEWAVE, 0>;
         case FK_SOURCES: return fp64 ? wf_march_kernel<FK_SOURCES, 1> : wf_march_kernel<FK_SOURCES, 0>;
         case FK_SPLINE: return fp64 ? wf_march_kernel<FK_SPLINE, 1> : wf_march_kernel<FK_SPLINE, 0>;
@@ -370,6 +376,7 @@ static WaveFn wf_finish_fn(int fk) {
         case FK_BESSEL0: return wf_finish_kernel<FK_BESSEL0>;
         case FK_BESSEL1: return wf_finish_kernel<FK_BESSEL1>;
         case FK_BESSEL2: return wf_finish_kernel<FK_BESSEL2>;
+        case FK_BESSELN: return wf_finish_kernel<FK_BESSELN>;
         case FK_PLANEWAVE: return wf_finish_kernel<FK_PLANEWAVE>;
         case FK_SOURCES: return wf_finish_kernel<FK_SOURCES>;
         case FK_SPLINE: return wf_finish_kernel<FK_SPLINE>;
@@ -382,6 +389,7 @@ static WaveFn wf_event_fn(int fk) {
         case FK_BESSEL0: return wf_event_kernel<FK_BESSEL0>;
         case FK_BESSEL1: return wf_event_kernel<FK_BESSEL1>;
         case FK_BESSEL2: return wf_event_kernel<FK_BESSEL2>;
+        case FK_BESSELN: return wf_event_kernel<FK_BESSELN>;
         case FK_PLANEWAVE: return wf_event_kernel<FK_PLANEWAVE>;
         case FK_SOURCES: return wf_event_kernel<FK_SOURCES>;
         case FK_SPLINE: return wf_event_kernel<FK_SPLINE>;
@@ -390,8 +398,33 @@ static WaveFn wf_event_fn(int fk) {
     }
 }
 
+static MarchFn plain_fn(int fk) {
+    switch (fk) {
+        case FK_BESSEL0: return plain_kernel<FK_BESSEL0>;
+        case FK_BESSEL1: return plain_kernel<FK_BESSEL1>;
+        case FK_BESSEL2: return plain_kernel<FK_BESSEL2>;
+        case FK_BESSELN: return plain_kernel<FK_BESSELN>;
+        case FK_PLANEWAVE: return plain_kernel<FK_PLANEWAVE>;
+        case FK_SOURCES: return plain_kernel<FK_SOURCES>;
+        case FK_SPLINE: return plain_kernel<FK_SPLINE>;
+        default: return nullptr;
+    }
+}
+
+// Kernels that stage the Bessel table take it as dynamic shared memory; above the default 48 KB
+// window (a table for k r beyond about 96) a kernel must be opted in to the larger size first.
+static int allow_dynamic_smem(const void *fn, size_t bytes) {
+    if (bytes <= 48u * 1024u) return SMP_OK;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    if (e != cudaSuccess)
+        return set_error(SMP_ERR_CUDA, "shared memory of %zu bytes for the Bessel table: %s", bytes, cudaGetErrorString(e));
+    return SMP_OK;
+}
+
 static int grid_for(int fk, int dev, int blocks_per_sm, size_t smem, int *grid) {
     MarchFn fn = march_fn(fk);
+    int rc = allow_dynamic_smem(reinterpret_cast<const void *>(fn), smem);
+    if (rc) return rc;
     int per_sm = blocks_per_sm;
     if (per_sm <= 0) {
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, smem);
@@ -427,7 +460,7 @@ struct smp_plan {
     smp_stats stats;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> launches;   // since the last clear
     // the slot pool of the two-kernel march (wavefront.cuh); allocated at the first trace
-    bool persistent = false;    // SMP_KERNEL=persistent: the single-kernel march of march.cuh instead
+    int kernel = SMP_KERNEL_POOL;   // smp_kernel (opts.kernel, or SMP_KERNEL=pool|persistent|plain)
     int wave_chunk = 96;
     int wave_slots_per_lane = 6;
     int wave_batch = 16;        // march/event launch pairs between live-slot checks
@@ -533,9 +566,13 @@ static int plan_setup_field(smp_plan *p, const smp_field_desc &f) {
         p->kp.field.coeff4 = p->d_coeff4;
     }
     p->smem_bytes = 0;
-    if (p->fk <= FK_BESSEL2) {
+    if (p->fk <= FK_BESSELN) {
+        const double xmax = box_max_kr(p->scene, p->kp.field.k_r);
+        if (p->fk == FK_BESSELN && xmax > kBesselMaxX)
+            return set_error(SMP_ERR_UNSUPPORTED, "Bessel mode %d: k r reaches %.1f over the box; orders above 2 "
+                             "are built for k r <= %.0f", f.mode, xmax, kBesselMaxX);
         std::vector<float4> tab;
-        bessel_table(f.mode, box_max_kr(p->scene, p->kp.field.k_r), tab);
+        bessel_table(f.mode, xmax, tab);
         cudaFree(p->d_btab);
         p->d_btab = nullptr;
         SMP_CUDA(cudaMalloc(&p->d_btab, tab.size() * sizeof(float4)));
@@ -602,7 +639,16 @@ int smp_plan_create(const smp_scene_desc *scene, const smp_medium_desc *medium, 
     smp_plan *p = new smp_plan();
     p->device = opts->device;
     if (const char *eb = std::getenv("SMP_EVENT_BATCH")) p->event_batch = std::max(1, std::min(32, std::atoi(eb)));
-    if (const char *kn = std::getenv("SMP_KERNEL")) p->persistent = std::strcmp(kn, "persistent") == 0;
+    if (opts->kernel < SMP_KERNEL_POOL || opts->kernel > SMP_KERNEL_PLAIN) {
+        delete p;
+        return set_error(SMP_ERR_BAD_ARG, "kernel %d: not an smp_kernel", opts->kernel);
+    }
+    p->kernel = opts->kernel;
+    if (const char *kn = std::getenv("SMP_KERNEL")) {
+        if (!std::strcmp(kn, "persistent")) p->kernel = SMP_KERNEL_PERSISTENT;
+        else if (!std::strcmp(kn, "plain")) p->kernel = SMP_KERNEL_PLAIN;
+        else if (!std::strcmp(kn, "pool")) p->kernel = SMP_KERNEL_POOL;
+    }
     if (const char *c = std::getenv("SMP_WF_CHUNK")) {
         p->wave_chunk = std::max(2, std::min(4096, std::atoi(c)));
         p->tune_chunk = false;
@@ -745,6 +791,9 @@ static int wave_setup(smp_plan *p) {
     WaveFn fm = wf_march_fn(p->fk, p->kp.fp64 != 0), fe = wf_event_fn(p->fk), ff = wf_finish_fn(p->fk);
     if (!fm || !fe || !ff) return set_error(SMP_ERR_BAD_ARG, "bad field kind");
     int sms = 0, pm = 0, pe = 0, pf = 0;
+    int rc = allow_dynamic_smem(reinterpret_cast<const void *>(fm), p->smem_bytes);
+    if (!rc) rc = allow_dynamic_smem(reinterpret_cast<const void *>(ff), p->smem_bytes);
+    if (rc) return rc;
     SMP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device));
     SMP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pm, fm, kBlock, p->smem_bytes));
     SMP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pe, fe, kBlock, 0));
@@ -933,8 +982,16 @@ static int launch(smp_plan *plan, int64_t first, int64_t n, int64_t weight_photo
     SMP_CUDA(cudaEventCreate(&e1));
     plan->launches.emplace_back(e0, e1);
     SMP_CUDA(cudaEventRecord(e0, s));
-    if (plan->persistent) {
+    if (plan->kernel == SMP_KERNEL_PERSISTENT) {
         march_fn(plan->fk)<<<plan->grid, kBlock, plan->smem_bytes, s>>>(k);
+        SMP_CUDA(cudaGetLastError());
+        plan->n_launched += 1;
+    } else if (plan->kernel == SMP_KERNEL_PLAIN) {
+        MarchFn fp = plain_fn(plan->fk);
+        if (!fp) return set_error(SMP_ERR_UNSUPPORTED, "no plain kernel for field kind %d", plan->fk);
+        const long long blocks = (n + kPlainBlock - 1) / kPlainBlock;
+        if (blocks > 0x7fffffffLL) return set_error(SMP_ERR_BAD_ARG, "too many photons for one plain launch");
+        fp<<<unsigned(blocks), kPlainBlock, 0, s>>>(k);
         SMP_CUDA(cudaGetLastError());
         plan->n_launched += 1;
     } else {
@@ -970,11 +1027,12 @@ static int collect_stats(smp_plan *plan) {
         SMP_CUDA(cudaEventElapsedTime(&ms, plan->march_ev[i], plan->march_ev[i + 1]));
         march_ms += ms;
     }
-    plan->stats.march_ms = plan->persistent ? ms_total : march_ms;
-    plan->stats.march_steps = plan->persistent ? (int64_t)c[CNT_STEPS] : (int64_t)c[CNT_MARCH_STEPS];
+    const bool one_kernel = plan->kernel != SMP_KERNEL_POOL;      // march and events in one kernel
+    plan->stats.march_ms = one_kernel ? ms_total : march_ms;
+    plan->stats.march_steps = one_kernel ? (int64_t)c[CNT_STEPS] : (int64_t)c[CNT_MARCH_STEPS];
     plan->stats.launches = plan->n_launched;
-    plan->stats.march_launches = plan->persistent ? plan->n_launched
-                                                  : (int64_t)(plan->march_ev_used / 2) + plan->graph_march_launches;
+    plan->stats.march_launches = one_kernel ? plan->n_launched
+                                            : (int64_t)(plan->march_ev_used / 2) + plan->graph_march_launches;
     if (c[CNT_STAGE_TIMEOUT]) return set_error(SMP_ERR_CUDA, "%llu block(s) timed out staging the field table", c[CNT_STAGE_TIMEOUT]);
     if (c[CNT_LOST]) return set_error(SMP_ERR_CUDA, "internal: %llu live slot(s) had no lane in the tail kernel", c[CNT_LOST]);
     if (c[CNT_STEP_CAP]) return set_error(SMP_ERR_STEP_CAP, "%llu photon(s) hit the per-photon step cap", c[CNT_STEP_CAP]);
@@ -1137,7 +1195,7 @@ int smp_field_eval(const smp_field_desc *field, double scaling, int64_t n_points
         F.coeff = d_coeff;
     }
     float4 *d_tab = nullptr;
-    if (fk <= FK_BESSEL2 && e == cudaSuccess) {
+    if (fk <= FK_BESSELN && e == cudaSuccess) {
         std::vector<float4> tab;
         bessel_table(field->mode, kBesselMaxX, tab);
         e = cudaMalloc(&d_tab, tab.size() * sizeof(float4));
@@ -1158,6 +1216,7 @@ int smp_field_eval(const smp_field_desc *field, double scaling, int64_t n_points
             case FK_BESSEL0: field_probe_kernel<FK_BESSEL0><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
             case FK_BESSEL1: field_probe_kernel<FK_BESSEL1><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
             case FK_BESSEL2: field_probe_kernel<FK_BESSEL2><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
+            case FK_BESSELN: field_probe_kernel<FK_BESSELN><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
             case FK_PLANEWAVE: field_probe_kernel<FK_PLANEWAVE><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
             case FK_SOURCES: field_probe_kernel<FK_SOURCES><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
             default: field_probe_kernel<FK_SPLINE><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
@@ -1561,9 +1620,12 @@ int smp_render_adjoint(const smp_scene_desc *scene, const smp_medium_desc *mediu
 // <= 1 MiB - 256 bytes (a 501 x 501 texture fits beside any table for k r up to 98; at most 262079
 // texels); Bessel fields (orders 0-2) and plane-wave fields only.
 // Every call on a device shares the scratch and overwrites what the previous call left there (the
-// call clears the counters itself); calls whose GPU work overlaps -- on two streams, or from two
-// host threads -- race on it. The first call on each device looks up the array's device address
-// (cudaGetSymbolAddress); make that first call before any stream capture.
+// call clears the counters itself). Calls whose GPU work overlapped would race on it; this entry
+// point prevents that within a process: it holds a process-wide lock from its first write to the
+// scratch until its own GPU work has finished (it synchronises the stream before returning), so
+// calls from several host threads, or on several streams, run one after another. The first call on
+// each device looks up the array's device address (cudaGetSymbolAddress); make that first call
+// before any stream capture. The caller's current device is restored on return.
 
 #define SMP_NOALLOC_SCRATCH_BYTES (1u << 20)
 static __device__ __align__(256) unsigned char g_noalloc_scratch[SMP_NOALLOC_SCRATCH_BYTES];
@@ -1618,6 +1680,12 @@ extern "C" int smp_render_noalloc(const smp_scene_desc *scene, const smp_medium_
     if (tab_bytes + (size_t(n_tex) + 1) * sizeof(float) > kNoAllocShared)
         return set_error(SMP_ERR_BAD_ARG, "texture has %lld texels; beside this field's Bessel table "
                          "smp_render_noalloc holds at most %zu", n_tex, (kNoAllocShared - tab_bytes) / sizeof(float) - 1);
+    // the caller's current device is put back on every return path
+    struct DeviceRestore {
+        int dev = -1;
+        ~DeviceRestore() { if (dev >= 0) cudaSetDevice(dev); }
+    } restore;
+    if (cudaGetDevice(&restore.dev) != cudaSuccess) restore.dev = -1;
     rc = check_device(opts->device);
     if (rc) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -292,6 +292,58 @@ __device__ __forceinline__ void bessel_field_rt(const FieldParams &F, const floa
     g = f3(0.0f, fmaf(a1, y, -a2 * z), fmaf(a1, z, a2 * y));
 }
 
+// Bessel mode m >= 3 (scene.cpp:206-257 take any integer order through jn(mode, .)): J_m and J_m+1
+// from the per-plan table, which the host sizes to cover the whole box (k r <= 128, checked when the
+// plan is made; a point beyond it reads the table's last interval); cos(m phi), sin(m phi) as
+// ((z + i y)/r)^m by m - 1 complex products.
+__device__ __forceinline__ void bessel_field_n(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) {
+    const int M = F.mode;
+    const float A = F.amp * (in_gap(F, p) ? 0.0f : s);
+    float y = p.y, z = p.z;
+    const float r2 = fmaf(y, y, z * z);
+    float rs = rsqrt_fast(r2);                 // +inf at r2 = 0
+    float r = r2 > 0.0f ? r2 * rs : 0.0f;
+    float cm = 1.0f, sm = 0.0f;
+    if (r2 > 0.0f) {
+        const float c = z * rs, sn = y * rs;
+        cm = c; sm = sn;
+        for (int k = 1; k < M; ++k) {
+            const float t = fmaf(cm, c, -sm * sn);
+            sm = fmaf(cm, sn, sm * c);
+            cm = t;
+        }
+    }
+    auto lookup = [&](float x, float &jm, float &jm1) {
+        float t = fminf(x * F.binv_h, float(F.bint) - 1.0f / 64.0f);
+        const float tb = __fadd_rd(t, 8388608.0f);
+        const int i = __float_as_int(tb) - 0x4B000000;
+        const float f = t - (tb - 8388608.0f);
+        const float4 a = tab[2 * i], b = tab[2 * i + 1];
+        jm = fmaf(fmaf(fmaf(a.w, f, a.z), f, a.y), f, a.x);
+        jm1 = fmaf(fmaf(fmaf(b.w, f, b.z), f, b.y), f, b.x);
+    };
+    float jm, jm1;
+    lookup(F.k_r * r, jm, jm1);
+    n = fmaf(A * jm, cm, F.n_o);
+    if (!(r >= kEps)) {                        // the gradient's near-axis substitution (scene.cpp:229-234)
+        y = kEps; z = kEps; r = kEps; rs = 1.0f / kEps;
+        lookup(F.k_r * kEps, jm, jm1);
+    }
+    const float fm = float(M);
+    const float djm = fmaf(fm * F.inv_k * rs, jm, -jm1);
+    const float a1 = A * djm * F.k_r * rs * cm;
+    const float a2 = A * jm * fm * sm * rs * rs;
+    g = f3(0.0f, fmaf(a1, y, -a2 * z), fmaf(a1, z, a2 * y));
+}
+template <> struct Field<FK_BESSELN> {
+    static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) {
+        bessel_field_n(F, tab, p, s, n, g);
+    }
+    static __device__ __forceinline__ void eval_ng(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) {
+        bessel_field_n(F, tab, p, s, n, g);
+    }
+};
+
 // batched sweep: the instance's Bessel field
 template <> struct Field<FK_BATCH> {
     static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *tab, float3 p, float s, float &n, float3 &g) {

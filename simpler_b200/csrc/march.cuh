@@ -13,10 +13,15 @@
 // Discrete decisions follow the reference CPU build exactly; the tests compare every photon's
 // splats and end state with the CPU restatement on injected uniform streams.
 #pragma once
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+
 #include "dev_field.cuh"
 #include "kparams.h"
 
 namespace smp {
+
+namespace cg = cooperative_groups;
 
 static constexpr unsigned kFull = 0xffffffffu;
 
@@ -202,12 +207,25 @@ __device__ __forceinline__ bool propagate_till_sensor(const KParams &P, float3 &
     return true;
 }
 
-// Scene::addEnergyToImage (scene.cpp:782-829) with bilinear sharing (USE_PIXEL_SHARING)
+// Scene::addEnergyToImage (scene.cpp:782-829) with bilinear sharing (USE_PIXEL_SHARING): one tap,
+// Image3::addEnergy (image.h:320-324) with the bounds check of addPixel (scene.h:305-312).
+// Warp-aggregated: the lanes that reach this call together are grouped by the film address they
+// add to (__match_any_sync through cooperative groups), each group sums its values (in double for
+// the FP64 film) and one lane issues the atomic. A narrow beam's direct light lands on a handful of
+// pixels, where one atomic per lane would serialise on the same address.
 __device__ __forceinline__ void add_pixel(const KParams &P, void *film, int x, int y, int z, float v) {
-    if (x >= 0 && x < P.X && y >= 0 && y < P.Y && z >= 0 && z < P.Z) {
-        size_t i = (size_t(z) * P.Y + y) * P.X + x;
-        if (P.fp64) atomicAdd(reinterpret_cast<double *>(film) + i, double(v));
-        else atomicAdd(reinterpret_cast<float *>(film) + i, v);
+    const bool in = x >= 0 && x < P.X && y >= 0 && y < P.Y && z >= 0 && z < P.Z;
+    const size_t i = in ? (size_t(z) * P.Y + y) * P.X + x : 0;
+    const unsigned long long key =
+        in ? reinterpret_cast<unsigned long long>(film) + (unsigned long long)i * (P.fp64 ? 8ull : 4ull) : 0ull;
+    const cg::coalesced_group active = cg::coalesced_threads();
+    const cg::coalesced_group same = cg::labeled_partition(active, key);
+    if (P.fp64) {
+        const double s = cg::reduce(same, double(v), cg::plus<double>());
+        if (in && same.thread_rank() == 0) atomicAdd(reinterpret_cast<double *>(film) + i, s);
+    } else {
+        const float s = cg::reduce(same, v, cg::plus<float>());
+        if (in && same.thread_rank() == 0) atomicAdd(reinterpret_cast<float *>(film) + i, s);
     }
 }
 
@@ -816,7 +834,7 @@ __global__ void __launch_bounds__(128, SMP_MIN_BLOCKS) march_kernel(const __grid
     L.end = 0;
     L.idx = 0;
     L.tab = P.field.btab;
-    if (FK <= FK_BESSEL2 && P.field.btab != nullptr) {
+    if (FK <= FK_BESSELN && P.field.btab != nullptr) {
         if (!stage_to_shared(smem_tab, P.field.btab, unsigned(P.field.bnodes) * 16u, P.counters + CNT_STAGE_TIMEOUT))
             return;                                  // whole block: other blocks take the photons
         L.tab = smem_tab;

@@ -159,7 +159,7 @@ wf_march_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
     const int lane = threadIdx.x & 31, cur = it & 1, nxt = cur ^ 1;
     const unsigned n = W.cnt[cur];
     if (n == 0u) return;
-    if (FK <= FK_BESSEL2) {
+    if (FK <= FK_BESSELN) {
         if (!stage_to_shared(smem_tab, P.field.btab, unsigned(P.field.bnodes) * 16u, P.counters + CNT_STAGE_TIMEOUT)) {
             // timed out (recorded in the counters): copy with plain loads; a late bulk copy
             // writes the same bytes
@@ -286,7 +286,7 @@ wf_finish_kernel(const __grid_constant__ KParams P, const __grid_constant__ Wave
     const unsigned gid = blockIdx.x * blockDim.x + threadIdx.x, lanes = gridDim.x * blockDim.x;
     if (gid == 0 && n > lanes) atomicAdd(P.counters + CNT_LOST, (unsigned long long)(n - lanes));
     const float4 *tab = P.field.btab;
-    if (FK <= FK_BESSEL2 && P.field.btab != nullptr) {
+    if (FK <= FK_BESSELN && P.field.btab != nullptr) {
         if (stage_to_shared(smem_tab, P.field.btab, unsigned(P.field.bnodes) * 16u, P.counters + CNT_STAGE_TIMEOUT))
             tab = smem_tab;
     }

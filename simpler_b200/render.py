@@ -220,22 +220,62 @@ def roi_weights(setup: Setup, size: int = 32) -> np.ndarray:
     return g
 
 
-def adjoint_sharded(plan, dJ_dfilm: np.ndarray, n_photons: int, rank: int = 0, world: int = 1,
-                    all_reduce=None) -> np.ndarray:
-    """The gradient of the n_photons render over `world` processes (one GPU each): this rank
-    differentiates its contiguous photon range -- photon k draws Philox stream (seed, k) on any
-    rank, so the ranges add up to the single-process gradient -- and `all_reduce` (a callable that
-    sums a float64 array over the ranks in place and returns it, e.g. over torch.distributed)
-    combines them. `plan` is this rank's Plan (anything with Plan.adjoint's signature)."""
+def shard_range(n_photons: int, rank: int, world: int) -> tuple[int, int]:
+    """This rank's contiguous photon range [first, first + n) of an n_photons render split over
+    `world` processes. Photon k draws Philox stream (seed, k) on any rank, so the shards add up to
+    the single-process render for any world size."""
     per = -(-int(n_photons) // int(world))
     first = int(rank) * per
-    n = max(0, min(per, int(n_photons) - first))
+    return first, max(0, min(per, int(n_photons) - first))
+
+
+_COUNT_KEYS = ("photons", "er_steps", "splats", "step_cap_hits", "nan_photons")
+_ADJ_COUNT_KEYS = ("photons", "dropped", "skipped", "aborted", "replay_mismatch")
+
+
+def render_sharded(plan, n_photons: int, rank: int = 0, world: int = 1, all_reduce=None,
+                   stream: int = 0) -> tuple[np.ndarray, dict]:
+    """The film of the n_photons render over `world` processes (one GPU each, photons split by
+    contiguous index range): this rank clears its plan's film, traces its own photon range with the render's
+    photon weight (Li T / n_photons, photon.h:76-80), and reads the FP64 film back; `all_reduce` (a
+    callable that sums a float64 numpy array over the ranks and returns it, e.g. over
+    torch.distributed) combines the films and the photon / step / splat counts in one call. Returns
+    (film, counts); without all_reduce, this rank's share."""
+    first, n = shard_range(n_photons, rank, world)
+    plan.clear(stream)
     if n > 0:
-        grad, _ = plan.adjoint(dJ_dfilm, first, n, int(n_photons))
+        plan.trace(first, n, int(n_photons), stream)
+    film = plan.read_image()
+    st = plan.stats()
+    counts = np.array([float(getattr(st, k)) for k in _COUNT_KEYS])
+    if all_reduce is not None:
+        packed = all_reduce(np.concatenate([film.ravel(), counts]))
+        film = np.asarray(packed[:film.size]).reshape(film.shape)
+        counts = np.asarray(packed[film.size:])
+    return film, {k: int(round(v)) for k, v in zip(_COUNT_KEYS, counts)}
+
+
+def adjoint_sharded(plan, dJ_dfilm: np.ndarray, n_photons: int, rank: int = 0, world: int = 1,
+                    all_reduce=None) -> tuple[np.ndarray, dict]:
+    """The gradient of the n_photons render over `world` processes (one GPU each): this rank
+    differentiates its contiguous photon range (`shard_range`) and `all_reduce` (a callable that
+    sums a float64 array over the ranks and returns it) combines the gradients together with the
+    photon counts of the adjoint statistics, so every rank sees how many photons were
+    differentiated and how many were dropped, skipped (sensor marches) or aborted anywhere. `plan`
+    is this rank's Plan (anything with Plan.adjoint's signature). Returns (gradient, counts)."""
+    first, n = shard_range(n_photons, rank, world)
+    counts = np.zeros(len(_ADJ_COUNT_KEYS))
+    if n > 0:
+        grad, st = plan.adjoint(dJ_dfilm, first, n, int(n_photons))
         grad = np.asarray(grad, dtype=np.float64)
+        if st is not None:
+            counts = np.array([float(getattr(st, k)) for k in _ADJ_COUNT_KEYS])
     else:
         grad = np.zeros(param_count(plan.setup), dtype=np.float64)
-    return all_reduce(grad) if all_reduce is not None else grad
+    if all_reduce is not None:
+        packed = all_reduce(np.concatenate([grad, counts]))
+        grad, counts = np.asarray(packed[:grad.size]), np.asarray(packed[grad.size:])
+    return grad, {k: int(round(v)) for k, v in zip(_ADJ_COUNT_KEYS, counts)}
 
 
 def adjoint(setup: Setup, n_photons: int, dJ_dfilm: np.ndarray) -> tuple[np.ndarray, L.AdjointStats]:

@@ -111,37 +111,44 @@ class Setup:
     sensor_march_max: float = 0.0
     device: int = 0
     blocks_per_sm: int = 0
+    kernel: int = L.KERNEL_POOL     # smp_kernel: slot pool (default), persistent lane loop, or plain
 
     # ---- descriptors -------------------------------------------------------------------------
     def film_shape(self) -> tuple:
         return (self.path_length_bins, self.spatial_y, self.spatial_x)
 
     def scene_desc(self) -> L.SceneDesc:
+        """The scene as the reference's front-end assembles it (renderer3d_sample.cpp:807-830): the
+        box, the source, lens and sensor origins and the film's extents are computed in its Float
+        (single precision) and handed over as those float values, so the FP32 path and an FP64
+        evaluation of the same descriptors place the source, the faces and the gaps identically
+        (a source point on the gap boundary is then inside the field in both)."""
+        f32 = np.float32
         s = L.SceneDesc()
         s.ior = self.ior
-        s.medium_l[:] = self.medium_l
-        s.medium_r[:] = self.medium_r
-        s.light_origin[:] = (self.medium_r[0] + self.emitter_distance, 0.0, 0.0)
+        s.medium_l[:] = tuple(float(f32(v)) for v in self.medium_l)
+        s.medium_r[:] = tuple(float(f32(v)) for v in self.medium_r)
+        s.light_origin[:] = (float(f32(self.medium_r[0]) + f32(self.emitter_distance)), 0.0, 0.0)
         ang = np.float32(math.pi)        # lightAngle = M_PI in Float (renderer3d_sample.cpp:815)
         s.light_dir[:] = (float(np.cos(ang)), float(np.sin(ang)), 0.0)
         s.half_theta_limit = self.half_theta_limit
-        s.light_plane[:] = (self.emitter_size, self.emitter_size)
+        s.light_plane[:] = (float(f32(self.emitter_size)), float(f32(self.emitter_size)))
         s.Li = self.Li
         tex = np.ascontiguousarray(self.texture, dtype=np.float64)
         self._tex_keep = tex
         s.tex_y, s.tex_x = tex.shape
         s.texture = tex.ctypes.data_as(C.POINTER(C.c_double))
-        s.emitter_lens_origin[:] = (self.medium_r[0], 0.0, 0.0)
+        s.emitter_lens_origin[:] = (float(f32(self.medium_r[0])), 0.0, 0.0)
         s.emitter_lens_aperture = self.emitter_lens_aperture
         s.emitter_lens_focal_length = self.emitter_lens_focal_length
         s.emitter_lens_active = int(self.emitter_lens_active)
         s.use_bounce_decomposition = int(self.use_bounce_decomposition)
-        s.view_origin[:] = (self.medium_l[0] - self.sensor_distance, 0.0, 0.0)
+        s.view_origin[:] = (float(f32(self.medium_l[0]) - f32(self.sensor_distance)), 0.0, 0.0)
         s.view_dir[:] = (-1.0, 0.0, 0.0)
         s.view_horizontal[:] = (0.0, -1.0, 0.0)
-        s.view_plane[:] = (self.sensor_size, self.sensor_size)
-        s.pathlength_range[:] = (self.path_length_min, self.path_length_max)
-        s.sensor_lens_origin[:] = (self.medium_l[0], 0.0, 0.0)
+        s.view_plane[:] = (float(f32(self.sensor_size)), float(f32(self.sensor_size)))
+        s.pathlength_range[:] = (float(f32(self.path_length_min)), float(f32(self.path_length_max)))
+        s.sensor_lens_origin[:] = (float(f32(self.medium_l[0])), 0.0, 0.0)
         s.sensor_lens_aperture = self.sensor_lens_aperture
         s.sensor_lens_focal_length = self.sensor_lens_focal_length
         s.sensor_lens_active = int(self.sensor_lens_active)
@@ -199,6 +206,7 @@ class Setup:
         o.step_cap = self.step_cap
         o.blocks_per_sm = self.blocks_per_sm
         o.sensor_march_max = self.sensor_march_max
+        o.kernel = self.kernel
         return o
 
     def descs(self):

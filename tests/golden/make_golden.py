@@ -27,7 +27,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+# the reference checkout: the first argument, else $SIMPLER_REFERENCE_ROOT, else /root/reference
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SIMPLER_REFERENCE_ROOT", "/root/reference")
 
 
 def read(rel):

@@ -91,16 +91,19 @@ def oracle_trace(setup, first: int, n: int, weight_photons: int, uniforms=None, 
 def oracle_fd_gradient(setup, index: int, h: float, n: int, G: np.ndarray, threads: int = 0) -> float:
     """FP64 reference gradient: the central difference of sum(G * film) in field parameter `index`
     (simpler_b200.field_params order) with the FP64 restatement on common random numbers (the same
-    Philox photons 0..n-1 on both sides). Parameters enter the FP64 arithmetic unrounded, so the
-    step is exactly 2h."""
+    Philox photons 0..n-1 on both sides). The step is the difference of the two parameter values as
+    the renders receive them (with_field_params stores spline coefficients in float32, so there it
+    is the float32 rounding of +-h; Bessel and plane-wave parameters stay float64)."""
     import simpler_b200 as sb
     th = sb.field_params(setup)
     tp, tm = th.copy(), th.copy()
     tp[index] += h
     tm[index] -= h
-    _, ip = oracle_trace(sb.with_field_params(setup, tp), 0, n, n, records=False, real_bits=64, threads=threads)
-    _, im = oracle_trace(sb.with_field_params(setup, tm), 0, n, n, records=False, real_bits=64, threads=threads)
-    return float(((ip - im) * G).sum()) / (2.0 * h)
+    sp, sm = sb.with_field_params(setup, tp), sb.with_field_params(setup, tm)
+    dh = float(sb.field_params(sp)[index]) - float(sb.field_params(sm)[index])
+    _, ip = oracle_trace(sp, 0, n, n, records=False, real_bits=64, threads=threads)
+    _, im = oracle_trace(sm, 0, n, n, records=False, real_bits=64, threads=threads)
+    return float(((ip - im) * G).sum()) / dh
 
 
 def oracle_field(setup, scaling: float, points: np.ndarray, real_bits: int = 64):

@@ -54,3 +54,35 @@ def summary(c: dict) -> str:
             f"max dir {c['dir_err'][c['same_events']].max() if c['same_events'].any() else 0:.3g} rad, "
             f"max path {c['path_err'][c['same_events']].max() if c['same_events'].any() else 0:.3g} m, "
             f"max splat rel value {c['spl_val'].max():.3g}")
+
+
+def run_pair(setup, n, per_photon=256, weight=1_000_000, threads=0, real_bits=32):
+    """The GPU (through the C ABI) and the oracle on the same injected SFMT streams: photon i draws
+    from SFMT-19937 seeded with setup.seed + i, the reference's per-photon seeding (photon.cpp:313).
+    Returns (gpu records, gpu film, oracle records, oracle film)."""
+    import oracle_bridge as ob
+    import simpler_b200 as sb
+    u, off = ob.sfmt_streams(setup.seed, 0, n, per_photon)
+    g, gimg = sb.trace_photons(setup, 0, n, weight, uniforms=u, offsets=off)
+    g = sb.records_to_arrays(g)
+    r, rimg = ob.oracle_trace(setup, 0, n, weight, uniforms=u, offsets=off, threads=threads, real_bits=real_bits)
+    return g, gimg, r, rimg
+
+
+def check(setup, n, min_ok=0.98, min_events=0.995, per_photon=256, img_tol=5e-4, real_bits=32, threads=0):
+    """Photon-by-photon parity of the GPU against the oracle: at least `min_events` of the photons
+    take the same discrete events and at least `min_ok` are within every tolerance above; the films
+    agree to `img_tol` in relative L1. Prints and returns the comparison."""
+    g, gimg, r, rimg = run_pair(setup, n, per_photon, real_bits=real_bits, threads=threads)
+    assert not (r["end"] == 8).any(), "oracle ran out of injected uniforms"
+    c = compare_records(g, r)
+    msg = summary(c)
+    print(msg)
+    assert c["same_events"].mean() >= min_events, msg
+    assert c["ok"].mean() >= min_ok, msg
+    denom = np.abs(rimg).sum()
+    if denom > 0:
+        rel = np.abs(gimg - rimg).sum() / denom
+        assert rel < img_tol, (rel, msg)
+    c["film_rel_l1"] = float(np.abs(gimg - rimg).sum() / denom) if denom > 0 else 0.0
+    return c

@@ -54,7 +54,7 @@ def test_bad_arguments_are_rejected_before_any_device_work():
     fd.er_stepsize = 0.0
     assert lib.smp_render(C.byref(sc), C.byref(md), C.byref(fd), C.byref(op), 10, C.c_void_p(img.ctypes.data), None) == L.SMP_ERR_BAD_ARG
     sc, md, fd, op = s.descs()
-    fd.mode = 7
+    fd.mode = 99                 # above the largest built order
     ptr = C.c_void_p()
     rc = lib.smp_plan_create(C.byref(sc), C.byref(md), C.byref(fd), C.byref(op), C.byref(ptr))
     assert rc in (L.SMP_ERR_UNSUPPORTED, L.SMP_ERR_NO_DEVICE)

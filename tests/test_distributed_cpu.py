@@ -1,6 +1,8 @@
-"""CPU, two gloo ranks: the multi-GPU decomposition of bench.py -- each rank traces its own
-contiguous photon range with streams keyed by the global photon index, then the FP64 films are
-summed -- reproduces the single-process render. The oracle stands in for the per-rank kernel."""
+"""CPU, two gloo ranks: the host logic of the multi-GPU decomposition -- each rank takes its own
+contiguous photon range (shard_range) with streams keyed by the global photon index, then the FP64
+films (or gradients, with their statistics) are summed -- reproduces the single-process result.
+With no GPU here, the oracle traces each rank's range; tests/test_distributed_gpu.py runs the same
+decomposition through real Plans on the GPU."""
 import os
 import socket
 
@@ -25,8 +27,8 @@ def _rank(rank, world, port, out):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
-    per = N // world
-    _, img = ob.oracle_trace(_setup(), rank * per, per, N, records=False, threads=2)
+    first, n = sb.shard_range(N, rank, world)
+    _, img = ob.oracle_trace(_setup(), first, n, N, records=False, threads=2)
     t = torch.from_numpy(img)
     dist.all_reduce(t)
     if rank == 0:
@@ -47,13 +49,18 @@ def test_two_rank_photon_sharding_matches_single_process(tmp_path):
 
 
 class _AdditivePlan:
-    """Stands in for a Plan: its 'gradient' of photons [first, first + n) is additive over photon
-    ranges, as Plan.adjoint's is (tests/test_adjoint.py checks that on the GPU)."""
+    """Stands in for a Plan in the split-and-reduce logic: its 'gradient' of photons [first, first +
+    n) is additive over photon ranges, as Plan.adjoint's is (tests/test_distributed_gpu.py runs the
+    real Plans), and every call reports one dropped photon."""
     setup = sb.config_planewave()
+
+    class _Stats:
+        def __init__(self, n):
+            self.photons, self.dropped, self.skipped, self.aborted, self.replay_mismatch = n, 1, 0, 0, 0
 
     def adjoint(self, G, first, n, weight):
         k = np.arange(first, first + n, dtype=np.float64)
-        return np.array([k.sum(), (k * k).sum(), np.sin(k).sum(), float(n)]) / weight, None
+        return np.array([k.sum(), (k * k).sum(), np.sin(k).sum(), float(n)]) / weight, self._Stats(n)
 
 
 def _adjoint_rank(rank, world, port, out, n_photons):
@@ -68,9 +75,9 @@ def _adjoint_rank(rank, world, port, out, n_photons):
         dist.all_reduce(t)
         return t.numpy()
 
-    g = sb.adjoint_sharded(_AdditivePlan(), None, n_photons, rank, world, all_reduce)
+    g, counts = sb.adjoint_sharded(_AdditivePlan(), None, n_photons, rank, world, all_reduce)
     if rank == 0:
-        np.save(out, g)
+        np.save(out, np.concatenate([g, [counts["photons"], counts["dropped"]]]))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -83,6 +90,9 @@ def test_two_rank_adjoint_sharding_matches_single_process(tmp_path):
     out = str(tmp_path / "grad.npy")
     mp.spawn(_adjoint_rank, args=(2, port, out, n_photons), nprocs=2, join=True)
     sharded = np.load(out)
-    single = sb.adjoint_sharded(_AdditivePlan(), None, n_photons)
-    assert np.allclose(sharded, single, rtol=1e-12)
+    single, counts = sb.adjoint_sharded(_AdditivePlan(), None, n_photons)
+    assert np.allclose(sharded[:4], single, rtol=1e-12)
     assert single[3] * n_photons == n_photons          # every photon exactly once
+    # the statistics travel with the gradient: photons counted once, drops from both ranks summed
+    assert sharded[4] == n_photons == counts["photons"]
+    assert sharded[5] == 2 * counts["dropped"] == 2

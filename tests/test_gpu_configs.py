@@ -1,0 +1,170 @@
+"""GPU parity on the configurations the basic parity cases leave out: thin lenses and the source
+cone, the spline field on its full 64^3 grid, the precision scale-up film at full size, Bessel orders
+above 2, a Bessel table larger than the default shared-memory window, every kernel choice, and an
+image test on independent random streams (each film bin within 3 sigma of its Monte Carlo error).
+
+Photon-by-photon cases inject the reference's per-photon SFMT streams into the GPU and the CPU
+oracle and compare records (tests/parity.py: positions 1e-4 mm, directions 1e-5 rad, path lengths
+1e-4 mm, splat values 1e-4 relative); each prints the fraction of photons within every tolerance.
+"""
+import numpy as np
+import pytest
+
+import oracle_bridge as ob
+import parity
+import simpler_b200 as sb
+from simpler_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+
+# ---- lenses and the source cone (lens.cpp:20-97, camera.cpp:54-75, scene.cpp:120-129) ----------
+def test_parity_emitter_lens_and_cone():
+    # the source 2 mm outside the medium, a thin lens on the entry face focusing 5 mm deep, and a
+    # 0.3 rad cone of directions around -x
+    s = sb.config_plain_small(rng=L.RNG_STREAM, emitter_distance=0.002, emitter_lens_active=True,
+                              emitter_lens_aperture=0.0004, emitter_lens_focal_length=0.005, half_theta_limit=0.3)
+    parity.check(s, 1500)
+
+
+def test_parity_emitter_lens_rejects_outside_aperture():
+    # an aperture smaller than the beam: photons outside it end at genRay (scene.cpp:130-134)
+    s = sb.config_plain_small(rng=L.RNG_STREAM, emitter_distance=0.001, emitter_lens_active=True,
+                              emitter_lens_aperture=0.0003, emitter_lens_focal_length=0.01)
+    g, _, r, _ = parity.run_pair(s, 800)
+    genray_fail = 1                             # smp_photon_end SMP_END_GENRAY_FAIL
+    assert (r["end"] == genray_fail).mean() > 0.2
+    assert ((g["end"] == genray_fail) == (r["end"] == genray_fail)).all()
+    c = parity.compare_records(g, r)
+    assert c["same_events"].mean() >= 0.995 and c["ok"].mean() >= 0.98, parity.summary(c)
+
+
+def test_parity_sensor_lens():
+    s = sb.config_plain_small(rng=L.RNG_STREAM, sensor_distance=0.003, sensor_lens_active=True,
+                              sensor_lens_aperture=0.004, sensor_lens_focal_length=0.004)
+    parity.check(s, 1500)
+
+
+def test_parity_all_optics_mode1():
+    s = sb.config_plain_small(rng=L.RNG_STREAM, mode=1, n_max=2e-3, n_clip=2e-3, emitter_distance=0.002,
+                              emitter_lens_active=True, emitter_lens_aperture=0.0005,
+                              emitter_lens_focal_length=0.006, half_theta_limit=0.15, sensor_distance=0.002,
+                              sensor_lens_active=True, sensor_lens_aperture=0.005, sensor_lens_focal_length=0.006)
+    parity.check(s, 1500)
+
+
+# ---- the benchmark configurations at their own sizes ------------------------------------------
+def test_parity_spline_full_64_grid():
+    # the spline adjoint configuration's own 64^3 Gaussian-filtered grid and 256x256x64 film
+    s = sb.config_spline(rng=L.RNG_STREAM)
+    parity.check(s, 300, per_photon=2048)
+
+
+def test_parity_precision_full_film():
+    # the headline configuration's 512x512x128 FP64 film (four oracle threads: one film each)
+    s = sb.config_precision(rng=L.RNG_STREAM)
+    parity.check(s, 2000, per_photon=1024, threads=4)
+
+
+# ---- kernels: all three run the same per-photon code ---------------------------------------------
+@pytest.mark.parametrize("kernel", [L.KERNEL_PLAIN, L.KERNEL_PERSISTENT])
+def test_parity_other_kernels(kernel):
+    parity.check(sb.config_plain_small(rng=L.RNG_STREAM, kernel=kernel), 2000)
+
+
+def test_plain_kernel_film_equals_pool_film():
+    s = sb.config_precision(seed=9, spatial_x=64, spatial_y=64, path_length_bins=16)
+    n = 100_000
+    pool, sp = sb.render(s, n)
+    s.kernel = L.KERNEL_PLAIN
+    plain, sq = sb.render(s, n)
+    assert sp.photons == sq.photons == n
+    assert sp.er_steps == sq.er_steps and sp.splats == sq.splats
+    rel = np.abs(plain - pool).sum() / np.abs(pool).sum()
+    assert rel < 1e-9, rel                      # FP64 film: only the order of the atomics differs
+
+
+# ---- Bessel orders above 2 (scene.cpp:206-257 take any order) -------------------------------------
+@pytest.mark.parametrize("mode,f_u", [(3, 848e3), (5, 2e6)])
+def test_parity_bessel_higher_orders(mode, f_u):
+    s = sb.config_plain_small(rng=L.RNG_STREAM, mode=mode, f_u=f_u, n_max=2e-3, n_clip=2e-3, emitter_gap=0.001)
+    parity.check(s, 1500)
+
+
+def test_field_probe_higher_orders():
+    rng = np.random.default_rng(1)
+    pts = rng.uniform(-0.005, 0.005, size=(4000, 3))
+    pts[:10, 1:] = 0.0
+    pts[10:20, 1:] *= 1e-5
+    for mode, f_u in ((3, 848e3), (4, 1.5e6), (7, 2e6)):
+        setup = sb.config_plain_small(mode=mode, f_u=f_u, n_max=2e-3)
+        gn, gg = sb.field_eval(setup, 0.8, pts)
+        rn, rg = ob.oracle_field(setup, 0.8, pts, real_bits=64)
+        assert np.abs(gn - rn).max() < 4e-7, (mode, np.abs(gn - rn).max())
+        scale = np.abs(rg).max()
+        assert np.abs(gg - rg).max() < 2e-4 * scale + 1e-6, (mode, np.abs(gg - rg).max(), scale)
+
+
+def test_bessel_order_above_table_range_is_rejected():
+    # orders above 2 read J_m from the table alone, which covers k r <= 128 over the box
+    s = sb.config_plain_small(mode=3, f_u=6e6)
+    with pytest.raises(sb.SmpError) as e:
+        sb.render(s, 10)
+    assert e.value.code == L.SMP_ERR_UNSUPPORTED
+
+
+# ---- a Bessel table beyond the 48 KB default shared-memory window -------------------------------
+def test_parity_large_bessel_table():
+    # 4 MHz in the 10 mm cube: k r reaches about 120, a 61 KB table staged in shared memory
+    s = sb.config_plain_small(rng=L.RNG_STREAM, mode=1, f_u=4e6, n_max=2e-3, n_clip=2e-3)
+    parity.check(s, 1500)
+    for kernel in (L.KERNEL_PERSISTENT, L.KERNEL_POOL):
+        img, st = sb.render(sb.config_plain_small(mode=1, f_u=4e6, n_max=2e-3, kernel=kernel, spatial_x=32,
+                                                  spatial_y=32, path_length_bins=8), 20_000)
+        assert st.photons == 20_000 and img.sum() > 0
+
+
+# ---- independent streams: the film within its Monte Carlo error -----------------------------------
+def test_film_within_three_sigma_of_fp64_oracle_independent_streams():
+    """The GPU film (Philox streams, FP32 march, FP64 film) and the FP64 oracle's film (SFMT streams,
+    the reference's own generator) are independent estimates of the same image: per bin their
+    difference is Monte Carlo noise. sigma per bin comes from the spread of K GPU sub-films; the
+    oracle's variance is the same per-photon variance over its own photon count.
+
+    The estimator is heavy-tailed: a connection whose sampled direction lines up with the photon's
+    own (Henyey-Greenstein g = 0.9 peaks at 190 times its mean) is a rare, large splat. A bin that
+    few photons reach is a sum of a handful of such values and not Gaussian, so the test keeps the
+    bins whose value is converged in every GPU sub-film (their spread below 25 % of their mean) and
+    prints the statistic over every bin with data beside it."""
+    shape = dict(spatial_x=12, spatial_y=12, path_length_bins=6, precision_mode=L.PREC_MIXED)
+    s = sb.config_plain_small(seed=11, **shape)
+    n_g, k_sub = 3_200_000, 32
+    per = n_g // k_sub
+    plan = sb.Plan(s)
+    subs = []
+    for k in range(k_sub):
+        plan.clear()
+        plan.trace(k * per, per, n_g)
+        subs.append(plan.read_image())
+    plan.close()
+    subs = np.stack(subs)                       # each a 1/K share of the N_g-photon film
+    film_g = subs.sum(axis=0)
+    var_g = subs.var(axis=0, ddof=1) * k_sub    # variance of the sum of K independent shares
+    n_r = 300_000
+    so = sb.config_plain_small(rng=L.RNG_SFMT, seed=0, **shape)
+    _, film_r = ob.oracle_trace(so, 0, n_r, n_r, records=False, real_bits=64)
+    sigma = np.sqrt(var_g * (1.0 + n_g / n_r))  # same per-photon variance, N_r photons
+    mean_sub = subs.mean(axis=0)
+    cv = subs.std(axis=0, ddof=1) / np.maximum(mean_sub, 1e-300)
+    converged = (mean_sub > 0) & (cv < 0.25)
+    any_data = (subs > 0).sum(axis=0) >= k_sub // 2
+    for name, sel in (("converged", converged), ("with data", any_data)):
+        z = (film_g - film_r)[sel] / sigma[sel]
+        print(f"{name}: {sel.sum()} bins, {np.mean(np.abs(z) <= 3.0) * 100:.2f} % within 3 sigma, "
+              f"mean z^2 {np.mean(z * z):.3f}")
+    print(f"film sums {film_g.sum():.6g} (GPU) {film_r.sum():.6g} (oracle)")
+    z = (film_g - film_r)[converged] / sigma[converged]
+    assert converged.sum() >= 60
+    assert np.mean(np.abs(z) <= 3.0) >= 0.99
+    assert np.mean(z * z) < 2.5
+    assert abs(film_g.sum() / film_r.sum() - 1.0) < 0.02

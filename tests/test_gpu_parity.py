@@ -17,27 +17,9 @@ from simpler_b200 import _lib as L
 pytestmark = pytest.mark.gpu
 
 
-def _run_pair(setup, n, per_photon=256, weight=1_000_000, threads=0, real_bits=32):
-    u, off = ob.sfmt_streams(setup.seed, 0, n, per_photon)
-    g, gimg = sb.trace_photons(setup, 0, n, weight, uniforms=u, offsets=off)
-    g = sb.records_to_arrays(g)
-    r, rimg = ob.oracle_trace(setup, 0, n, weight, uniforms=u, offsets=off, threads=threads, real_bits=real_bits)
-    return g, gimg, r, rimg
-
-
 def _check(setup, n, min_ok=0.98, min_events=0.995, per_photon=256, img_tol=5e-4, real_bits=32):
-    g, gimg, r, rimg = _run_pair(setup, n, per_photon, real_bits=real_bits)
-    assert (r["end"] != L.SMP_ERR_STREAM).all()
-    assert not (r["end"] == 8).any(), "oracle ran out of injected uniforms"
-    c = parity.compare_records(g, r)
-    msg = parity.summary(c)
-    assert c["same_events"].mean() >= min_events, msg
-    assert c["ok"].mean() >= min_ok, msg
-    # photons with equal events: every splat position / path / value within tolerance for most
-    denom = np.abs(rimg).sum()
-    if denom > 0:
-        assert np.abs(gimg - rimg).sum() / denom < img_tol, msg
-    return c
+    return parity.check(setup, n, min_ok=min_ok, min_events=min_events, per_photon=per_photon, img_tol=img_tol,
+                        real_bits=real_bits)
 
 
 def test_parity_bessel_mode0_plain_small():
