@@ -4,6 +4,8 @@
   compiled for sm_100a only, plus the C++ host layer (``csrc/host/smp_host.cpp``: file formats,
   the reference's key=value and JSON front-ends);
 * ``bin/renderer3d`` and ``bin/simplER`` -- the reference's two command-line front-ends over it;
+* ``pybind_ext/{tvector,phase,medium,image,scene,photon}_pybind`` -- the reference's Python modules,
+  compiled with pybind11 over the C ABI;
 * the CPU oracle (``oracle/liboracle*.so``) and, when the reference checkout is present, the
   reference's own primitives (``oracle/_ref``) -- test infrastructure, built here so the GPU box
   receives them prebuilt.
@@ -108,6 +110,40 @@ def build_frontends(force: bool = False) -> None:
         os.replace(out + ".tmp", out)
 
 
+PYBIND_DIR = os.path.join(HERE, "pybind_ext")
+PYBIND_MODULES = ["tvector_pybind", "phase_pybind", "medium_pybind", "image_pybind", "scene_pybind", "photon_pybind"]
+
+
+def build_pybind(force: bool = False) -> None:
+    """The reference's six pybind11 modules (renderer/pybindFiles/*_pybind.cpp) under their own names,
+    compiled over the C ABI into simpler_b200/pybind_ext/ (put that directory on sys.path, as the
+    reference's users put its build directory there, and `import scene_pybind` works unchanged)."""
+    import sysconfig
+
+    import pybind11
+    os.makedirs(PYBIND_DIR, exist_ok=True)
+    src_dir = os.path.join(CSRC, "pybind")
+    suffix = sysconfig.get_config_var("EXT_SUFFIX") or ".so"
+    cxx = shutil.which("g++") or "g++"
+    procs = []
+    for name in PYBIND_MODULES:
+        out = os.path.join(PYBIND_DIR, name + suffix)
+        src = os.path.join(src_dir, name + ".cpp")
+        deps = [src, os.path.join(src_dir, "pybind_types.h"), os.path.join(CSRC, "host", "smp_host.h"),
+                os.path.join(ROOT, "include", "simpler_b200.h"), LIB]
+        if not force and not _stale(out, deps):
+            continue
+        cmd = [cxx, "-std=c++17", "-O2", "-shared", "-fPIC", src, "-I", pybind11.get_include(),
+               "-I", sysconfig.get_paths()["include"], "-L", HERE, "-lsimpler_b200", "-Wl,-rpath,$ORIGIN/..",
+               "-o", out + ".tmp"]
+        procs.append((name, out, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    for name, out, pr in procs:
+        o, e = pr.communicate()
+        if pr.returncode != 0:
+            raise RuntimeError(f"pybind module {name} failed to build:\n{o}\n{e}")
+        os.replace(out + ".tmp", out)
+
+
 def build_oracle() -> None:
     """Test infrastructure: the CPU checker and the reference primitives used to pin it."""
     odir = os.path.join(ROOT, "oracle")
@@ -128,6 +164,7 @@ def build_oracle() -> None:
 def build_all(verbose: bool = False, force: bool = False) -> None:
     build_library(verbose=verbose, force=force)
     build_frontends(force=force)
+    build_pybind(force=force)
     build_oracle()
 
 

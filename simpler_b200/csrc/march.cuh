@@ -379,9 +379,9 @@ __device__ __forceinline__ bool march_has_steps(const Lane &L) { return L.stop >
 // members.
 //
 // The tests are arranged for the common case, an accepted step with steps to go: the box test
-// (thresholds box_lo/box_hi, exact) and the distance test (dist_acc + cur <= dlimit) are one
-// minimum compared with 0, and the loop count and the step cap share one counter (`stop` is
-// the loop's end clamped to the cap; the cap is told apart on the rare path).
+// (thresholds box_lo/box_hi, exact) and the distance test (dist_acc + cur <= dlimit) are one chain
+// of predicate comparisons, and the loop count and the step cap share one counter (`stop` is the
+// loop's end clamped to the cap; the cap is told apart on the rare path).
 template <int FK, int FP = -1, class S>
 __device__ __forceinline__ bool march_step(S &L, const KParams &P) {
     const bool f64 = FP < 0 ? P.fp64 != 0 : FP != 0;     // FP: the path-length form, if fixed at compile time
@@ -394,9 +394,10 @@ __device__ __forceinline__ bool march_step(S &L, const KParams &P) {
     const float3 d2 = f3(fmaf(L.hh, g2.x, d.x), fmaf(L.hh, g2.y, d.y), fmaf(L.hh, g2.z, d.z));
     ++L.steps;
     const float sacc = L.dist_acc + L.cur;
-    float m = fminf(fminf(p.x - P.box_lo[0], P.box_hi[0] - p.x), fminf(p.y - P.box_lo[1], P.box_hi[1] - p.y));
-    m = fminf(m, fminf(fminf(p.z - P.box_lo[2], P.box_hi[2] - p.z), L.dlimit - sacc));
-    const bool ok = m >= 0.0f;
+    // p - L > -eps and R - p > -eps per axis (as thresholds) and dist + h <= dlimit, as one chain of
+    // predicate comparisons; a NaN coordinate fails it, as it fails the reference's test
+    const bool ok = (p.x >= P.box_lo[0]) & (p.x <= P.box_hi[0]) & (p.y >= P.box_lo[1]) & (p.y <= P.box_hi[1]) &
+                    (p.z >= P.box_lo[2]) & (p.z <= P.box_hi[2]) & (sacc <= L.dlimit);
     if (ok && L.steps < L.stop) {
         L.mp = p; L.md = d2; L.mn = n2; L.mg = g2;
         L.dist_acc = sacc;

@@ -254,7 +254,11 @@ wf_event_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
             }
             if (FK != FK_BATCH) L.tab = P.field.btab;         // a batched photon's table is set at its start
             while (st == ST_FETCH) {
-                const unsigned long long k = atomicAdd(P.counters + CNT_NEXT_PHOTON, 1ull);
+                // one atomic per group of lanes that fetch together
+                const cg::coalesced_group g = cg::coalesced_threads();
+                unsigned long long k = 0;
+                if (g.thread_rank() == 0) k = atomicAdd(P.counters + CNT_NEXT_PHOTON, (unsigned long long)g.size());
+                k = g.shfl(k, 0) + g.thread_rank();
                 if (k < (unsigned long long)P.n_photons) {
                     L.idx = P.first_photon + (long long)k;
                     L.end = 0;

@@ -1,10 +1,14 @@
-"""Drop-in Python modules for the reference's pybind11 bindings (renderer/pybindFiles/*.cpp).
+"""The Python side of the reference's pybind users.
 
-``from simpler_b200.pybind import scene_pybind, photon_pybind, ...`` replaces ``import
-scene_pybind, photon_pybind, ...``: same module, class, constructor and method names and argument
-order, with the render running on the B200 kernel through the C ABI. Scalars pass through float32
-as the reference's ``Float`` arguments do.
+The reference's six pybind11 modules (renderer/pybindFiles/{tvector,phase,medium,image,scene,
+photon}_pybind.cpp) are compiled under their own names from simpler_b200/csrc/pybind/ into
+``module_dir()``; put that directory on sys.path and ``import scene_pybind, photon_pybind, ...``
+works unchanged, rendering on the B200 kernels. ``autograd`` holds the torch.autograd.Function over
+the render and its adjoint.
 """
-from . import image_pybind, medium_pybind, phase_pybind, photon_pybind, scene_pybind, tvector_pybind
+import os
 
-__all__ = ["image_pybind", "medium_pybind", "phase_pybind", "photon_pybind", "scene_pybind", "tvector_pybind"]
+
+def module_dir() -> str:
+    """The directory holding the compiled tvector/phase/medium/image/scene/photon_pybind modules."""
+    return os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "pybind_ext")

@@ -16,6 +16,8 @@ def _ensure_built():
     """Build the native libraries if they are missing or stale (a no-op on a prebuilt tree)."""
     from simpler_b200 import build
     build.build_library()
+    build.build_frontends()
+    build.build_pybind()
     if not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):
         build.build_oracle()
 

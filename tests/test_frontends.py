@@ -8,6 +8,7 @@ import ctypes as C
 import json
 import math
 import os
+import sys
 import subprocess
 
 import numpy as np
@@ -16,7 +17,17 @@ import pytest
 import simpler_b200 as sb
 from simpler_b200 import _lib as L
 from simpler_b200 import pfm
-from simpler_b200.pybind import image_pybind, medium_pybind, phase_pybind, photon_pybind, scene_pybind, tvector_pybind
+from simpler_b200 import build as _build
+
+# the reference's modules under their own names: their directory goes on sys.path, as the reference's
+# build directory does for its users, and `import scene_pybind` is unchanged
+sys.path.insert(0, _build.PYBIND_DIR)
+import image_pybind  # noqa: E402
+import medium_pybind  # noqa: E402
+import phase_pybind  # noqa: E402
+import photon_pybind  # noqa: E402
+import scene_pybind  # noqa: E402
+import tvector_pybind  # noqa: E402
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BIN = os.path.join(ROOT, "simpler_b200", "bin")
@@ -226,17 +237,26 @@ def test_pybind_scene_descriptors(texture_file):
     setup = sb.config_plain_small(texture=tex, spatial_x=16, spatial_y=16, path_length_bins=4)
     sc = pybind_scene(path, setup)
     ref_s, ref_f = setup.scene_desc(), setup.field_desc()
+    got_s, got_f = descs(sc)
     for name in ("medium_l", "medium_r", "light_origin", "light_dir", "view_origin", "view_dir", "view_horizontal",
                  "emitter_lens_origin", "sensor_lens_origin", "pathlength_range", "light_plane", "view_plane"):
-        assert list(getattr(sc.scene_desc, name)) == [f32(v) for v in getattr(ref_s, name)], name
-    assert (sc.scene_desc.tex_x, sc.scene_desc.tex_y) == (ref_s.tex_x, ref_s.tex_y)
+        assert list(getattr(got_s, name)) == [f32(v) for v in getattr(ref_s, name)], name
+    assert (got_s.tex_x, got_s.tex_y) == (ref_s.tex_x, ref_s.tex_y)
     np.testing.assert_array_equal(sc.texture, tex)
     for name in ("type", "mode", "precision", "f_u", "speed_u", "n_o", "n_max", "n_clip", "phi_min", "phi_max",
                  "er_stepsize", "egap_end_x", "sgap_begin_x"):
-        assert getattr(sc.field_desc, name) == pytest.approx(f32(getattr(ref_f, name)), rel=1e-7), name
+        assert getattr(got_f, name) == pytest.approx(f32(getattr(ref_f, name)), rel=1e-7), name
     sc.set_n_max(5e-4)
     sc.set_f_u(1e6)
-    assert sc.field_desc.n_max == f32(5e-4) and sc.field_desc.f_u == 1e6
+    got_s, got_f = descs(sc)
+    assert got_f.n_max == f32(5e-4) and got_f.f_u == 1e6
+    assert sc.form == "rif_analytical"
+
+
+def descs(sc):
+    """The compiled Scene's C-ABI descriptors (smp_scene_desc, smp_field_desc) as ctypes structs."""
+    b_s, b_f = sc.descriptors()
+    return L.SceneDesc.from_buffer_copy(b_s), L.FieldDesc.from_buffer_copy(b_f)
 
 
 def test_pybind_scene_forms(texture_file, tmp_path):
@@ -247,6 +267,12 @@ def test_pybind_scene_forms(texture_file, tmp_path):
     assert (img.get_x_res(), img.get_y_res(), img.getZRes()) == (4, 4, 2)
     img.pixels[1, 2, 3] = 7.0
     assert img.get_pixel(3, 2, 1) == 7.0
+    view = np.asarray(img)                                # buffer protocol: the same memory, no copy
+    assert view.shape == (2, 4, 4) and view[1, 2, 3] == 7.0
+    view[0, 0, 0] = 2.5
+    assert img.get_pixel(0, 0, 0) == 2.5
+    img.writePFM3D(str(tmp_path / "img.pfm3d"))
+    np.testing.assert_array_equal(pfm.read_pfm3d(str(tmp_path / "img.pfm3d")), view)
     med = medium_pybind.Medium(100.0, 0.9, phase_pybind.henyey_greenstein(0.9))
     assert med.getSigmaT() == 100.0 and med.phase.getG() == f32(0.9)
     v = tvector_pybind.Vec3f(1.0, 2.0, 3.0)
@@ -313,5 +339,5 @@ def test_pybind_renderer_matches_render(texture_file):
     setup.medium_l = tuple(f32(v) for v in setup.medium_l)
     setup.medium_r = tuple(f32(v) for v in setup.medium_r)
     ref, _ = sb.render(setup, 20000)
-    assert ref.sum() > 0 and r.last_stats.photons == 20000
+    assert ref.sum() > 0 and r.last_stats["photons"] == 20000
     np.testing.assert_allclose(img.pixels, ref, rtol=1e-9, atol=1e-12 * ref.max())

@@ -128,43 +128,43 @@ def test_parity_large_bessel_table():
 def test_film_within_three_sigma_of_fp64_oracle_independent_streams():
     """The GPU film (Philox streams, FP32 march, FP64 film) and the FP64 oracle's film (SFMT streams,
     the reference's own generator) are independent estimates of the same image: per bin their
-    difference is Monte Carlo noise. sigma per bin comes from the spread of K GPU sub-films; the
-    oracle's variance is the same per-photon variance over its own photon count.
+    difference is Monte Carlo noise. Each side's variance per bin comes from the spread of its own K
+    sub-films (disjoint photon ranges), so a rare large splat in either film widens its own sigma.
 
-    The estimator is heavy-tailed: a connection whose sampled direction lines up with the photon's
-    own (Henyey-Greenstein g = 0.9 peaks at 190 times its mean) is a rare, large splat. A bin that
-    few photons reach is a sum of a handful of such values and not Gaussian, so the test keeps the
-    bins whose value is converged in every GPU sub-film (their spread below 25 % of their mean) and
-    prints the statistic over every bin with data beside it."""
-    shape = dict(spatial_x=12, spatial_y=12, path_length_bins=6, precision_mode=L.PREC_MIXED)
+    The medium's Henyey-Greenstein g is 0.5 here rather than the configuration's 0.9: at g = 0.9 the
+    phase function peaks at 190 times its mean, a connection that lines up with the photon's own
+    direction is a rare, very large splat, and a bin that few photons reach is not Gaussian at any
+    affordable photon count (the per-bin test then measures the tail of that distribution, not the
+    renderer). The test keeps the bins whose combined sigma is below 10 % of their value."""
+    shape = dict(spatial_x=12, spatial_y=12, path_length_bins=6, precision_mode=L.PREC_MIXED, g=0.5)
+    k_sub = 32
+
+    def spread(films):
+        films = np.stack(films)                 # each a 1/K share of the whole film
+        return films.sum(axis=0), films.var(axis=0, ddof=1) * k_sub
+
     s = sb.config_plain_small(seed=11, **shape)
-    n_g, k_sub = 3_200_000, 32
-    per = n_g // k_sub
+    n_g = 3_200_000
     plan = sb.Plan(s)
     subs = []
     for k in range(k_sub):
         plan.clear()
-        plan.trace(k * per, per, n_g)
+        plan.trace(k * (n_g // k_sub), n_g // k_sub, n_g)
         subs.append(plan.read_image())
     plan.close()
-    subs = np.stack(subs)                       # each a 1/K share of the N_g-photon film
-    film_g = subs.sum(axis=0)
-    var_g = subs.var(axis=0, ddof=1) * k_sub    # variance of the sum of K independent shares
-    n_r = 300_000
+    film_g, var_g = spread(subs)
     so = sb.config_plain_small(rng=L.RNG_SFMT, seed=0, **shape)
-    _, film_r = ob.oracle_trace(so, 0, n_r, n_r, records=False, real_bits=64)
-    sigma = np.sqrt(var_g * (1.0 + n_g / n_r))  # same per-photon variance, N_r photons
-    mean_sub = subs.mean(axis=0)
-    cv = subs.std(axis=0, ddof=1) / np.maximum(mean_sub, 1e-300)
-    converged = (mean_sub > 0) & (cv < 0.25)
-    any_data = (subs > 0).sum(axis=0) >= k_sub // 2
-    for name, sel in (("converged", converged), ("with data", any_data)):
-        z = (film_g - film_r)[sel] / sigma[sel]
-        print(f"{name}: {sel.sum()} bins, {np.mean(np.abs(z) <= 3.0) * 100:.2f} % within 3 sigma, "
-              f"mean z^2 {np.mean(z * z):.3f}")
-    print(f"film sums {film_g.sum():.6g} (GPU) {film_r.sum():.6g} (oracle)")
-    z = (film_g - film_r)[converged] / sigma[converged]
-    assert converged.sum() >= 60
-    assert np.mean(np.abs(z) <= 3.0) >= 0.99
-    assert np.mean(z * z) < 2.5
-    assert abs(film_g.sum() / film_r.sum() - 1.0) < 0.02
+    n_r = 320_000
+    per = n_r // k_sub
+    film_r, var_r = spread([ob.oracle_trace(so, k * per, per, n_r, records=False, real_bits=64)[1]
+                            for k in range(k_sub)])
+    sigma = np.sqrt(var_g + var_r)
+    sel = (film_r > 0) & (sigma < 0.1 * film_r)
+    z = (film_g - film_r)[sel] / sigma[sel]
+    inside = np.mean(np.abs(z) <= 3.0)
+    print(f"{sel.sum()} bins, {inside * 100:.2f} % within 3 sigma, mean z^2 {np.mean(z * z):.3f}, "
+          f"film sums {film_g.sum():.6g} (GPU) {film_r.sum():.6g} (oracle)")
+    assert sel.sum() >= 100
+    assert inside >= 0.99, inside
+    assert 0.6 < np.mean(z * z) < 1.6
+    assert abs(film_g.sum() / film_r.sum() - 1.0) < 0.01
