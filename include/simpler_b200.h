@@ -200,6 +200,10 @@ typedef struct smp_stats {
     int64_t march_steps;          /* er_step evaluations executed by that kernel                    */
     int64_t launches;             /* kernels launched                                               */
     int64_t march_launches;       /* of which ER-march kernel launches                              */
+    /* the slot pool's schedule of the last trace (smp_plan_tune): march-kernel block size, slots
+       per march lane, chunk (ER steps per slot per march launch; 0 while it was still being tuned
+       online), and 1 when the plan was tuned */
+    int32_t march_block, slots_per_lane, chunk, tuned;
 } smp_stats;
 
 /* ---- parity records (smp_trace_photons) ---------------------------------------------------- */
@@ -284,6 +288,23 @@ int smp_plan_film(smp_plan *plan, void **dev_ptr, int32_t *bytes_per_pixel);
 int smp_plan_stats(smp_plan *plan, smp_stats *stats_out);
 /* Whole render through a plan: clear, trace [0,n), read back to host. */
 int smp_plan_render(smp_plan *plan, int64_t n_photons, double *image_out, smp_stats *stats_out);
+
+/* Autotuner (no counterpart in the reference): times trial traces of n_sample photons (photons
+   [0, n_sample) of this plan's render) over the slot pool's march-kernel block size (128, 256),
+   resident slots per march lane (2-8) and chunk (ER steps per slot per march launch, 64-192), keeps
+   the fastest for the plan and caches it per process under the device, field kind, precision, film,
+   medium, field, scene and sample size, so a later plan of the same configuration takes it without
+   trials. The trials render into the plan's film, which is cleared on return: tune before tracing.
+   Plans that are not tuned keep their defaults and tune the chunk alone, online, while they trace. */
+typedef struct smp_tuning {
+    int32_t march_block;          /* threads per march-kernel block                                 */
+    int32_t slots_per_lane;       /* resident photon slots per march lane                           */
+    int32_t chunk;                /* ER steps per slot per march launch                             */
+    int32_t trials;               /* configurations timed (0: taken from the cache)                 */
+    double  ms;                   /* device time of the chosen configuration's trial trace          */
+    double  paths_per_s;          /* its photon paths/s                                             */
+} smp_tuning;
+int smp_plan_tune(smp_plan *plan, int64_t n_sample, smp_tuning *out);
 
 /* Parity mode: traces n_photons with per-photon injected uniforms
    (photon i consumes uniforms[offsets[i] .. offsets[i+1]) ), or with the opts->rng stream when

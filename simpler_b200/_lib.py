@@ -112,6 +112,14 @@ class Stats(C.Structure):
         ("step_cap_hits", C.c_int64), ("nan_photons", C.c_int64), ("stream_exhausted", C.c_int64),
         ("kernel_ms", C.c_double), ("march_ms", C.c_double), ("march_steps", C.c_int64),
         ("launches", C.c_int64), ("march_launches", C.c_int64),
+        ("march_block", C.c_int32), ("slots_per_lane", C.c_int32), ("chunk", C.c_int32), ("tuned", C.c_int32),
+    ]
+
+
+class Tuning(C.Structure):
+    _fields_ = [
+        ("march_block", C.c_int32), ("slots_per_lane", C.c_int32), ("chunk", C.c_int32), ("trials", C.c_int32),
+        ("ms", C.c_double), ("paths_per_s", C.c_double),
     ]
 
 
@@ -147,7 +155,7 @@ STRUCTS = {
     "smp_field_desc": FieldDesc, "smp_scene_desc": SceneDesc, "smp_medium_desc": MediumDesc,
     "smp_render_opts": RenderOpts, "smp_stats": Stats, "smp_photon_record": PhotonRecord,
     "smp_splat_record": SplatRecord, "smp_instance_desc": InstanceDesc,
-    "smp_adjoint_stats": AdjointStats,
+    "smp_adjoint_stats": AdjointStats, "smp_tuning": Tuning,
 }
 
 # every entry point declared in include/simpler_b200.h
@@ -156,7 +164,7 @@ EXPORTS = [
     "smp_plan_create", "smp_plan_destroy", "smp_plan_set_field", "smp_plan_clear", "smp_plan_trace",
     "smp_plan_read_image", "smp_plan_film", "smp_plan_stats", "smp_plan_render", "smp_trace_photons",
     "smp_field_eval", "smp_texture_cdf", "smp_spline_prefilter", "smp_render_batch", "smp_fp32_peak",
-    "smp_render_noalloc", "smp_adjoint_param_count", "smp_plan_adjoint", "smp_render_adjoint",
+    "smp_render_noalloc", "smp_adjoint_param_count", "smp_plan_adjoint", "smp_render_adjoint", "smp_plan_tune",
 ]
 
 _lib = None
@@ -202,6 +210,7 @@ def load() -> C.CDLL:
     lib.smp_fp32_peak.argtypes = [C.c_int, P(C.c_double)]
     lib.smp_render_noalloc.argtypes = [P(SceneDesc), P(MediumDesc), P(FieldDesc), P(RenderOpts), C.c_int64, C.c_int64,
                                        C.c_int64, vp, vp, P(Stats)]
+    lib.smp_plan_tune.argtypes = [vp, C.c_int64, P(Tuning)]
     lib.smp_adjoint_param_count.restype = C.c_int64
     lib.smp_adjoint_param_count.argtypes = [P(FieldDesc)]
     lib.smp_plan_adjoint.argtypes = [vp, C.c_int64, C.c_int64, C.c_int64, vp, vp, P(AdjointStats)]

@@ -35,12 +35,14 @@ NVCC_FLAGS = [
     "-fmad=false",
 ]
 
-CU_SOURCES = ["capi.cu", "adjoint_sweep.cu", "host/smp_host.cpp"]
+# the kernels are split over translation units (dispatch.h) so that they compile in parallel
+CU_SOURCES = ["capi.cu", "k_march.cu", "k_wave.cu", "k_adjoint.cu", "adjoint_sweep.cu", "host/smp_host.cpp"]
 # Per-file overrides of NVCC_FLAGS. The adjoint's backward sweep does not take part in any
 # bit-for-bit comparison (its inputs are read back from the replayed trajectories), so its
 # arithmetic may contract a*b+c into FMAs.
 FILE_FLAGS = {"adjoint_sweep.cu": ["-fmad=true"]}
-HEADERS = ["kparams.h", "dev_math.cuh", "dev_field.cuh", "march.cuh", "wavefront.cuh", "adjoint.cuh", "adjoint_sweep.cu", "host/smp_host.h"]
+HEADERS = ["kparams.h", "dispatch.h", "dev_math.cuh", "dev_field.cuh", "march.cuh", "wavefront.cuh", "plain.cuh",
+           "adjoint.cuh", "host/smp_host.h"]
 BIN = os.path.join(HERE, "bin")
 MAINS = {"renderer3d": "host/renderer3d_main.cpp", "simplER": "host/simpler_main.cpp",
          "merge_renderings": "host/merge_main.cpp"}

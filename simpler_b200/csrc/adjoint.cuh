@@ -35,6 +35,7 @@
 // The splat's value (Fresnel exit, foreshortening, Henyey-Greenstein, exp(-sigma_t d), bilinear
 // weights) and the HG frame rotation at a vertex are differentiated with forward-mode dual numbers.
 #pragma once
+#include "dispatch.h"
 #include "march.cuh"
 
 namespace smp {
@@ -1024,8 +1025,7 @@ __global__ void __launch_bounds__(128, 3) adjoint_replay_kernel(const __grid_con
 // until few lanes are left sweeping.
 enum AdjJob : int { JOB_CONN = 1, JOB_MOVE = 2, JOB_DIRECT = 3, JOB_SOURCE = 4 };
 
-typedef void (*AdjRoundFn)(KParams, AdjParams, int);
-AdjRoundFn adjoint_sweep_fn(int fk);     // adjoint_sweep.cu
+
 
 template <int FK>
 __global__ void __launch_bounds__(128, 3) adjoint_sweep_kernel(const __grid_constant__ KParams P,

@@ -13,12 +13,13 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include "kparams.h"
-#include "march.cuh"
+#include "dispatch.h"
 #include "wavefront.cuh"
 #include "plain.cuh"
 #include "adjoint.cuh"
@@ -340,76 +341,7 @@ static int check_device(int dev) {
 }
 
 // ---- kernel dispatch ---------------------------------------------------------------------------
-typedef void (*MarchFn)(KParams);
-static MarchFn march_fn(int fk) {
-    switch (fk) {
-        case FK_BESSEL0: return march_kernel<FK_BESSEL0>;
-        case FK_BESSEL1: return march_kernel<FK_BESSEL1>;
-        case FK_BESSEL2: return march_kernel<FK_BESSEL2>;
-        case FK_BESSELN: return march_kernel<FK_BESSELN>;
-        case FK_PLANEWAVE: return march_kernel<FK_PLANEWAVE>;
-        case FK_SOURCES: return march_kernel<FK_SOURCES>;
-        case FK_SPLINE: return march_kernel<FK_SPLINE>;
-        case FK_BATCH: return march_kernel<FK_BATCH>;
-        default: return nullptr;
-    }
-}
-
 static const int kBlock = 128;
-
-typedef void (*WaveFn)(KParams, WaveParams, int);
-static WaveFn wf_march_fn(int fk, bool fp64) {
-    switch (fk) {
-        case FK_BESSEL0: return fp64 ? wf_march_kernel<FK_BESSEL0, 1> : wf_march_kernel<FK_BESSEL0, 0>;
-        case FK_BESSEL1: return fp64 ? wf_march_kernel<FK_BESSEL1, 1> : wf_march_kernel<FK_BESSEL1, 0>;
-        case FK_BESSEL2: return fp64 ? wf_march_kernel<FK_BESSEL2, 1> : wf_march_kernel<FK_BESSEL2, 0>;
-        case FK_BESSELN: return fp64 ? wf_march_kernel<FK_BESSELN, 1> : wf_march_kernel<FK_BESSELN, 0>;
-        case FK_PLANEWAVE: return fp64 ? wf_march_kernel<FK_PLANEWAVE, 1> : wf_march_kernel<FK_PLANEWAVE, 0>;
-        case FK_SOURCES: return fp64 ? wf_march_kernel<FK_SOURCES, 1> : wf_march_kernel<FK_SOURCES, 0>;
-        case FK_SPLINE: return fp64 ? wf_march_kernel<FK_SPLINE, 1> : wf_march_kernel<FK_SPLINE, 0>;
-        case FK_BATCH: return fp64 ? wf_march_kernel<FK_BATCH, 1> : wf_march_kernel<FK_BATCH, 0>;
-        default: return nullptr;
-    }
-}
-static WaveFn wf_finish_fn(int fk) {
-    switch (fk) {
-        case FK_BESSEL0: return wf_finish_kernel<FK_BESSEL0>;
-        case FK_BESSEL1: return wf_finish_kernel<FK_BESSEL1>;
-        case FK_BESSEL2: return wf_finish_kernel<FK_BESSEL2>;
-        case FK_BESSELN: return wf_finish_kernel<FK_BESSELN>;
-        case FK_PLANEWAVE: return wf_finish_kernel<FK_PLANEWAVE>;
-        case FK_SOURCES: return wf_finish_kernel<FK_SOURCES>;
-        case FK_SPLINE: return wf_finish_kernel<FK_SPLINE>;
-        case FK_BATCH: return wf_finish_kernel<FK_BATCH>;
-        default: return nullptr;
-    }
-}
-static WaveFn wf_event_fn(int fk) {
-    switch (fk) {
-        case FK_BESSEL0: return wf_event_kernel<FK_BESSEL0>;
-        case FK_BESSEL1: return wf_event_kernel<FK_BESSEL1>;
-        case FK_BESSEL2: return wf_event_kernel<FK_BESSEL2>;
-        case FK_BESSELN: return wf_event_kernel<FK_BESSELN>;
-        case FK_PLANEWAVE: return wf_event_kernel<FK_PLANEWAVE>;
-        case FK_SOURCES: return wf_event_kernel<FK_SOURCES>;
-        case FK_SPLINE: return wf_event_kernel<FK_SPLINE>;
-        case FK_BATCH: return wf_event_kernel<FK_BATCH>;
-        default: return nullptr;
-    }
-}
-
-static MarchFn plain_fn(int fk) {
-    switch (fk) {
-        case FK_BESSEL0: return plain_kernel<FK_BESSEL0>;
-        case FK_BESSEL1: return plain_kernel<FK_BESSEL1>;
-        case FK_BESSEL2: return plain_kernel<FK_BESSEL2>;
-        case FK_BESSELN: return plain_kernel<FK_BESSELN>;
-        case FK_PLANEWAVE: return plain_kernel<FK_PLANEWAVE>;
-        case FK_SOURCES: return plain_kernel<FK_SOURCES>;
-        case FK_SPLINE: return plain_kernel<FK_SPLINE>;
-        default: return nullptr;
-    }
-}
 
 // Kernels that stage the Bessel table take it as dynamic shared memory; above the default 48 KB
 // window (a table for k r beyond about 96) a kernel must be opted in to the larger size first.
@@ -463,6 +395,9 @@ struct smp_plan {
     int kernel = SMP_KERNEL_POOL;   // smp_kernel (opts.kernel, or SMP_KERNEL=pool|persistent|plain)
     int wave_chunk = 96;
     int wave_slots_per_lane = 6;
+    int march_block = 128;      // threads per march-kernel block (128 or 256)
+    bool tuned = false;         // the schedule came from smp_plan_tune
+    size_t wave_cap = 0;        // slots the pool allocation holds
     int wave_batch = 16;        // march/event launch pairs between live-slot checks
     void *d_wave = nullptr;
     size_t wave_bytes = 0;
@@ -608,6 +543,7 @@ size_t smp_sizeof(const char *t) {
     if (!std::strcmp(t, "smp_splat_record")) return sizeof(smp_splat_record);
     if (!std::strcmp(t, "smp_instance_desc")) return sizeof(smp_instance_desc);
     if (!std::strcmp(t, "smp_adjoint_stats")) return sizeof(smp_adjoint_stats);
+    if (!std::strcmp(t, "smp_tuning")) return sizeof(smp_tuning);
     return 0;
 }
 
@@ -656,6 +592,7 @@ int smp_plan_create(const smp_scene_desc *scene, const smp_medium_desc *medium, 
     if (const char *c = std::getenv("SMP_WF_TUNE")) p->tune_chunk = p->tune_chunk && std::atoi(c) != 0;
     if (const char *c = std::getenv("SMP_WF_GRAPH")) p->use_graph = std::atoi(c) != 0;
     if (const char *c = std::getenv("SMP_WF_SLOTS")) p->wave_slots_per_lane = std::max(1, std::min(16, std::atoi(c)));
+    if (const char *c = std::getenv("SMP_WF_BLOCK")) p->march_block = std::atoi(c) == 256 ? 256 : 128;
     if (const char *c = std::getenv("SMP_WF_BATCH")) p->wave_batch = std::max(1, std::min(256, std::atoi(c)));
     p->scene = *scene;
     p->medium = *medium;
@@ -788,24 +725,28 @@ static float photon_weight(const smp_scene_desc &s, int64_t n) {
 // the march grid x wave_slots_per_lane), allocated at the first trace and grown if a new field
 // kind needs more.
 static int wave_setup(smp_plan *p) {
-    WaveFn fm = wf_march_fn(p->fk, p->kp.fp64 != 0), fe = wf_event_fn(p->fk), ff = wf_finish_fn(p->fk);
+    WaveFn fm = wf_march_fn(p->fk, p->kp.fp64 != 0, p->march_block), fe = wf_event_fn(p->fk), ff = wf_finish_fn(p->fk);
     if (!fm || !fe || !ff) return set_error(SMP_ERR_BAD_ARG, "bad field kind");
     int sms = 0, pm = 0, pe = 0, pf = 0;
     int rc = allow_dynamic_smem(reinterpret_cast<const void *>(fm), p->smem_bytes);
     if (!rc) rc = allow_dynamic_smem(reinterpret_cast<const void *>(ff), p->smem_bytes);
     if (rc) return rc;
     SMP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device));
-    SMP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pm, fm, kBlock, p->smem_bytes));
+    SMP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pm, fm, p->march_block, p->smem_bytes));
     SMP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pe, fe, kBlock, 0));
     SMP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, ff, kBlock, p->smem_bytes));
     p->grid_march = sms * std::max(pm, 1);
     p->grid_event = sms * std::max(pe, 1);
     p->grid_finish = sms * std::max(pf, 1);
-    const size_t n = size_t(p->grid_march) * kBlock * size_t(p->wave_slots_per_lane);
+    const size_t n = size_t(p->grid_march) * size_t(p->march_block) * size_t(p->wave_slots_per_lane);
     p->wp.chunk = p->wave_chunk;
-    if (p->d_wave && size_t(p->wp.n_slots) >= n) return SMP_OK;
+    if (p->d_wave && p->wave_cap >= n) {            // the allocation holds this many slots
+        p->wp.n_slots = int(n);
+        return SMP_OK;
+    }
     cudaFree(p->d_wave);
     p->d_wave = nullptr;
+    p->wave_cap = 0;
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t b4 = al(n * sizeof(float4)), bi = al(n * sizeof(int4)), bd = al(n * sizeof(double)),
                  be = al(n * sizeof(EventPart)), bl = al(n * sizeof(int));
@@ -816,6 +757,7 @@ static int wave_setup(smp_plan *p) {
         return set_error(e == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "slot pool (%zu bytes): %s", bytes, cudaGetErrorString(e));
     }
     p->wave_bytes = bytes;
+    p->wave_cap = n;
     char *b = static_cast<char *>(p->d_wave);
     WaveParams &W = p->wp;
     W.ma = reinterpret_cast<float4 *>(b); b += b4;
@@ -845,8 +787,9 @@ static int wave_setup(smp_plan *p) {
 static int wave_run(smp_plan *p, const KParams &k, cudaStream_t s) {
     int rc = wave_setup(p);
     if (rc) return rc;
-    WaveFn fm = wf_march_fn(p->fk, p->kp.fp64 != 0), fe = wf_event_fn(p->fk), ff = wf_finish_fn(p->fk);
+    WaveFn fm = wf_march_fn(p->fk, p->kp.fp64 != 0, p->march_block), fe = wf_event_fn(p->fk), ff = wf_finish_fn(p->fk);
     WaveParams W = p->wp;
+    const int mb = p->march_block;
     // once the live slots fit in one persistent grid, the finisher runs them to the end
     const unsigned finish_at = unsigned(p->grid_finish) * unsigned(kBlock);
     SMP_CUDA(cudaMemsetAsync(W.cnt, 0, 4 * sizeof(unsigned), s));
@@ -891,7 +834,7 @@ static int wave_run(smp_plan *p, const KParams &k, cudaStream_t s) {
                 cudaGraph_t g = nullptr;
                 SMP_CUDA(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
                 for (int j = 0; j < p->wave_batch; ++j) {
-                    fm<<<p->grid_march, kBlock, p->smem_bytes, p->cap_stream>>>(k, W, j);
+                    fm<<<p->grid_march, mb, p->smem_bytes, p->cap_stream>>>(k, W, j);
                     fe<<<p->grid_event, kBlock, 0, p->cap_stream>>>(k, W, j);
                 }
                 SMP_CUDA(cudaStreamEndCapture(p->cap_stream, &g));
@@ -905,7 +848,7 @@ static int wave_run(smp_plan *p, const KParams &k, cudaStream_t s) {
         } else {
             for (int j = 0; j < p->wave_batch; ++j, ++it) {
                 SMP_CUDA(cudaEventRecord(p->march_ev[p->march_ev_used], s));
-                fm<<<p->grid_march, kBlock, p->smem_bytes, s>>>(k, W, int(it & 0x3fffffff));
+                fm<<<p->grid_march, mb, p->smem_bytes, s>>>(k, W, int(it & 0x3fffffff));
                 SMP_CUDA(cudaEventRecord(p->march_ev[p->march_ev_used + 1], s));
                 p->march_ev_used += 2;
                 fe<<<p->grid_event, kBlock, 0, s>>>(k, W, int(it & 0x3fffffff));
@@ -1031,6 +974,10 @@ static int collect_stats(smp_plan *plan) {
     plan->stats.march_ms = one_kernel ? ms_total : march_ms;
     plan->stats.march_steps = one_kernel ? (int64_t)c[CNT_STEPS] : (int64_t)c[CNT_MARCH_STEPS];
     plan->stats.launches = plan->n_launched;
+    plan->stats.march_block = plan->march_block;
+    plan->stats.slots_per_lane = plan->wave_slots_per_lane;
+    plan->stats.chunk = plan->tuned_chunk > 0 ? plan->tuned_chunk : (plan->tune_chunk ? 0 : plan->wave_chunk);
+    plan->stats.tuned = plan->tuned ? 1 : 0;
     plan->stats.march_launches = one_kernel ? plan->n_launched
                                             : (int64_t)(plan->march_ev_used / 2) + plan->graph_march_launches;
     if (c[CNT_STAGE_TIMEOUT]) return set_error(SMP_ERR_CUDA, "%llu block(s) timed out staging the field table", c[CNT_STAGE_TIMEOUT]);
@@ -1105,6 +1052,127 @@ int smp_plan_render(smp_plan *plan, int64_t n_photons, double *image_out, smp_st
     if (stats_out) *stats_out = plan->stats;
     return rs;
 }
+
+}  // extern "C"
+
+// ---- autotuner ------------------------------------------------------------------------------------
+// Trial traces over march-kernel block size x slots per lane x chunk; the winner is kept by the plan
+// and cached per process under a key of everything that changes the march's cost. A batched sweep's
+// key is its scene, film and first instance's medium (not the instance list), so a smaller sweep of
+// the same scene run first tunes the larger one.
+namespace {
+std::mutex g_tune_mutex;
+std::map<std::string, smp_tuning> g_tune_cache;
+
+std::string tune_key(const smp_plan *p, int64_t n_sample) {
+    const KParams &k = p->kp;
+    const FieldParams &F = k.field;
+    cudaDeviceProp prop;
+    std::string dev = cudaGetDeviceProperties(&prop, p->device) == cudaSuccess ? prop.name : "?";
+    char buf[768];
+    std::snprintf(buf, sizeof(buf),
+                  "%s|%d|fk%d|fp%d|%dx%dx%d|tex%d|st%.9g|al%.9g|g%.9g|h%.9g|pr%d|amp%.9g|k%.9g|m%d|w%d|N%d,%d,%d|"
+                  "dir%d|ang%d|md%d|L%.9g,%.9g,%.9g|R%.9g,%.9g,%.9g|ni%d|n%lld",
+                  dev.c_str(), p->device, p->fk, k.fp64, k.X, k.Y, k.Z, k.n_tex, k.sigma_t, k.albedo, k.g, k.h0,
+                  k.precision, F.amp, F.k_r, F.mode, F.n_waves, F.N[0], F.N[1], F.N[2], k.use_direct, k.use_angular,
+                  k.max_depth, k.L[0], k.L[1], k.L[2], k.R[0], k.R[1], k.R[2], k.n_inst > 0 ? 1 : 0,
+                  (long long)n_sample);
+    return buf;
+}
+
+void tune_apply(smp_plan *p, const smp_tuning &t) {
+    p->tuned = true;
+    p->march_block = t.march_block;
+    p->wave_slots_per_lane = t.slots_per_lane;
+    p->wave_chunk = t.chunk;
+    p->tuned_chunk = t.chunk;
+    p->tune_chunk = false;
+}
+
+// one timed trial trace of photons [0, n) into the (cleared) film
+int tune_trial(smp_plan *p, int64_t n, int64_t weight, double *ms) {
+    int rc = smp_plan_clear(p, nullptr);
+    if (rc) return rc;
+    cudaEvent_t a, b;
+    SMP_CUDA(cudaEventCreate(&a));
+    SMP_CUDA(cudaEventCreate(&b));
+    cudaEventRecord(a, nullptr);
+    rc = launch(p, 0, n, weight, nullptr, nullptr, nullptr, nullptr);
+    cudaEventRecord(b, nullptr);
+    cudaError_t e = cudaEventSynchronize(b);
+    float f = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&f, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    if (e != cudaSuccess) return set_error(SMP_ERR_CUDA, "tuning trial: %s", cudaGetErrorString(e));
+    rc = collect_stats(p);
+    *ms = f;
+    return rc;
+}
+}  // namespace
+
+extern "C" int smp_plan_tune(smp_plan *plan, int64_t n_sample, smp_tuning *out) {
+    if (!plan || n_sample <= 0) return set_error(SMP_ERR_BAD_ARG, "bad plan / sample size");
+    if (plan->kernel != SMP_KERNEL_POOL)
+        return set_error(SMP_ERR_UNSUPPORTED, "the tuner chooses the slot pool's parameters (kernel SMP_KERNEL_POOL)");
+    SMP_CUDA(cudaSetDevice(plan->device));
+    const std::string key = tune_key(plan, n_sample);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            smp_tuning t = it->second;
+            t.trials = 0;
+            tune_apply(plan, t);
+            if (out) *out = t;
+            return smp_plan_clear(plan, nullptr);
+        }
+    }
+    // n_inst > 0 (a batched sweep): each instance carries its own weight, the argument is unused
+    const int64_t weight = n_sample;
+    static const int kSlots[4] = {8, 6, 4, 2};      // largest first: the pool is allocated once
+    static const int kChunks[4] = {64, 96, 128, 192};
+    smp_tuning best;
+    std::memset(&best, 0, sizeof(best));
+    best.ms = 1e300;
+    int trials = 0;
+    double ms = 0.0;
+    smp_tuning t;
+    std::memset(&t, 0, sizeof(t));
+    t.march_block = 128; t.slots_per_lane = kSlots[0]; t.chunk = kChunks[1];
+    tune_apply(plan, t);
+    int rc = tune_trial(plan, n_sample, weight, &ms);          // warm-up: allocations, module load
+    if (rc) return rc;
+    for (int si = 0; si < 4; ++si)
+        for (int ci = 0; ci < 4; ++ci) {
+            t.slots_per_lane = kSlots[si];
+            t.chunk = kChunks[ci];
+            tune_apply(plan, t);
+            rc = tune_trial(plan, n_sample, weight, &ms);
+            if (rc) return rc;
+            ++trials;
+            if (ms < best.ms) { best = t; best.ms = ms; }
+        }
+    t = best;
+    t.march_block = 256;
+    tune_apply(plan, t);
+    rc = tune_trial(plan, n_sample, weight, &ms);
+    if (rc) return rc;
+    ++trials;
+    if (ms < best.ms) { best = t; best.ms = ms; }
+    best.trials = trials;
+    best.paths_per_s = double(n_sample) / (best.ms * 1e-3);
+    tune_apply(plan, best);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tune_cache[key] = best;
+    }
+    if (out) *out = best;
+    return smp_plan_clear(plan, nullptr);
+}
+
+extern "C" {
 
 int smp_render(const smp_scene_desc *scene, const smp_medium_desc *medium, const smp_field_desc *field,
                const smp_render_opts *opts, int64_t n_photons, double *image_out, smp_stats *stats_out) {
@@ -1212,15 +1280,7 @@ int smp_field_eval(const smp_field_desc *field, double scaling, int64_t n_points
     if (e == cudaSuccess) {
         int blocks = int((np + 255) / 256);
         float s = float(scaling);
-        switch (fk) {
-            case FK_BESSEL0: field_probe_kernel<FK_BESSEL0><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
-            case FK_BESSEL1: field_probe_kernel<FK_BESSEL1><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
-            case FK_BESSEL2: field_probe_kernel<FK_BESSEL2><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
-            case FK_BESSELN: field_probe_kernel<FK_BESSELN><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
-            case FK_PLANEWAVE: field_probe_kernel<FK_PLANEWAVE><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
-            case FK_SOURCES: field_probe_kernel<FK_SOURCES><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
-            default: field_probe_kernel<FK_SPLINE><<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g); break;
-        }
+        field_probe_fn(fk)<<<blocks, 256>>>(F, s, n_points, d_pts, d_n, d_g);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpy(n_out, d_n, np * sizeof(double), cudaMemcpyDeviceToHost);
@@ -1368,6 +1428,19 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
         p->fk = FK_BATCH;
         p->smem_bytes = 0;
         rc = grid_for(FK_BATCH, p->device, p->opts.blocks_per_sm, 0, &p->grid);
+        // the schedule from the tuner (trials on the sweep's first photons, cached per process),
+        // and each batch of march/event launches replayed as one CUDA graph once it is fixed
+        const char *tune_env = std::getenv("SMP_TUNE");
+        if (!rc && total > 0 && p->kernel == SMP_KERNEL_POOL && !(tune_env && std::atoi(tune_env) == 0)) {
+            smp_tuning tt;
+            rc = smp_plan_tune(p, std::min<long long>(total, 2000000LL), &tt);
+            if (!rc) {
+                e = cudaMemset(d_films, 0, px * bpp * size_t(n_inst));      // the trials' photons
+                if (e != cudaSuccess) rc = set_error(SMP_ERR_CUDA, "batch films: %s", cudaGetErrorString(e));
+            }
+        }
+        const char *graph_env = std::getenv("SMP_WF_GRAPH");
+        p->use_graph = !(graph_env && std::atoi(graph_env) == 0);
         if (!rc) rc = smp_plan_clear(p, nullptr);
         // the weight argument is unused: each instance carries its own Li T / N
         if (!rc && total > 0) rc = launch(p, 0, total, 1, nullptr, nullptr, nullptr, nullptr);
@@ -1411,28 +1484,6 @@ int64_t smp_adjoint_param_count(const smp_field_desc *f) {
         return 3;
     }
     return set_error(SMP_ERR_UNSUPPORTED, "the adjoint is built for Bessel (modes 0-2), plane-wave and spline fields");
-}
-
-typedef void (*AdjFn)(KParams, AdjParams);
-static AdjFn adjoint_trace_fn(int fk) {
-    switch (fk) {
-        case FK_BESSEL0: return adjoint_trace_kernel<FK_BESSEL0>;
-        case FK_BESSEL1: return adjoint_trace_kernel<FK_BESSEL1>;
-        case FK_BESSEL2: return adjoint_trace_kernel<FK_BESSEL2>;
-        case FK_PLANEWAVE: return adjoint_trace_kernel<FK_PLANEWAVE>;
-        case FK_SPLINE: return adjoint_trace_kernel<FK_SPLINE>;
-        default: return nullptr;
-    }
-}
-static AdjRoundFn adjoint_replay_fn(int fk) {
-    switch (fk) {
-        case FK_BESSEL0: return adjoint_replay_kernel<FK_BESSEL0>;
-        case FK_BESSEL1: return adjoint_replay_kernel<FK_BESSEL1>;
-        case FK_BESSEL2: return adjoint_replay_kernel<FK_BESSEL2>;
-        case FK_PLANEWAVE: return adjoint_replay_kernel<FK_PLANEWAVE>;
-        case FK_SPLINE: return adjoint_replay_kernel<FK_SPLINE>;
-        default: return nullptr;
-    }
 }
 
 static int env_int(const char *name, int def, int lo, int hi) {

@@ -182,7 +182,17 @@ __device__ __forceinline__ void bspline_weights(float t, float w[4], float dw[4]
     dw[2] = -(1.5f * g - 2.0f) * g;
     dw[3] = 0.5f * f2;
 }
-__device__ __forceinline__ void spline_field(const FieldParams &F, float3 p, float &n, float3 &g) {
+// The march kernel of the slot pool stages one brick of the coefficient grid in shared memory (the
+// x-tap quads of kSplineBrick^3 cells and their rows' one-cell apron below and two-cell apron above
+// in y and z: kSplineBrick x (kSplineBrick + 3)^2 quads) and passes it as `brick`: entry 0 holds the
+// brick's first cell (x, y, z) as ints and a valid flag, the quads follow, x fastest. A point whose
+// 4x4x4 taps lie in the brick reads them there; any other point (and every kernel without a brick,
+// brick == nullptr) reads the global quads. The values and sums are the same either way.
+static constexpr int kSplineBrick = 16;
+static constexpr int kSplineBrickRows = kSplineBrick + 3;
+static constexpr int kSplineBrickQuads = kSplineBrick * kSplineBrickRows * kSplineBrickRows;
+
+__device__ __forceinline__ void spline_field(const FieldParams &F, const float4 *brick, float3 p, float &n, float3 &g) {
     if (p.x > F.egap || p.x < F.sgap) {
         n = F.n_o;
         g = f3(0.0f, 0.0f, 0.0f);
@@ -206,12 +216,26 @@ __device__ __forceinline__ void spline_field(const FieldParams &F, float3 p, flo
     // x-tap quads: one 16-byte load per row when floor(t_x) lies on the grid (same values, same
     // sums as the four single loads)
     const bool quad = F.coeff4 != nullptr && unsigned(bx + 1) < unsigned(N0);
+    // the staged brick holds every tap when floor(t) lies in its cells on all three axes (and on
+    // the grid)
+    const float4 *bq = nullptr;
+    if (brick != nullptr) {
+        const int4 h = *reinterpret_cast<const int4 *>(brick);
+        const int ox = bx + 1 - h.x, oy = by + 1 - h.y, oz = bz + 1 - h.z;
+        if (h.w != 0 && unsigned(ox) < unsigned(kSplineBrick) && unsigned(oy) < unsigned(kSplineBrick) &&
+            unsigned(oz) < unsigned(kSplineBrick) && unsigned(bx + 1) < unsigned(N0) && unsigned(by + 1) < unsigned(N1) &&
+            unsigned(bz + 1) < unsigned(N2))
+            bq = brick + 1 + (oz * kSplineBrickRows + oy) * kSplineBrick + ox;
+    }
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             float r0, r1, r2, r3;
-            if (quad) {
+            if (bq != nullptr) {
+                const float4 q = bq[(c * kSplineBrickRows + b) * kSplineBrick];
+                r0 = q.x; r1 = q.y; r2 = q.z; r3 = q.w;
+            } else if (quad) {
                 const float4 q = __ldg(F.coeff4 + (iz[c] + iy[b] + bx + 1));
                 r0 = q.x; r1 = q.y; r2 = q.z; r3 = q.w;
             } else {
@@ -361,9 +385,10 @@ template <> struct Field<FK_SOURCES> {
     static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *, float3 p, float, float &n, float3 &g) { sources_field(F, p, n, g); }
     static __device__ __forceinline__ void eval_ng(const FieldParams &F, const float4 *, float3 p, float, float &n, float3 &g) { sources_field(F, p, n, g); }
 };
+// the spline's `tab` argument is the staged brick of the slot pool's march kernel (or nullptr)
 template <> struct Field<FK_SPLINE> {
-    static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *, float3 p, float, float &n, float3 &g) { spline_field(F, p, n, g); }
-    static __device__ __forceinline__ void eval_ng(const FieldParams &F, const float4 *, float3 p, float, float &n, float3 &g) { spline_field(F, p, n, g); }
+    static __device__ __forceinline__ void eval(const FieldParams &F, const float4 *brick, float3 p, float, float &n, float3 &g) { spline_field(F, brick, p, n, g); }
+    static __device__ __forceinline__ void eval_ng(const FieldParams &F, const float4 *brick, float3 p, float, float &n, float3 &g) { spline_field(F, brick, p, n, g); }
 };
 
 }  // namespace smp

@@ -1,0 +1,31 @@
+// dispatch.h -- the kernels of the library, compiled in translation units of their own (k_march.cu,
+// k_wave.cu, k_adjoint.cu, adjoint_sweep.cu) so that they build in parallel, and handed to the host
+// code in capi.cu as function pointers per field kind.
+#pragma once
+#include "kparams.h"
+
+namespace smp {
+
+struct WaveParams;
+struct AdjParams;
+
+typedef void (*MarchFn)(KParams);
+typedef void (*WaveFn)(KParams, WaveParams, int);
+typedef void (*ProbeFn)(FieldParams, float, long long, const double *, double *, double *);
+typedef void (*AdjFn)(KParams, AdjParams);
+typedef void (*AdjRoundFn)(KParams, AdjParams, int);
+
+// k_march.cu
+MarchFn march_fn(int fk);                        // persistent lane loop (march.cuh)
+MarchFn plain_fn(int fk);                        // one thread per photon (plain.cuh)
+ProbeFn field_probe_fn(int fk);                  // field at host-given points
+// k_wave.cu: the slot pool (wavefront.cuh); the march kernel in blocks of 128 or 256 threads
+WaveFn wf_march_fn(int fk, bool fp64, int block);
+WaveFn wf_event_fn(int fk);
+WaveFn wf_finish_fn(int fk);
+// k_adjoint.cu, adjoint_sweep.cu
+AdjFn adjoint_trace_fn(int fk);
+AdjRoundFn adjoint_replay_fn(int fk);
+AdjRoundFn adjoint_sweep_fn(int fk);
+
+}  // namespace smp

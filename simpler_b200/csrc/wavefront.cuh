@@ -148,12 +148,13 @@ __device__ __forceinline__ void warp_append(int *arr, unsigned *cnt, unsigned ma
     if (mask & (1u << lane)) arr[base + unsigned(__popc(mask & ((1u << lane) - 1u)))] = v;
 }
 
-// March launch `it`: slots on list[it & 1] advance up to `chunk` ER steps each. When fewer slots
+// March launch `it` (BLOCK threads per block, a choice of the plan's tuner): slots on list[it & 1]
+// advance up to `chunk` ER steps each. When fewer slots
 // are live than the grid has lanes, the chunk grows in proportion (up to 64x) so the last photons
 // are not paced by launch latency. F64: the FP64 path-length form (only its accumulator is
 // loaded, carried and stored).
-template <int FK, int F64>
-__global__ void __launch_bounds__(128, FK == FK_SPLINE ? 4 : SMP_WF_MARCH_MIN_BLOCKS)
+template <int FK, int F64, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, (FK == FK_SPLINE ? 4 : SMP_WF_MARCH_MIN_BLOCKS) * 128 / BLOCK)
 wf_march_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveParams W, int it) {
     extern __shared__ __align__(16) float4 smem_tab[];
     const int lane = threadIdx.x & 31, cur = it & 1, nxt = cur ^ 1;

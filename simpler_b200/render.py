@@ -86,6 +86,13 @@ class Plan:
         L.check(self.lib.smp_plan_adjoint(self.handle, int(first), n, w, _ptr(g), _ptr(grad), C.byref(st)))
         return grad, st
 
+    def tune(self, n_sample: int) -> L.Tuning:
+        """Autotune the slot pool (march-kernel block size, slots per lane, chunk) with trial traces of
+        n_sample photons; cached per process for the same configuration. Clears the film."""
+        t = L.Tuning()
+        L.check(self.lib.smp_plan_tune(self.handle, int(n_sample), C.byref(t)))
+        return t
+
     def set_field(self, setup: Setup) -> None:
         fd = setup.field_desc()
         L.check(self.lib.smp_plan_set_field(self.handle, C.byref(fd)))
