@@ -102,7 +102,7 @@ class RenderOpts(C.Structure):
         ("step_cap", C.c_int64),
         ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32),
         ("sensor_march_max", C.c_double),
-        ("kernel", C.c_int32), ("_pad0", C.c_int32),
+        ("kernel", C.c_int32), ("spline_bricks", C.c_int32),
     ]
 
 

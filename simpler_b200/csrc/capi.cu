@@ -5,6 +5,8 @@
 // photon, and copies a float film back. Here a plan uploads the scene once (texture CDF, source
 // table, spline coefficients, film) and each render runs asynchronously on the caller's stream (the
 // slot-pool march of wavefront.cuh by default), so renders of one plan can be queued back to back.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -139,6 +141,37 @@ static void spline_quads(const int N[3], const std::vector<float> &delta, std::v
             quads[r * N[0] + x] = make_float4(row[spline_mirror(x - 1, N[0])], row[x], row[spline_mirror(x + 1, N[0])],
                                               row[spline_mirror(x + 2, N[0])]);
         }
+}
+
+// The quads again with their rows padded for the brick march kernel (dev_field.cuh kSplineBrick): row
+// (y', z') of the padded array is grid row (y' - 1, z' - 1) under the mirror rule, y' in [0, N1 + 3),
+// z' in [0, N2 + 3) -- every row a tap of an on-grid point can need.
+static void spline_quads_padded(const int N[3], const std::vector<float> &delta, std::vector<float4> &quads) {
+    const int ny = N[1] + 3, nz = N[2] + 3;
+    quads.resize(size_t(N[0]) * ny * nz);
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y) {
+            const float *row = delta.data() + (size_t(spline_mirror(z - 1, N[2])) * N[1] + spline_mirror(y - 1, N[1])) * N[0];
+            float4 *out = quads.data() + (size_t(z) * ny + y) * N[0];
+            for (int x = 0; x < N[0]; ++x)
+                out[x] = make_float4(row[spline_mirror(x - 1, N[0])], row[x], row[spline_mirror(x + 1, N[0])],
+                                     row[spline_mirror(x + 2, N[0])]);
+        }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against the driver library)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }
+    return fn;
 }
 
 // Spline coefficients as float offsets from their mean (see spline_field in dev_field.cuh).
@@ -385,6 +418,14 @@ struct smp_plan {
     float4 *d_coeff4 = nullptr;
     float4 *d_btab = nullptr;
     size_t smem_bytes = 0;
+    // spline bricks (wavefront.cuh wf_march_spline_kernel): padded quads, their TMA map, brick counts
+    bool bricks = false;        // smp_render_opts.spline_bricks (spline fields)
+    float4 *d_bquads = nullptr;
+    CUtensorMap bmap;
+    int nb = 0, nbx = 0, nby = 0, nbz = 0, bdim[3] = {0, 0, 0};
+    void *d_blist = nullptr;    // two parities of nb brick lists (wave_setup) and their counts
+    size_t blist_cap = 0;       // slots per brick list
+    size_t march_smem = 0;      // dynamic shared memory of the pool's march kernel
     int event_batch = 8;
     void *d_film = nullptr;
     size_t film_elems = 0;
@@ -439,6 +480,8 @@ static void plan_free(smp_plan *p) {
     cudaFree(p->d_centers);
     cudaFree(p->d_coeff);
     cudaFree(p->d_coeff4);
+    cudaFree(p->d_bquads);
+    cudaFree(p->d_blist);
     cudaFree(p->d_btab);
     cudaFree(p->d_film);
     cudaFree(p->d_counters);
@@ -499,6 +542,36 @@ static int plan_setup_field(smp_plan *p, const smp_field_desc &f) {
         SMP_CUDA(cudaMalloc(&p->d_coeff4, quads.size() * sizeof(float4)));
         SMP_CUDA(cudaMemcpy(p->d_coeff4, quads.data(), quads.size() * sizeof(float4), cudaMemcpyHostToDevice));
         p->kp.field.coeff4 = p->d_coeff4;
+        // bricks for the slot pool's march kernel (opts.spline_bricks): the padded quads and a tiled
+        // TMA map over them
+        const int nbx = (f.grid_n[0] + kSplineBrick - 1) / kSplineBrick, nby = (f.grid_n[1] + kSplineBrick - 1) / kSplineBrick,
+                  nbz = (f.grid_n[2] + kSplineBrick - 1) / kSplineBrick;
+        p->bricks = p->opts.spline_bricks != 0;
+        if (p->bricks && nbx * nby * nbz > kMaxBricks)
+            return set_error(SMP_ERR_UNSUPPORTED, "spline bricks: the grid has %d bricks of %d^3 cells, at most %d are built",
+                             nbx * nby * nbz, kSplineBrick, kMaxBricks);
+        if (p->bricks && tensor_map_encoder() == nullptr)
+            return set_error(SMP_ERR_CUDA, "spline bricks: cuTensorMapEncodeTiled is not available from the driver");
+        cudaFree(p->d_bquads);
+        p->d_bquads = nullptr;
+        if (p->bricks) {
+            std::vector<float4> pq;
+            spline_quads_padded(f.grid_n, delta, pq);
+            SMP_CUDA(cudaMalloc(&p->d_bquads, pq.size() * sizeof(float4)));
+            SMP_CUDA(cudaMemcpy(p->d_bquads, pq.data(), pq.size() * sizeof(float4), cudaMemcpyHostToDevice));
+            p->nbx = nbx; p->nby = nby; p->nbz = nbz; p->nb = nbx * nby * nbz;
+            p->bdim[0] = f.grid_n[0]; p->bdim[1] = f.grid_n[1] + 3; p->bdim[2] = f.grid_n[2] + 3;
+            const cuuint64_t dims[4] = {4, cuuint64_t(p->bdim[0]), cuuint64_t(p->bdim[1]), cuuint64_t(p->bdim[2])};
+            const cuuint64_t strides[3] = {16, 16ull * p->bdim[0], 16ull * p->bdim[0] * p->bdim[1]};
+            const cuuint32_t box[4] = {4, cuuint32_t(kSplineBrick), cuuint32_t(kSplineBrickRows), cuuint32_t(kSplineBrickRows)};
+            const cuuint32_t estr[4] = {1, 1, 1, 1};
+            CUresult r = tensor_map_encoder()(&p->bmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, p->d_bquads, dims, strides, box,
+                                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return set_error(SMP_ERR_CUDA, "cuTensorMapEncodeTiled (spline bricks) failed: %d", int(r));
+        }
+    } else {
+        p->bricks = false;
     }
     p->smem_bytes = 0;
     if (p->fk <= FK_BESSELN) {
@@ -724,15 +797,20 @@ static float photon_weight(const smp_scene_desc &s, int64_t n) {
 // Grid sizes from occupancy for the plan's current field kind, and the slot pool (slots = lanes of
 // the march grid x wave_slots_per_lane), allocated at the first trace and grown if a new field
 // kind needs more.
+static int wave_bricks(smp_plan *p);
+
 static int wave_setup(smp_plan *p) {
-    WaveFn fm = wf_march_fn(p->fk, p->kp.fp64 != 0, p->march_block), fe = wf_event_fn(p->fk), ff = wf_finish_fn(p->fk);
+    const bool bricks = p->fk == FK_SPLINE && p->bricks;
+    WaveFn fm = wf_march_fn(p->fk, p->kp.fp64 != 0, p->march_block, bricks), fe = wf_event_fn(p->fk),
+           ff = wf_finish_fn(p->fk);
     if (!fm || !fe || !ff) return set_error(SMP_ERR_BAD_ARG, "bad field kind");
+    p->march_smem = bricks ? size_t(kBrickSmemBytes) : p->smem_bytes;
     int sms = 0, pm = 0, pe = 0, pf = 0;
-    int rc = allow_dynamic_smem(reinterpret_cast<const void *>(fm), p->smem_bytes);
+    int rc = allow_dynamic_smem(reinterpret_cast<const void *>(fm), p->march_smem);
     if (!rc) rc = allow_dynamic_smem(reinterpret_cast<const void *>(ff), p->smem_bytes);
     if (rc) return rc;
     SMP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device));
-    SMP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pm, fm, p->march_block, p->smem_bytes));
+    SMP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pm, fm, p->march_block, p->march_smem));
     SMP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pe, fe, kBlock, 0));
     SMP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, ff, kBlock, p->smem_bytes));
     p->grid_march = sms * std::max(pm, 1);
@@ -742,7 +820,7 @@ static int wave_setup(smp_plan *p) {
     p->wp.chunk = p->wave_chunk;
     if (p->d_wave && p->wave_cap >= n) {            // the allocation holds this many slots
         p->wp.n_slots = int(n);
-        return SMP_OK;
+        return wave_bricks(p);
     }
     cudaFree(p->d_wave);
     p->d_wave = nullptr;
@@ -778,6 +856,39 @@ static int wave_setup(smp_plan *p) {
         if (!p->live_ev[i]) SMP_CUDA(cudaEventCreateWithFlags(&p->live_ev[i], cudaEventDisableTiming));
         for (int j = 0; j < 2; ++j) if (!p->batch_ev[i][j]) SMP_CUDA(cudaEventCreate(&p->batch_ev[i][j]));
     }
+    return wave_bricks(p);
+}
+
+// The brick lists of a spline plan (two parities of nb lists of up to n_slots slot indices, and
+// their counts), grown with the pool; the brick fields of the WaveParams.
+static int wave_bricks(smp_plan *p) {
+    WaveParams &W = p->wp;
+    W.nb = 0;
+    if (!(p->bricks && p->fk == FK_SPLINE)) return SMP_OK;
+    const size_t n = size_t(W.n_slots), nb = size_t(p->nb);
+    if (!p->d_blist || p->blist_cap < n) {
+        cudaFree(p->d_blist);
+        p->d_blist = nullptr;
+        p->blist_cap = 0;
+        const size_t bytes = 2 * nb * n * sizeof(int) + 2 * nb * sizeof(unsigned) + 256;
+        cudaError_t e = cudaMalloc(&p->d_blist, bytes);
+        if (e != cudaSuccess) {
+            p->d_blist = nullptr;
+            return set_error(e == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "spline brick lists (%zu bytes): %s",
+                             bytes, cudaGetErrorString(e));
+        }
+        p->blist_cap = n;
+    }
+    int *lists = static_cast<int *>(p->d_blist);
+    W.blist[0] = lists;
+    W.blist[1] = lists + nb * p->blist_cap;
+    W.bcnt[0] = reinterpret_cast<unsigned *>(lists + 2 * nb * p->blist_cap);
+    W.bcnt[1] = W.bcnt[0] + nb;
+    W.bstride = int(p->blist_cap);
+    W.nb = p->nb; W.nbx = p->nbx; W.nby = p->nby; W.nbz = p->nbz;
+    W.bquads = p->d_bquads;
+    for (int i = 0; i < 3; ++i) W.bdim[i] = p->bdim[i];
+    W.bmap = p->bmap;
     return SMP_OK;
 }
 
@@ -787,9 +898,11 @@ static int wave_setup(smp_plan *p) {
 static int wave_run(smp_plan *p, const KParams &k, cudaStream_t s) {
     int rc = wave_setup(p);
     if (rc) return rc;
-    WaveFn fm = wf_march_fn(p->fk, p->kp.fp64 != 0, p->march_block), fe = wf_event_fn(p->fk), ff = wf_finish_fn(p->fk);
+    WaveFn fm = wf_march_fn(p->fk, p->kp.fp64 != 0, p->march_block, p->wp.nb > 0), fe = wf_event_fn(p->fk),
+           ff = wf_finish_fn(p->fk);
     WaveParams W = p->wp;
     const int mb = p->march_block;
+    if (W.nb > 0) SMP_CUDA(cudaMemsetAsync(W.bcnt[0], 0, 2 * size_t(W.nb) * sizeof(unsigned), s));
     // once the live slots fit in one persistent grid, the finisher runs them to the end
     const unsigned finish_at = unsigned(p->grid_finish) * unsigned(kBlock);
     SMP_CUDA(cudaMemsetAsync(W.cnt, 0, 4 * sizeof(unsigned), s));
@@ -834,7 +947,7 @@ static int wave_run(smp_plan *p, const KParams &k, cudaStream_t s) {
                 cudaGraph_t g = nullptr;
                 SMP_CUDA(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
                 for (int j = 0; j < p->wave_batch; ++j) {
-                    fm<<<p->grid_march, mb, p->smem_bytes, p->cap_stream>>>(k, W, j);
+                    fm<<<p->grid_march, mb, p->march_smem, p->cap_stream>>>(k, W, j);
                     fe<<<p->grid_event, kBlock, 0, p->cap_stream>>>(k, W, j);
                 }
                 SMP_CUDA(cudaStreamEndCapture(p->cap_stream, &g));
@@ -848,7 +961,7 @@ static int wave_run(smp_plan *p, const KParams &k, cudaStream_t s) {
         } else {
             for (int j = 0; j < p->wave_batch; ++j, ++it) {
                 SMP_CUDA(cudaEventRecord(p->march_ev[p->march_ev_used], s));
-                fm<<<p->grid_march, mb, p->smem_bytes, s>>>(k, W, int(it & 0x3fffffff));
+                fm<<<p->grid_march, mb, p->march_smem, s>>>(k, W, int(it & 0x3fffffff));
                 SMP_CUDA(cudaEventRecord(p->march_ev[p->march_ev_used + 1], s));
                 p->march_ev_used += 2;
                 fe<<<p->grid_event, kBlock, 0, s>>>(k, W, int(it & 0x3fffffff));
@@ -1144,6 +1257,8 @@ extern "C" int smp_plan_tune(smp_plan *plan, int64_t n_sample, smp_tuning *out) 
     tune_apply(plan, t);
     int rc = tune_trial(plan, n_sample, weight, &ms);          // warm-up: allocations, module load
     if (rc) return rc;
+    // keep each trial near 150 ms: a sample that takes longer is scaled down (not below 1e5 photons)
+    if (ms > 150.0) n_sample = std::max<int64_t>(std::min<int64_t>(n_sample, 100000), int64_t(double(n_sample) * 150.0 / ms));
     for (int si = 0; si < 4; ++si)
         for (int ci = 0; ci < 4; ++ci) {
             t.slots_per_lane = kSlots[si];

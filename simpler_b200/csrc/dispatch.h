@@ -19,8 +19,9 @@ typedef void (*AdjRoundFn)(KParams, AdjParams, int);
 MarchFn march_fn(int fk);                        // persistent lane loop (march.cuh)
 MarchFn plain_fn(int fk);                        // one thread per photon (plain.cuh)
 ProbeFn field_probe_fn(int fk);                  // field at host-given points
-// k_wave.cu: the slot pool (wavefront.cuh); the march kernel in blocks of 128 or 256 threads
-WaveFn wf_march_fn(int fk, bool fp64, int block);
+// k_wave.cu: the slot pool (wavefront.cuh); the march kernel in blocks of 128 or 256 threads; for a
+// spline plan with TMA-staged coefficient bricks (smp_render_opts.spline_bricks) the brick kernel
+WaveFn wf_march_fn(int fk, bool fp64, int block, bool bricks);
 WaveFn wf_event_fn(int fk);
 WaveFn wf_finish_fn(int fk);
 // k_adjoint.cu, adjoint_sweep.cu

@@ -22,7 +22,11 @@ static WaveFn wf_march_fn_b(int fk, bool fp64) {
     }
 }
 
-WaveFn wf_march_fn(int fk, bool fp64, int block) {
+WaveFn wf_march_fn(int fk, bool fp64, int block, bool bricks) {
+    if (fk == FK_SPLINE && bricks) {
+        if (block == 256) return fp64 ? wf_march_spline_kernel<1, 256> : wf_march_spline_kernel<0, 256>;
+        return fp64 ? wf_march_spline_kernel<1, 128> : wf_march_spline_kernel<0, 128>;
+    }
     return block == 256 ? wf_march_fn_b<256>(fk, fp64) : wf_march_fn_b<128>(fk, fp64);
 }
 

@@ -22,6 +22,8 @@
 // extra launch is needed. Per-photon arithmetic is the same code as the persistent kernel
 // (march_step, run_events), so every photon's result is identical.
 #pragma once
+#include <cuda.h>
+
 #include "march.cuh"
 
 namespace smp {
@@ -82,7 +84,59 @@ struct WaveParams {
     unsigned *cnt;     // cnt[0..1] march-list lengths, cnt[2..3] event-queue lengths
     int n_slots;
     int chunk;         // ER steps per slot per march launch (grows when few slots are live)
+    // Spline bricks (FK_SPLINE; nb == 0 without them): the march lists binned by the brick of
+    // kSplineBrick^3 grid cells each slot's march position lies in -- per parity, brick b's list is
+    // blist[par][b * n_slots ...] with bcnt[par][b] entries (cnt[par] still counts them all) -- so a
+    // block of the march kernel marches one brick's slots with that brick's coefficients staged in
+    // shared memory.
+    int *blist[2];
+    unsigned *bcnt[2];
+    int nb, nbx, nby, nbz;
+    int bstride;               // capacity of one brick's list (>= n_slots)
+    const float4 *bquads;      // the x-tap quads with their y and z rows padded by -1 .. +2 (mirrored):
+                               // N0 x (N1 + 3) x (N2 + 3), the fallback copy's source
+    int bdim[3];               // N0, N1 + 3, N2 + 3
+    CUtensorMap bmap;          // tiled TMA map of bquads as floats {4, N0, N1 + 3, N2 + 3}, box
+                               // {4, kSplineBrick, kSplineBrickRows, kSplineBrickRows}
 };
+
+// the brick (cells kSplineBrick b .. kSplineBrick b + kSplineBrick - 1 per axis) a march position lies
+// in, clamped to the grid
+__device__ __forceinline__ int spline_brick_of(const FieldParams &F, const WaveParams &W, float3 p) {
+    const float t[3] = {(p.x - F.xmin[0]) * F.xres[0], (p.y - F.xmin[1]) * F.xres[1], (p.z - F.xmin[2]) * F.xres[2]};
+    const int nbs[3] = {W.nbx, W.nby, W.nbz};
+    int b[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float c = fminf(fmaxf(floorf(t[a]), 0.0f), float(F.N[a] - 1));    // NaN -> 0
+        b[a] = min(int(c) / kSplineBrick, nbs[a] - 1);
+    }
+    return (b[2] * W.nby + b[1]) * W.nbx + b[0];
+}
+
+// Appends `slot` of every lane in `mask` to the list of its brick (parity par) and counts them in
+// cnt[par]: one atomic per warp for the count and one per group of lanes of the same brick. All 32
+// lanes call it.
+__device__ __forceinline__ void brick_append(const WaveParams &W, int par, unsigned mask, int brick, int slot, int lane) {
+    if (mask == 0u) return;
+    if (lane == __ffs(mask) - 1) atomicAdd(W.cnt + par, unsigned(__popc(mask)));
+    if (mask & (1u << lane)) {
+        const unsigned same = __match_any_sync(mask, brick);
+        const int leader = __ffs(same) - 1;
+        unsigned base = 0u;
+        if (lane == leader) base = atomicAdd(W.bcnt[par] + brick, unsigned(__popc(same)));
+        base = __shfl_sync(same, base, leader);
+        W.blist[par][size_t(brick) * size_t(W.bstride) + base + unsigned(__popc(same & ((1u << lane) - 1u)))] = slot;
+    }
+}
+
+// live march slot number i of parity par, counted across the brick lists in brick order
+__device__ __forceinline__ int brick_slot(const WaveParams &W, int par, unsigned i) {
+    int b = 0;
+    unsigned acc = 0u;
+    while (b < W.nb - 1 && acc + W.bcnt[par][b] <= i) acc += W.bcnt[par][b++];
+    return W.blist[par][size_t(b) * size_t(W.bstride) + (i - acc)];
+}
 
 __device__ __forceinline__ void wf_load_march(const WaveParams &W, const KParams &P, int slot, MarchState &M) {
     const float4 a = W.ma[slot], b = W.mb[slot], c = W.mc[slot], d = W.mdd[slot];
@@ -194,7 +248,7 @@ wf_march_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
                 M.inst = P.insts + __float_as_int(d.w);
                 M.tab = M.inst->field.btab;
             } else {
-                M.tab = smem_tab;
+                M.tab = FK == FK_SPLINE ? nullptr : smem_tab;   // no staged brick: global quads
             }
             const int steps0 = M.steps;
             for (int k = 0; k < chunk; k += 2) {
@@ -219,6 +273,154 @@ wf_march_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
     if (lane == 0 && wd) atomicAdd(P.counters + CNT_MARCH_STEPS, wd);
 }
 
+// ---- the spline's march kernel with TMA-staged coefficient bricks ------------------------------
+// Dynamic shared memory of the brick march kernel: alignment slack, the 16-byte header, the quads.
+static constexpr unsigned kBrickSmemBytes = 256u + 16u * unsigned(kSplineBrickQuads);
+static constexpr int kMaxBricks = 1024;
+
+// Stages brick (bx, by, bz) of the padded quads into shared memory with one tiled tensor copy
+// (cp.async.bulk.tensor.4d, no multicast; the tensor map covers this GPU's memory only) on a
+// bounded mbarrier wait. The block's thread 0 issues the copy; `phase` is the barrier's next
+// parity. On a timeout the block waits once more (bounded), records the failure and returns false,
+// and the caller copies with plain loads; after a failure it stops using the copy engine (use_tma).
+__device__ __forceinline__ bool stage_brick_tma(float4 *dst, const WaveParams &W, int bx, int by, int bz,
+                                                unsigned bar, unsigned &phase, bool &use_tma,
+                                                unsigned long long *err) {
+    if (!use_tma) return false;
+    const unsigned bytes = 16u * unsigned(kSplineBrickQuads);
+    if (threadIdx.x == 0) {
+        // the block's earlier reads of this memory (generic proxy) come before the copy's writes
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+            ::"r"(smem_u32(dst)), "l"(reinterpret_cast<unsigned long long>(&W.bmap)), "r"(0), "r"(kSplineBrick * bx),
+              "r"(kSplineBrick * by), "r"(kSplineBrick * bz), "r"(bar)
+            : "memory");
+    }
+    bool ok = mbar_wait_bounded(bar, phase, 1 << 22);
+    if (!ok) {
+        ok = mbar_wait_bounded(bar, phase, 1 << 22);       // the copy may still land: wait for it once more
+        if (threadIdx.x == 0) atomicAdd(err, 1ull);
+    }
+    ok = __syncthreads_and(ok ? 1 : 0) != 0;
+    if (ok) phase ^= 1u;
+    else use_tma = false;
+    return ok;
+}
+
+// The brick with plain loads (the TMA copy's fallback), zero outside the padded grid as the tensor
+// copy fills it.
+__device__ __forceinline__ void stage_brick_loads(float4 *dst, const WaveParams &W, int bx, int by, int bz) {
+    for (int i = threadIdx.x; i < kSplineBrickQuads; i += blockDim.x) {
+        const int x = i % kSplineBrick, y = (i / kSplineBrick) % kSplineBrickRows, z = i / (kSplineBrick * kSplineBrickRows);
+        const int gx = kSplineBrick * bx + x, gy = kSplineBrick * by + y, gz = kSplineBrick * bz + z;
+        float4 q = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (gx < W.bdim[0] && gy < W.bdim[1] && gz < W.bdim[2])
+            q = W.bquads[(size_t(gz) * W.bdim[1] + gy) * W.bdim[0] + gx];
+        dst[i] = q;
+    }
+}
+
+// March launch `it` of a spline plan with bricks. The list of parity it & 1 is binned by brick; the
+// kernel walks it in groups of BLOCK slots of one brick (grid-stride over the groups of all bricks,
+// in brick order), stages each new brick's coefficients with the Tensor Memory Accelerator, and
+// marches the group's slots as wf_march_kernel does, their spline evaluations reading the brick in
+// shared memory (a point whose taps leave the brick reads the global quads). Slots whose march
+// continues are binned by the brick they now lie in.
+template <int F64, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 256 / BLOCK)
+wf_march_spline_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveParams W, int it) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ unsigned s_pref[kMaxBricks + 1];
+    __shared__ __align__(8) unsigned long long s_bar;
+    const int lane = threadIdx.x & 31, cur = it & 1, nxt = cur ^ 1;
+    const unsigned n = W.cnt[cur];
+    if (n == 0u) return;
+    // the brick: quads 128-byte aligned, the header in the 16 bytes before them
+    float4 *quads = reinterpret_cast<float4 *>((reinterpret_cast<uintptr_t>(smem_raw) + 16u + 127u) & ~uintptr_t(127));
+    float4 *brick = quads - 1;
+    const unsigned bar = smem_u32(&s_bar);
+    if (threadIdx.x == 0) {
+        unsigned acc = 0u;
+        s_pref[0] = 0u;
+        for (int b = 0; b < W.nb; ++b) {
+            acc += (W.bcnt[cur][b] + unsigned(BLOCK) - 1u) / unsigned(BLOCK);
+            s_pref[b + 1] = acc;
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const unsigned groups = s_pref[W.nb];
+    const unsigned lanes = gridDim.x * blockDim.x;
+    const int chunk = W.chunk * int(min(64u, max(1u, lanes / n)));
+    unsigned phase = 0u;
+    bool use_tma = true;
+    int staged = -1;
+    unsigned done = 0;                               // ER steps this lane executed
+    for (unsigned g = blockIdx.x; g < groups; g += gridDim.x) {
+        // the brick of group g: the last b with s_pref[b] <= g (empty bricks have no groups)
+        int lo = 0, hi = W.nb;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_pref[mid] <= g) lo = mid; else hi = mid;
+        }
+        const int b = lo;
+        if (b != staged) {
+            __syncthreads();                         // every lane is done with the previous brick
+            const int bx = b % W.nbx, by = (b / W.nbx) % W.nby, bz = b / (W.nbx * W.nby);
+            if (!stage_brick_tma(quads, W, bx, by, bz, bar, phase, use_tma, P.counters + CNT_STAGE_TIMEOUT)) {
+                stage_brick_loads(quads, W, bx, by, bz);
+            }
+            if (threadIdx.x == 0)
+                *reinterpret_cast<int4 *>(brick) = make_int4(kSplineBrick * bx, kSplineBrick * by, kSplineBrick * bz, 1);
+            __syncthreads();
+            staged = b;
+        }
+        const unsigned i = (g - s_pref[b]) * unsigned(BLOCK) + threadIdx.x;
+        const bool valid = i < W.bcnt[cur][b];
+        bool ended = false;
+        int slot = 0, key = 0;
+        if (valid) {
+            slot = W.blist[cur][size_t(b) * size_t(W.bstride) + i];
+            MarchState M;
+            const float4 a = W.ma[slot], bb = W.mb[slot], c = W.mc[slot], d = W.mdd[slot];
+            const int4 e = W.mi[slot];
+            M.mp = f3(a.x, a.y, a.z); M.mn = a.w;
+            M.md = f3(bb.x, bb.y, bb.z); M.cur = bb.w;
+            M.mg = f3(c.x, c.y, c.z); M.dist_acc = c.w;
+            M.dlimit = d.x; M.s = d.y; M.mtotf = d.z;
+            M.steps = e.x; M.end = 0; M.prec = e.z; M.stop = e.w;   // a marching slot has no end code
+            M.hh = 0.5f * M.cur;
+            M.cur_d = double(M.cur);
+            M.mtot = F64 ? W.mt[slot] : 0.0;
+            M.tab = brick;
+            M.inst = nullptr;
+            const int steps0 = M.steps;
+            for (int k = 0; k < chunk; k += 2) {
+                if (march_step<FK_SPLINE, F64>(M, P) || march_step<FK_SPLINE, F64>(M, P)) { ended = true; break; }
+            }
+            done += unsigned(M.steps - steps0);
+            W.ma[slot] = make_float4(M.mp.x, M.mp.y, M.mp.z, M.mn);
+            W.mb[slot] = make_float4(M.md.x, M.md.y, M.md.z, M.cur);
+            W.mc[slot] = make_float4(M.mg.x, M.mg.y, M.mg.z, M.dist_acc);
+            if (F64) W.mt[slot] = M.mtot;
+            else W.mdd[slot] = make_float4(M.dlimit, M.s, M.mtotf, d.w);
+            W.mi[slot] = make_int4(M.steps, M.end, M.prec, M.stop);
+            if (!ended) key = spline_brick_of(P.field, W, M.mp);
+        }
+        const unsigned em = __ballot_sync(kFull, valid && ended);
+        const unsigned cm = __ballot_sync(kFull, valid && !ended);
+        warp_append(W.queue[cur], W.cnt + 2 + cur, em, slot, lane);
+        brick_append(W, nxt, cm, key, slot, lane);
+    }
+    unsigned long long wd = done;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wd += __shfl_down_sync(kFull, wd, o);
+    if (lane == 0 && wd) atomicAdd(P.counters + CNT_MARCH_STEPS, wd);
+}
+
 // Event launch `it` (or the initial fill when it < 0): queued slots run their discrete logic;
 // finished photons are replaced from the global photon counter; slots that start a march are
 // appended to the next march list. Also resets the march-list counter just consumed and the event
@@ -234,12 +436,14 @@ wf_event_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
         W.cnt[cur] = 0u;          // consumed by march launch `it`
         W.cnt[2 + nxt] = 0u;      // filled by march launch `it + 1`
     }
+    if (FK == FK_SPLINE && !init && blockIdx.x == 0)
+        for (int b = threadIdx.x; b < W.nb; b += blockDim.x) W.bcnt[cur][b] = 0u;   // the brick lists too
     LaneStats S;
     const unsigned lanes = gridDim.x * blockDim.x, nwarps = lanes >> 5;
     for (unsigned base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; base < n; base += nwarps * 32u) {
         const unsigned i = base + unsigned(lane);
         const bool valid = i < n;
-        int st = ST_DONE, slot = 0;
+        int st = ST_DONE, slot = 0, key = 0;
         if (valid) {
             slot = init ? int(i) : W.queue[cur][i];
             Lane L;
@@ -269,10 +473,14 @@ wf_event_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
                     st = ST_DONE;
                 }
             }
-            if (st == ST_MARCH) wf_store_lane(W, P, slot, L);
+            if (st == ST_MARCH) {
+                wf_store_lane(W, P, slot, L);
+                if (FK == FK_SPLINE && W.nb) key = spline_brick_of(P.field, W, L.mp);
+            }
         }
         const unsigned mm = __ballot_sync(kFull, valid && st == ST_MARCH);
-        warp_append(W.list[nxt], W.cnt + nxt, mm, slot, lane);
+        if (FK == FK_SPLINE && W.nb) brick_append(W, nxt, mm, key, slot, lane);
+        else warp_append(W.list[nxt], W.cnt + nxt, mm, slot, lane);
     }
     flush_stats(S, P, lane);
 }
@@ -301,7 +509,7 @@ wf_finish_kernel(const __grid_constant__ KParams P, const __grid_constant__ Wave
     int st = ST_FETCH;
     L.inst = nullptr;
     if (gid < n) {
-        wf_load_lane(W, P, W.list[cur][gid], L);
+        wf_load_lane(W, P, (FK == FK_SPLINE && W.nb) ? brick_slot(W, cur, gid) : W.list[cur][gid], L);
         st = ST_MARCH;
     }
     L.tab = (FK == FK_BATCH && L.inst) ? L.inst->field.btab : tab;

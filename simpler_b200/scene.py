@@ -112,6 +112,7 @@ class Setup:
     device: int = 0
     blocks_per_sm: int = 0
     kernel: int = L.KERNEL_POOL     # smp_kernel: slot pool (default), persistent lane loop, or plain
+    spline_bricks: bool = False     # spline fields: TMA-staged coefficient bricks in shared memory
 
     # ---- descriptors -------------------------------------------------------------------------
     def film_shape(self) -> tuple:
@@ -207,6 +208,7 @@ class Setup:
         o.blocks_per_sm = self.blocks_per_sm
         o.sensor_march_max = self.sensor_march_max
         o.kernel = self.kernel
+        o.spline_bricks = int(self.spline_bricks)
         return o
 
     def descs(self):

@@ -60,6 +60,20 @@ def test_parity_spline_full_64_grid():
     parity.check(s, 300, per_photon=2048)
 
 
+def test_parity_spline_tma_bricks():
+    """The slot pool's spline march with the coefficient grid staged in shared memory brick by brick
+    (Tensor Memory Accelerator copies, march lists binned by brick) gives the photons of the oracle
+    and, on Philox streams, the film of the default path."""
+    s = sb.config_spline(rng=L.RNG_STREAM, spline_bricks=True)
+    parity.check(s, 300, per_photon=2048)
+    s = sb.config_spline(seed=3, spatial_x=64, spatial_y=64, path_length_bins=16, precision_mode=L.PREC_MIXED)
+    ref, rst = sb.render(s, 40_000)
+    s.spline_bricks = True
+    got, gst = sb.render(s, 40_000)
+    assert gst.er_steps == rst.er_steps and gst.splats == rst.splats
+    assert np.abs(got - ref).sum() <= 1e-12 * np.abs(ref).sum()
+
+
 def test_parity_precision_full_film():
     # the headline configuration's 512x512x128 FP64 film (four oracle threads: one film each)
     s = sb.config_precision(rng=L.RNG_STREAM)
