@@ -307,7 +307,8 @@ def test_plan_adjoint_and_autograd():
     np.testing.assert_allclose(ga + gb, g1, rtol=1e-6)
     theta = torch.tensor(sb.field_params(s), requires_grad=True)
     film = render_torch(theta, s, n)
+    assert film.is_cuda                                                              # no host round trip
     ref, _ = sb.render(s, n)
-    np.testing.assert_allclose(film.detach().numpy(), ref, rtol=1e-5, atol=1e-12)   # FP32 film atomics
-    (film * torch.from_numpy(G)).sum().backward()
+    np.testing.assert_allclose(film.detach().cpu().numpy(), ref, rtol=1e-5, atol=1e-12)   # FP32 film atomics
+    (film * torch.from_numpy(G).to(film.device)).sum().backward()
     np.testing.assert_allclose(theta.grad.numpy(), g1, rtol=1e-6)
