@@ -41,15 +41,21 @@ def compare_records(gpu, ref) -> dict:
         rel = np.abs(gs["value"] - rs["value"]) / np.maximum(np.abs(rs["value"]), 1e-30)
         spl_val = np.where(m, np.maximum(spl_val, rel), spl_val)
         spl_depth &= ~m | (gs["depth"] == rs["depth"])
-    ok = same_events & (pos_err <= POS_TOL_M) & (dir_err <= DIR_TOL_RAD) & (path_err <= PATH_TOL_M) & (
-        spl_pos <= POS_TOL_M) & (spl_path <= PATH_TOL_M) & (spl_val <= VALUE_RTOL) & spl_depth
-    return {"ok": ok, "same_events": same_events, "pos_err": pos_err, "dir_err": dir_err, "path_err": path_err,
-            "spl_pos": spl_pos, "spl_path": spl_path, "spl_val": spl_val}
+    # the acceptance bounds of the path: every event equal, positions (end and splats) within 1e-4 mm,
+    # directions within 1e-5 rad, path lengths within 1e-4 mm
+    ok_geom = same_events & (pos_err <= POS_TOL_M) & (dir_err <= DIR_TOL_RAD) & (path_err <= PATH_TOL_M) & (
+        spl_pos <= POS_TOL_M) & (spl_path <= PATH_TOL_M) & spl_depth
+    # and, stricter, every splat value within 1e-4 relative (its exp(-sigma_t d) factor compounds the
+    # FP32 rounding of metres of internally reflected path)
+    ok = ok_geom & (spl_val <= VALUE_RTOL)
+    return {"ok": ok, "ok_geom": ok_geom, "same_events": same_events, "pos_err": pos_err, "dir_err": dir_err,
+            "path_err": path_err, "spl_pos": spl_pos, "spl_path": spl_path, "spl_val": spl_val}
 
 
 def summary(c: dict) -> str:
     n = len(c["ok"])
-    return (f"{c['ok'].sum()}/{n} photons within tolerance; events equal {c['same_events'].sum()}/{n}; "
+    return (f"{c['ok_geom'].sum()}/{n} photons within the position, direction and path bounds, "
+            f"{c['ok'].sum()}/{n} also within the splat-value bound; events equal {c['same_events'].sum()}/{n}; "
             f"max pos {c['pos_err'][c['same_events']].max() if c['same_events'].any() else 0:.3g} m, "
             f"max dir {c['dir_err'][c['same_events']].max() if c['same_events'].any() else 0:.3g} rad, "
             f"max path {c['path_err'][c['same_events']].max() if c['same_events'].any() else 0:.3g} m, "
@@ -69,16 +75,19 @@ def run_pair(setup, n, per_photon=256, weight=1_000_000, threads=0, real_bits=32
     return g, gimg, r, rimg
 
 
-def check(setup, n, min_ok=0.98, min_events=0.995, per_photon=256, img_tol=5e-4, real_bits=32, threads=0):
+def check(setup, n, min_ok=0.98, min_events=0.995, per_photon=256, img_tol=5e-4, real_bits=32, threads=0,
+          min_geom=0.995):
     """Photon-by-photon parity of the GPU against the oracle: at least `min_events` of the photons
-    take the same discrete events and at least `min_ok` are within every tolerance above; the films
-    agree to `img_tol` in relative L1. Prints and returns the comparison."""
+    take the same discrete events, at least `min_geom` are within the position, direction and path
+    bounds and at least `min_ok` within every bound above; the films agree to `img_tol` in relative
+    L1. Prints and returns the comparison."""
     g, gimg, r, rimg = run_pair(setup, n, per_photon, real_bits=real_bits, threads=threads)
     assert not (r["end"] == 8).any(), "oracle ran out of injected uniforms"
     c = compare_records(g, r)
     msg = summary(c)
     print(msg)
     assert c["same_events"].mean() >= min_events, msg
+    assert c["ok_geom"].mean() >= min_geom, msg
     assert c["ok"].mean() >= min_ok, msg
     denom = np.abs(rimg).sum()
     if denom > 0:

@@ -36,7 +36,8 @@ def test_parity_emitter_lens_rejects_outside_aperture():
     assert (r["end"] == genray_fail).mean() > 0.2
     assert ((g["end"] == genray_fail) == (r["end"] == genray_fail)).all()
     c = parity.compare_records(g, r)
-    assert c["same_events"].mean() >= 0.995 and c["ok"].mean() >= 0.98, parity.summary(c)
+    assert c["same_events"].mean() >= 0.995 and c["ok_geom"].mean() >= 0.995 and c["ok"].mean() >= 0.98, \
+        parity.summary(c)
 
 
 def test_parity_sensor_lens():
