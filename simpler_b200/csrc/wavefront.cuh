@@ -425,8 +425,11 @@ wf_march_spline_kernel(const __grid_constant__ KParams P, const __grid_constant_
 // finished photons are replaced from the global photon counter; slots that start a march are
 // appended to the next march list. Also resets the march-list counter just consumed and the event
 // queue the next march launch fills.
+#ifndef SMP_WF_EVENT_MIN_BLOCKS
+#define SMP_WF_EVENT_MIN_BLOCKS 4
+#endif
 template <int FK>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128, SMP_WF_EVENT_MIN_BLOCKS)
 wf_event_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveParams W, int it) {
     const int lane = threadIdx.x & 31;
     const bool init = it < 0;
