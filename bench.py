@@ -563,7 +563,8 @@ def run_adjoint(args):
     clocks = ClockSampler(0)
     clocks.start()
     ms, tot = [], {k: 0 for k in ("er_steps_forward", "er_steps_replay", "points", "splats", "dropped", "skipped",
-                                  "replay_mismatch", "photons", "trace_ms", "launches")}
+                                  "replay_mismatch", "photons", "trace_ms", "replay_ms", "sweep_ms",
+                                  "launches")}
     for i in range(args.steps):
         _, st = plan.adjoint(G, (args.warmup + i) * n, n, n)
         ms.append(st.kernel_ms)

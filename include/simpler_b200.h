@@ -378,8 +378,10 @@ typedef struct smp_adjoint_stats {
     int64_t splats;               /* splats whose value entered the objective                       */
     double  kernel_ms;            /* device time of the adjoint, both kernels, all batches          */
     double  trace_ms;             /* of which the checkpointing trace                               */
-    int64_t launches;             /* kernels launched (a trace per batch, a replay and a sweep per
-                                     round)                                                         */
+    int64_t launches;             /* kernels launched (the trace's per batch, a replay and a sweep
+                                     per round)                                                     */
+    double  replay_ms;            /* of kernel_ms: the segment replays                              */
+    double  sweep_ms;             /* of kernel_ms: the backward sweeps                              */
 } smp_adjoint_stats;
 /* Number of parameters smp_render_adjoint returns for this field, or a negative smp_status:
    Bessel modes 0-2: 3 (n_max, phi_min, phi_max); plane waves 2*n_waves (amplitudes

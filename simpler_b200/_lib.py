@@ -147,7 +147,7 @@ class AdjointStats(C.Structure):
         ("photons", C.c_int64), ("dropped", C.c_int64), ("skipped", C.c_int64), ("aborted", C.c_int64),
         ("replay_mismatch", C.c_int64), ("er_steps_forward", C.c_int64), ("er_steps_replay", C.c_int64),
         ("points", C.c_int64), ("splats", C.c_int64), ("kernel_ms", C.c_double), ("trace_ms", C.c_double),
-        ("launches", C.c_int64),
+        ("launches", C.c_int64), ("replay_ms", C.c_double), ("sweep_ms", C.c_double),
     ]
 
 

@@ -37,6 +37,7 @@
 #pragma once
 #include "dispatch.h"
 #include "march.cuh"
+#include "wavefront.cuh"
 
 namespace smp {
 
@@ -188,12 +189,19 @@ struct AdjParams {
     unsigned long long *traj_next;
     AdjSeg *segs;              // 2 * pool_cap entries
     int *pending;              // a replay round left photons for the next round
-    AdjVertex *tverts;         // checkpointing trace: [threads][vcap] checkpoints of the current photon
+    AdjVertex *tverts;         // checkpointing trace: [slots][vcap] checkpoints of each slot's photon
+    int4 *tstate;              // per slot: checkpoints so far, flags (bit 0 overflow, bit 1 the direct
+                               // splat reaches dJ/dfilm), trajectory entries of the current segment,
+                               // the ER-step count at the start of the slot's current march
     int vcap;
     AdjVertex *pool;           // the batch's checkpoints, photon after photon
     long long pool_cap;
     unsigned long long *pool_next;
     AdjPhoton *photons;        // per photon of the batch
+    int *order;                // the photons the replays and sweeps take, longest trajectory first
+                               // (adjoint_order_*), so that a warp's lanes carry similar lengths
+    unsigned *obucket;         // kOrderBuckets counters of the ordering
+    unsigned long long *n_order;   // entries of `order`
     double *grad;              // dJ/dtheta (layout per field kind, see FieldAdj)
     unsigned long long *cnt;   // AdjCounter
 };
@@ -660,6 +668,7 @@ __device__ __forceinline__ void add_axis(float3 &v, int ax, float x) {
 struct Sweep {
     int i;                     // entry whose step is undone next
     float4 e;
+    float4 pn;                 // entry i - 1, loaded one step ahead (its latency overlaps a step)
     float3 d, gk, Pa, Da, b0;
     float T, a0, n0;
 };
@@ -671,6 +680,7 @@ __device__ __forceinline__ void sweep_begin(Sweep &w, const KParams &P, const Ad
     const FieldParams &F = P.field;
     w.i = nent - 1;
     w.e = traj_get(A, base, w.i);
+    w.pn = traj_get(A, base, w.i - 1);          // nent >= 2
     const float3 pk = f3(w.e.x, w.e.y, w.e.z);
     float n_k, H[6];
     float3 g_k;
@@ -699,13 +709,15 @@ __device__ __forceinline__ int sweep_point(Sweep &w, const KParams &P, const Adj
     const float c = w.e.w, hh = 0.5f * c;
     int j = w.i - 1;
     if (j < 0) return 2;
-    float4 pe = traj_get(A, base, j);
+    float4 pe = w.pn;
     const bool junction = pe.w < 0.0f;
     if (junction) {
         j -= 1;
         if (j < 0) return 2;
         pe = traj_get(A, base, j);
     }
+    // the next call's entry, in flight while this step is undone
+    const float4 nx = (j >= 1 && pe.w != 0.0f) ? traj_get(A, base, j - 1) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const float3 pp = f3(pe.x, pe.y, pe.z);
     float n1, H[6];
     float3 g1;
@@ -744,6 +756,7 @@ __device__ __forceinline__ int sweep_point(Sweep &w, const KParams &P, const Adj
     w.Pa = Pa; w.Da = Da;
     w.i = j;
     w.e = pe;
+    w.pn = nx;
     return 0;
 }
 
@@ -868,6 +881,137 @@ __global__ void __launch_bounds__(128, 4) adjoint_trace_kernel(const __grid_cons
     atomicAdd(A.cnt + ADJ_ABORTED, h.nabort);
 }
 
+// ---- the checkpointing trace on the slot pool ------------------------------------------------------
+// The render's two-kernel march (wavefront.cuh) with the recording hook in the event and tail kernels:
+// wf_march_kernel marches the slots unchanged, and each slot carries its photon's checkpoints
+// (A.tverts) and hook state (A.tstate) between launches. The hook counts a segment's trajectory
+// entries as its march-start markers plus the accepted ER steps; the march kernel does not count:
+// a march's accepted steps are its steps less its refinements (a refinement restores the position,
+// every other step moves it), and the refinements are the precision levels it used,
+// precision - max(prec, 0) at its end.
+__device__ __forceinline__ void trace_hook_load(AdjTraceHook &h, const KParams &P, const AdjParams &A, int slot,
+                                                const Lane &L) {
+    const int4 hs = A.tstate[slot];
+    h.v = A.tverts + size_t(slot) * size_t(A.vcap);
+    h.nv = hs.x;
+    h.overflow = hs.y & 1;
+    h.direct_hit = (hs.y >> 1) & 1;
+    h.seg_entries = hs.z + (L.steps - hs.w) - (P.precision - max(L.prec, 0));
+}
+
+template <int FK>
+__global__ void __launch_bounds__(128, 4)
+adjoint_trace_event_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveParams W,
+                           const __grid_constant__ AdjParams A, int it) {
+    const int lane = threadIdx.x & 31;
+    const bool init = it < 0;
+    const int cur = init ? 1 : (it & 1), nxt = cur ^ 1;
+    const unsigned n = init ? unsigned(W.n_slots) : W.cnt[2 + cur];
+    if (!init && blockIdx.x == 0 && threadIdx.x == 0) {
+        W.cnt[cur] = 0u;          // consumed by march launch `it`
+        W.cnt[2 + nxt] = 0u;      // filled by march launch `it + 1`
+    }
+    LaneStats S;
+    AdjTraceHook h;
+    h.P = &P;
+    h.A = &A;
+    h.vcap = A.vcap;
+    h.nok = h.ndrop = h.nabort = 0;
+    const unsigned lanes = gridDim.x * blockDim.x, nwarps = lanes >> 5;
+    for (unsigned base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; base < n; base += nwarps * 32u) {
+        const unsigned i = base + unsigned(lane);
+        const bool valid = i < n;
+        int st = ST_DONE, slot = 0;
+        if (valid) {
+            slot = init ? int(i) : W.queue[cur][i];
+            Lane L;
+            L.inst = nullptr;
+            if (init) {
+                L.end = 0;
+                L.idx = 0;
+                st = ST_FETCH;
+                h.v = A.tverts + size_t(slot) * size_t(A.vcap);
+            } else {
+                wf_load_lane(W, P, slot, L);
+                L.tab = P.field.btab;
+                trace_hook_load(h, P, A, slot, L);
+                st = run_events<FK, AdjTraceHook>(L, P, EV_MARCH_END, &h);
+                if (st == ST_FETCH) {
+                    finish_photon_stats<FK>(L, S);
+                    h.photon_end(L);
+                }
+            }
+            L.tab = P.field.btab;
+            while (st == ST_FETCH) {
+                const cg::coalesced_group g = cg::coalesced_threads();
+                unsigned long long k = 0;
+                if (g.thread_rank() == 0) k = atomicAdd(P.counters + CNT_NEXT_PHOTON, (unsigned long long)g.size());
+                k = g.shfl(k, 0) + g.thread_rank();
+                if (k < (unsigned long long)P.n_photons) {
+                    L.idx = P.first_photon + (long long)k;
+                    L.end = 0;
+                    h.photon_begin(L);
+                    st = run_events<FK, AdjTraceHook>(L, P, EV_NEW, &h);
+                    if (st == ST_FETCH) {
+                        finish_photon_stats<FK>(L, S);
+                        h.photon_end(L);
+                    }
+                } else {
+                    st = ST_DONE;
+                }
+            }
+            if (st == ST_MARCH) {
+                wf_store_lane(W, P, slot, L);
+                // + 1: the march's start marker
+                A.tstate[slot] = make_int4(h.nv, h.overflow | (h.direct_hit << 1), h.seg_entries + 1, L.steps);
+            }
+        }
+        const unsigned mm = __ballot_sync(kFull, valid && st == ST_MARCH);
+        warp_append(W.list[nxt], W.cnt + nxt, mm, slot, lane);
+    }
+    flush_stats(S, P, lane);
+    if (h.nok) atomicAdd(A.cnt + ADJ_PHOTONS, h.nok);
+    if (h.ndrop) atomicAdd(A.cnt + ADJ_DROPPED, h.ndrop);
+    if (h.nabort) atomicAdd(A.cnt + ADJ_ABORTED, h.nabort);
+}
+
+// the trace's tail: the live slots, with their checkpoints and hook state, on the persistent lane loop
+template <int FK>
+__global__ void __launch_bounds__(128, 4)
+adjoint_trace_finish_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveParams W,
+                            const __grid_constant__ AdjParams A, int it) {
+    const int lane = threadIdx.x & 31, cur = it & 1;
+    const unsigned n = W.cnt[cur];
+    const unsigned gid = blockIdx.x * blockDim.x + threadIdx.x, lanes = gridDim.x * blockDim.x;
+    if (gid == 0 && n > lanes) atomicAdd(P.counters + CNT_LOST, (unsigned long long)(n - lanes));
+    Lane L;
+    L.end = 0;
+    L.idx = 0;
+    L.inst = nullptr;
+    L.tab = P.field.btab;
+    AdjTraceHook h;
+    h.P = &P;
+    h.A = &A;
+    h.vcap = A.vcap;
+    h.nok = h.ndrop = h.nabort = 0;
+    h.v = A.tverts;
+    h.nv = 0; h.overflow = 0; h.direct_hit = 0; h.seg_entries = 0;
+    int st = ST_FETCH;
+    if (gid < n) {
+        const int slot = W.list[cur][gid];
+        wf_load_lane(W, P, slot, L);
+        L.tab = P.field.btab;
+        trace_hook_load(h, P, A, slot, L);
+        st = ST_MARCH;
+    }
+    LaneStats S;
+    lane_loop<FK, AdjTraceHook>(L, st, P, S, lane, &h);
+    flush_stats(S, P, lane);
+    if (h.nok) atomicAdd(A.cnt + ADJ_PHOTONS, h.nok);
+    if (h.ndrop) atomicAdd(A.cnt + ADJ_DROPPED, h.ndrop);
+    if (h.nabort) atomicAdd(A.cnt + ADJ_ABORTED, h.nabort);
+}
+
 // Segment c of a photon is needed by the sweep: the direct march if its splat reaches dJ/dfilm,
 // a connection if its splat does, a move if a later connection does.
 __device__ __forceinline__ bool seg_needed(const AdjPhoton &r, const AdjVertex *V, int c) {
@@ -899,6 +1043,7 @@ __global__ void __launch_bounds__(128, 3) adjoint_replay_kernel(const __grid_con
     AdjSeg *segs = A.segs;
     AdjPhoton r;
     r.last = 0; r.nv = 0;
+    const long long n_order = (long long)*A.n_order;
     int mode = M_DISC, c = 0, K = -1, ev = EV_NEW;
     bool in_seg = false, first = true, trunc = false;
     long long base = 0, pos = 0, pend = 0;          // pend: end of the photon's reserved entries
@@ -911,8 +1056,9 @@ __global__ void __launch_bounds__(128, 3) adjoint_replay_kernel(const __grid_con
                 ++c;
                 while (c <= 2 * K && !seg_needed(r, V, c)) ++c;
                 if (c > 2 * K) {
-                    const long long k = (long long)atomicAdd(A.cnt + ADJ_NEXT, 1ull);
-                    if (k >= P.n_photons) { mode = M_EXIT; break; }
+                    const long long q = (long long)atomicAdd(A.cnt + ADJ_NEXT, 1ull);
+                    if (q >= n_order) { mode = M_EXIT; break; }
+                    const long long k = A.order[q];
                     r = A.photons[k];
                     K = -1;
                     if (r.status != PH_OK || !r.hits || r.round != 0) continue;
@@ -1040,6 +1186,7 @@ __global__ void __launch_bounds__(128, 3) adjoint_sweep_kernel(const __grid_cons
     const int rr_draw = (albedo > 0.0f && albedo < 1.0f) ? 1 : 0;
     const AdjVertex *V = A.pool;
     const AdjSeg *segs = A.segs;
+    const long long n_order = (long long)*A.n_order;
     int mode = M_DISC, job = 0, kv = 0;
     bool busy = false;                          // a photon is in progress
     float s = 0.0f;
@@ -1098,8 +1245,9 @@ __global__ void __launch_bounds__(128, 3) adjoint_sweep_kernel(const __grid_cons
                 } else job = JOB_SOURCE;
             }
             if (!busy) {
-                const long long k = (long long)atomicAdd(A.cnt + ADJ_NEXT, 1ull);
-                if (k >= P.n_photons) { mode = M_EXIT; break; }
+                const long long q = (long long)atomicAdd(A.cnt + ADJ_NEXT, 1ull);
+                if (q >= n_order) { mode = M_EXIT; break; }
+                const long long k = A.order[q];
                 const AdjPhoton r = A.photons[k];
                 if (r.round != round) continue;
                 L.idx = P.first_photon + k;

@@ -1614,6 +1614,61 @@ static int grid_of(const void *fn, int dev) {
     return sms * std::max(per_sm, 1);
 }
 
+// The adjoint's checkpointing trace on the slot pool: the render's march kernel (no hook: the
+// accepted ER steps of a march follow from its step count and refinement level) alternating with
+// the checkpointing event kernel, whose per-slot state (checkpoints, flags, trajectory entries)
+// stays in AdjParams.tverts/tstate between launches; the live slots' tail runs on the persistent
+// lane loop once they fit in one grid. Spline plans march without coefficient bricks here.
+static cudaError_t adjoint_trace_pool(smp_plan *p, const KParams &k, const AdjParams &a, AdjWaveFn fe, AdjWaveFn ff,
+                                      int grid_f, long long *launches) {
+    WaveParams W = p->wp;
+    W.nb = 0;
+    WaveFn fm = wf_march_fn(p->fk, p->kp.fp64 != 0, p->march_block, false);
+    if (!fm) return cudaErrorInvalidDeviceFunction;
+    if (p->smem_bytes > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void *>(fm), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(p->smem_bytes));
+        if (e != cudaSuccess) return e;
+    }
+    const unsigned finish_at = unsigned(grid_f) * unsigned(kBlock);
+    const long long max_iter = (long long)k.step_cap * 4 + (1LL << 20);
+    cudaError_t e = cudaMemsetAsync(W.cnt, 0, 4 * sizeof(unsigned), 0);
+    if (e != cudaSuccess) return e;
+    fe<<<p->grid_event, kBlock>>>(k, W, a, -1);
+    *launches += 1;
+    long long it = 0;
+    bool pending = false;
+    int par = 0;
+    for (;;) {
+        for (int j = 0; j < p->wave_batch; ++j, ++it) {
+            fm<<<p->grid_march, p->march_block, p->smem_bytes>>>(k, W, int(it & 0x3fffffff));
+            fe<<<p->grid_event, kBlock>>>(k, W, a, int(it & 0x3fffffff));
+        }
+        *launches += 2 * p->wave_batch;
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (pending) {                              // the previous batch's live count
+            const int q = par ^ 1;
+            if ((e = cudaEventSynchronize(p->live_ev[q])) != cudaSuccess) return e;
+            const unsigned long long live = p->h_live[2 * q];
+            if (live == 0u) break;
+            if (live <= finish_at && live < (unsigned long long)W.n_slots) {
+                ff<<<grid_f, kBlock>>>(k, W, a, int(it & 0x3fffffff));
+                *launches += 1;
+                return cudaGetLastError();
+            }
+        }
+        p->h_live[2 * par] = 0;
+        if ((e = cudaMemcpyAsync(p->h_live + 2 * par, W.cnt + (it & 1), sizeof(unsigned), cudaMemcpyDeviceToHost, 0)) !=
+            cudaSuccess)
+            return e;
+        if ((e = cudaEventRecord(p->live_ev[par], 0)) != cudaSuccess) return e;
+        pending = true;
+        par ^= 1;
+        if (it > max_iter) return cudaErrorLaunchFailure;
+    }
+    return cudaSuccess;
+}
+
 // Photons are differentiated in batches. Per batch: the checkpointing trace (one checkpoint per
 // scatter vertex into the batch pool), then rounds of replay (every segment the sweep needs,
 // written to the trajectory buffer, as many photons as fit) and sweep (the backward pass over
@@ -1628,16 +1683,25 @@ int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, in
     const int64_t np = smp_adjoint_param_count(&plan->field);
     if (np < 0) return int(np);
     AdjFn fa = adjoint_trace_fn(plan->fk);
+    AdjWaveFn fte = adjoint_trace_event_fn(plan->fk), ftf = adjoint_trace_finish_fn(plan->fk);
     AdjRoundFn fr = adjoint_replay_fn(plan->fk), fs = adjoint_sweep_fn(plan->fk);
-    if (!fa || !fr || !fs) return set_error(SMP_ERR_UNSUPPORTED, "no adjoint for field kind %d", plan->fk);
+    if (!fa || !fte || !ftf || !fr || !fs) return set_error(SMP_ERR_UNSUPPORTED, "no adjoint for field kind %d", plan->fk);
     if (plan->kp.rng != SMP_RNG_PHILOX) return set_error(SMP_ERR_UNSUPPORTED, "the adjoint replays Philox streams only");
     if (plan->kp.src_lens_active || plan->kp.cam_lens_active)
         return set_error(SMP_ERR_UNSUPPORTED, "the adjoint is built for scenes without lenses");
     SMP_CUDA(cudaSetDevice(plan->device));
+    // the trace runs on the slot pool (march kernel + a checkpointing event kernel), or, with
+    // SMP_ADJ_TRACE=lanes, as one persistent lane-loop launch
+    const char *trace_env = std::getenv("SMP_ADJ_TRACE");
+    const bool trace_lanes = trace_env && std::strcmp(trace_env, "lanes") == 0;
+    int rc0 = wave_setup(plan);
+    if (rc0) return rc0;
     const int grid_a = grid_of(reinterpret_cast<const void *>(fa), plan->device);
+    const int grid_tf = grid_of(reinterpret_cast<const void *>(ftf), plan->device);
     const int grid_r = grid_of(reinterpret_cast<const void *>(fr), plan->device);
     const int grid_s = grid_of(reinterpret_cast<const void *>(fs), plan->device);
-    if (!grid_a || !grid_r || !grid_s) return set_error(SMP_ERR_CUDA, "adjoint occupancy query failed");
+    if (!grid_a || !grid_tf || !grid_r || !grid_s) return set_error(SMP_ERR_CUDA, "adjoint occupancy query failed");
+    const size_t trace_threads = trace_lanes ? size_t(grid_a) * kBlock : size_t(plan->wp.n_slots);
     AdjParams a;
     std::memset(&a, 0, sizeof(a));
     a.X = plan->kp.X; a.Y = plan->kp.Y; a.Z = plan->kp.Z;
@@ -1647,14 +1711,14 @@ int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, in
     a.pool_cap = batch * per_photon;
     a.traj_cap = (long long)env_int("SMP_ADJ_TRAJ_MB", 8192, 16, 1 << 20) * (1LL << 20) / (long long)sizeof(float4);
     const size_t film = size_t(a.X) * a.Y * a.Z;
-    const int ncnt = ADJ_COUNT + CNT_COUNT + 3;          // + pool_next, traj_next, pending
+    const int ncnt = ADJ_COUNT + CNT_COUNT + 4;          // + pool_next, traj_next, pending, n_order
     auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t bG = up(film * sizeof(double)), bgrad = up(size_t(np) * sizeof(double));
     const size_t bcnt = up(ncnt * sizeof(unsigned long long));
-    const size_t btv = up(size_t(a.vcap) * grid_a * kBlock * sizeof(AdjVertex));
+    const size_t btv = up(size_t(a.vcap) * trace_threads * sizeof(AdjVertex)) + up(trace_threads * sizeof(int4));
     const size_t bpool = up(size_t(a.pool_cap) * sizeof(AdjVertex));
     const size_t bsegs = up(2 * size_t(a.pool_cap) * sizeof(AdjSeg));
-    const size_t bph = up(size_t(batch) * sizeof(AdjPhoton));
+    const size_t bph = up(size_t(batch) * sizeof(AdjPhoton)) + up(size_t(batch) * sizeof(int)) + up(1024 * sizeof(unsigned));
     const size_t btraj = size_t(a.traj_cap) * sizeof(float4);
     const size_t need = bG + bgrad + bcnt + btv + bpool + bsegs + bph + btraj;
     if (plan->adj_bytes < need) {
@@ -1671,27 +1735,33 @@ int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, in
     double *d_G = reinterpret_cast<double *>(base); base += bG;
     double *d_grad = reinterpret_cast<double *>(base); base += bgrad;
     unsigned long long *d_cnt = reinterpret_cast<unsigned long long *>(base); base += bcnt;
-    a.tverts = reinterpret_cast<AdjVertex *>(base); base += btv;
+    a.tverts = reinterpret_cast<AdjVertex *>(base);
+    a.tstate = reinterpret_cast<int4 *>(base + up(size_t(a.vcap) * trace_threads * sizeof(AdjVertex)));
+    base += btv;
     a.pool = reinterpret_cast<AdjVertex *>(base); base += bpool;
     a.segs = reinterpret_cast<AdjSeg *>(base); base += bsegs;
-    a.photons = reinterpret_cast<AdjPhoton *>(base); base += bph;
+    a.photons = reinterpret_cast<AdjPhoton *>(base);
+    a.order = reinterpret_cast<int *>(base + up(size_t(batch) * sizeof(AdjPhoton)));
+    a.obucket = reinterpret_cast<unsigned *>(base + up(size_t(batch) * sizeof(AdjPhoton)) + up(size_t(batch) * sizeof(int)));
+    base += bph;
     a.traj = reinterpret_cast<float4 *>(base);
     a.G = d_G; a.grad = d_grad; a.cnt = d_cnt;
     unsigned long long *d_kcnt = d_cnt + ADJ_COUNT;
     a.pool_next = d_kcnt + CNT_COUNT;
     a.traj_next = a.pool_next + 1;
     a.pending = reinterpret_cast<int *>(a.pool_next + 2);
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    a.n_order = a.pool_next + 3;
+    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     int rc = SMP_OK;
     cudaError_t e = cudaMemcpy(d_G, dJ_dfilm, film * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(d_grad, 0, size_t(np) * sizeof(double));
     if (e == cudaSuccess) e = cudaMemset(d_cnt, 0, ncnt * sizeof(unsigned long long));
-    for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&ev[i]);
+    for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&ev[i]);
     unsigned long long c[ADJ_COUNT] = {0};
     unsigned long long fwd_steps = 0;
     long long launches = 0;
     float ms = 0.0f;
-    double trace_ms = 0.0;
+    double trace_ms = 0.0, replay_ms = 0.0, sweep_ms = 0.0;
     if (e != cudaSuccess) {
         rc = set_error(SMP_ERR_CUDA, "adjoint setup: %s", cudaGetErrorString(e));
     } else if (n_photons > 0) {
@@ -1709,24 +1779,42 @@ int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, in
             k.n_photons = std::min<long long>(batch, n_photons - done);
             e = cudaMemsetAsync(d_kcnt, 0, (CNT_COUNT + 1) * sizeof(unsigned long long), 0);
             cudaEventRecord(ev[2], 0);
-            if (e == cudaSuccess) { fa<<<grid_a, kBlock>>>(k, a); ++launches; }
+            if (e == cudaSuccess) {
+                if (trace_lanes) { fa<<<grid_a, kBlock>>>(k, a); ++launches; }
+                else {
+                    long long nl = 0;
+                    e = adjoint_trace_pool(plan, k, a, fte, ftf, grid_tf, &nl);
+                    launches += nl;
+                }
+            }
+            if (e == cudaSuccess) { e = adjoint_order(a, k.n_photons, grid_r, 0); launches += 3; }
             cudaEventRecord(ev[3], 0);
+            float tms = 0.0f;
+            if (e == cudaSuccess) e = cudaEventSynchronize(ev[3]);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&tms, ev[2], ev[3]);
+            trace_ms += tms;
             for (int round = 1; e == cudaSuccess; ++round) {
                 e = cudaMemsetAsync(a.traj_next, 0, 2 * sizeof(unsigned long long), 0);
                 if (e == cudaSuccess) e = cudaMemsetAsync(d_cnt + ADJ_NEXT, 0, sizeof(unsigned long long), 0);
+                cudaEventRecord(ev[2], 0);
                 if (e == cudaSuccess) { fr<<<grid_r, kBlock>>>(k, a, round); ++launches; }
+                cudaEventRecord(ev[4], 0);
                 if (e == cudaSuccess) e = cudaMemsetAsync(d_cnt + ADJ_NEXT, 0, sizeof(unsigned long long), 0);
+                cudaEventRecord(ev[5], 0);
                 if (e == cudaSuccess) { fs<<<grid_s, kBlock>>>(k, a, round); ++launches; }
+                cudaEventRecord(ev[3], 0);
                 if (e == cudaSuccess) e = cudaGetLastError();
                 int pending = 0;
                 if (e == cudaSuccess) e = cudaMemcpy(&pending, a.pending, sizeof(int), cudaMemcpyDeviceToHost);
+                float rms = 0.0f, sms = 0.0f;
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&rms, ev[2], ev[4]);
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&sms, ev[5], ev[3]);
+                replay_ms += rms;
+                sweep_ms += sms;
                 if (!pending) break;
             }
             unsigned long long steps = 0;
             if (e == cudaSuccess) e = cudaMemcpy(&steps, d_kcnt + CNT_STEPS, sizeof(steps), cudaMemcpyDeviceToHost);
-            float tms = 0.0f;
-            if (e == cudaSuccess) e = cudaEventElapsedTime(&tms, ev[2], ev[3]);
-            trace_ms += tms;
             fwd_steps += steps;
         }
         cudaEventRecord(ev[1], 0);
@@ -1751,8 +1839,10 @@ int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, in
         stats_out->kernel_ms = ms;
         stats_out->trace_ms = trace_ms;
         stats_out->launches = launches;
+        stats_out->replay_ms = replay_ms;
+        stats_out->sweep_ms = sweep_ms;
     }
-    for (int i = 0; i < 4; ++i) if (ev[i]) cudaEventDestroy(ev[i]);
+    for (int i = 0; i < 6; ++i) if (ev[i]) cudaEventDestroy(ev[i]);
     if (!rc && c[ADJ_MISMATCH])
         rc = set_error(SMP_ERR_CUDA, "internal: %llu segment replay(s) diverged from their checkpoint", c[ADJ_MISMATCH]);
     return rc;

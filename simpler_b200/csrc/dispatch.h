@@ -2,6 +2,8 @@
 // k_wave.cu, k_adjoint.cu, adjoint_sweep.cu) so that they build in parallel, and handed to the host
 // code in capi.cu as function pointers per field kind.
 #pragma once
+#include <cuda_runtime.h>
+
 #include "kparams.h"
 
 namespace smp {
@@ -14,6 +16,7 @@ typedef void (*WaveFn)(KParams, WaveParams, int);
 typedef void (*ProbeFn)(FieldParams, float, long long, const double *, double *, double *);
 typedef void (*AdjFn)(KParams, AdjParams);
 typedef void (*AdjRoundFn)(KParams, AdjParams, int);
+typedef void (*AdjWaveFn)(KParams, WaveParams, AdjParams, int);
 
 // k_march.cu
 MarchFn march_fn(int fk);                        // persistent lane loop (march.cuh)
@@ -25,8 +28,12 @@ WaveFn wf_march_fn(int fk, bool fp64, int block, bool bricks);
 WaveFn wf_event_fn(int fk);
 WaveFn wf_finish_fn(int fk);
 // k_adjoint.cu, adjoint_sweep.cu
-AdjFn adjoint_trace_fn(int fk);
+AdjFn adjoint_trace_fn(int fk);                  // the trace on the persistent lane loop
+AdjWaveFn adjoint_trace_event_fn(int fk);        // the trace on the slot pool: event and tail kernels
+AdjWaveFn adjoint_trace_finish_fn(int fk);
 AdjRoundFn adjoint_replay_fn(int fk);
 AdjRoundFn adjoint_sweep_fn(int fk);
+// the batch's photons in the order replays and sweeps take them (A.order, *A.n_order)
+cudaError_t adjoint_order(const AdjParams &A, long long n, int grid, cudaStream_t s);
 
 }  // namespace smp
