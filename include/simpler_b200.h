@@ -395,7 +395,11 @@ int64_t smp_adjoint_param_count(const smp_field_desc *field);
    and ER step sequences are held fixed, and marches ending on a face end on the face plane.
    dJ_dfilm: host, X*Y*Z doubles (Image3 layout); grad_out: host, smp_adjoint_param_count doubles,
    overwritten. Bessel (modes 0-2), plane-wave and spline fields, Philox streams, no lenses; others
-   return SMP_ERR_UNSUPPORTED. Synchronous. */
+   return SMP_ERR_UNSUPPORTED. Synchronous. Device memory, sized at the plan's first adjoint and
+   kept by the plan: photons are differentiated in batches of 2^22 (2^21 when less than 64 GiB is
+   free), each with 16 checkpoints per photon in its pool, and the replayed trajectories go through
+   a buffer of a quarter of the free memory, 1-40 GiB (environment: SMP_ADJ_BATCH photons,
+   SMP_ADJ_TRAJ_MB MiB, SMP_ADJ_POOL_PER_PHOTON); a smaller buffer only means more replay rounds. */
 int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, int64_t weight_photons,
                      const double *dJ_dfilm, double *grad_out, smp_adjoint_stats *stats_out);
 int smp_render_adjoint(const smp_scene_desc *scene, const smp_medium_desc *medium,

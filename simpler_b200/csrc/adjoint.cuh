@@ -202,6 +202,8 @@ struct AdjParams {
                                // (adjoint_order_*), so that a warp's lanes carry similar lengths
     unsigned *obucket;         // kOrderBuckets counters of the ordering
     unsigned long long *n_order;   // entries of `order`
+    int idle_replay, idle_sweep;   // a warp leaves its march / sweep loop for discrete work once this
+                                   // many 32nds of its live lanes wait
     double *grad;              // dJ/dtheta (layout per field kind, see FieldAdj)
     unsigned long long *cnt;   // AdjCounter
 };
@@ -228,13 +230,14 @@ template <int FK> struct FieldAdj;
 //   grad n = sum_i a_i cos(.) k_i,  H = -sum_i a_i sin(.) k_i k_i^T,
 //   dJ/da_i += a sin + cos (k_i.b),  dJ/dphase_i += a a_i cos - a_i sin (k_i.b)
 // for the cotangent (a, b) of (n, grad n). Gradient layout: a_0..a_{W-1}, phase_0..phase_{W-1}.
-template <> struct FieldAdj<FK_PLANEWAVE> {
-    struct Acc { float ga[SMP_MAX_WAVES], gp[SMP_MAX_WAVES]; };
-    struct Cache { float sn[SMP_MAX_WAVES], cs[SMP_MAX_WAVES]; int gap; };   // eval_h -> theta_c at one point
+// NW: the largest wave count the instance handles (its accumulators and caches live in registers)
+template <int NW> struct FieldAdjPW {
+    struct Acc { float ga[NW], gp[NW]; };
+    struct Cache { float sn[NW], cs[NW]; int gap; };   // eval_h -> theta_c at one point
     static __device__ __forceinline__ void begin(Acc &, Lane &, const KParams &, float) {}
     static __device__ __forceinline__ void clear(Acc &c) {
 #pragma unroll
-        for (int i = 0; i < SMP_MAX_WAVES; ++i) { c.ga[i] = 0.0f; c.gp[i] = 0.0f; }
+        for (int i = 0; i < NW; ++i) { c.ga[i] = 0.0f; c.gp[i] = 0.0f; }
     }
     static __device__ __forceinline__ void eval_h(const FieldParams &F, float3 p, float tau, float &n, float3 &g, float H[6]) {
 #pragma unroll
@@ -243,7 +246,7 @@ template <> struct FieldAdj<FK_PLANEWAVE> {
         g = f3(0.0f, 0.0f, 0.0f);
         if (in_gap(F, p)) return;
 #pragma unroll
-        for (int i = 0; i < SMP_MAX_WAVES; ++i) {
+        for (int i = 0; i < NW; ++i) {
             if (i < F.n_waves) {
                 const float kx = F.wk[i][0], ky = F.wk[i][1], kz = F.wk[i][2];
                 float sn, cs;
@@ -259,7 +262,7 @@ template <> struct FieldAdj<FK_PLANEWAVE> {
     static __device__ __forceinline__ void theta(const FieldParams &F, float3 p, float tau, float a, float3 b, Acc &c, const AdjParams &) {
         if (in_gap(F, p)) return;
 #pragma unroll
-        for (int i = 0; i < SMP_MAX_WAVES; ++i) {
+        for (int i = 0; i < NW; ++i) {
             if (i < F.n_waves) {
                 const float kx = F.wk[i][0], ky = F.wk[i][1], kz = F.wk[i][2];
                 float sn, cs;
@@ -280,7 +283,7 @@ template <> struct FieldAdj<FK_PLANEWAVE> {
         k.gap = in_gap(F, p);
         if (k.gap) return;
 #pragma unroll
-        for (int i = 0; i < SMP_MAX_WAVES; ++i) {
+        for (int i = 0; i < NW; ++i) {
             if (i < F.n_waves) {
                 const float kx = F.wk[i][0], ky = F.wk[i][1], kz = F.wk[i][2];
                 float sn, cs;
@@ -298,7 +301,7 @@ template <> struct FieldAdj<FK_PLANEWAVE> {
                                                    const AdjParams &, const Cache &k) {
         if (k.gap) return;
 #pragma unroll
-        for (int i = 0; i < SMP_MAX_WAVES; ++i) {
+        for (int i = 0; i < NW; ++i) {
             if (i < F.n_waves) {
                 const float kb = F.wk[i][0] * b.x + F.wk[i][1] * b.y + F.wk[i][2] * b.z;
                 c.ga[i] += a * k.sn[i] + k.cs[i] * kb;
@@ -308,7 +311,7 @@ template <> struct FieldAdj<FK_PLANEWAVE> {
     }
     static __device__ __forceinline__ void flush(const Acc &c, const FieldParams &F, const AdjParams &A) {
 #pragma unroll
-        for (int i = 0; i < SMP_MAX_WAVES; ++i) {
+        for (int i = 0; i < NW; ++i) {
             if (i < F.n_waves) {
                 atomicAdd(A.grad + i, double(c.ga[i]));
                 atomicAdd(A.grad + F.n_waves + i, double(c.gp[i]));
@@ -316,6 +319,8 @@ template <> struct FieldAdj<FK_PLANEWAVE> {
         }
     }
 };
+
+template <> struct FieldAdj<FK_PLANEWAVE> : FieldAdjPW<SMP_MAX_WAVES> {};
 
 // Tricubic B-spline n = sum_taps c w_x w_y w_z (the coefficient mean is stored apart, which is the
 // same function because the weights sum to 1). dJ/dc for each of the 64 taps is
@@ -673,10 +678,10 @@ struct Sweep {
     float T, a0, n0;
 };
 
-template <int FK>
+template <int FK, class FA>
 __device__ __forceinline__ void sweep_begin(Sweep &w, const KParams &P, const AdjParams &A, long long base, int nent,
                                             float3 md_end, float3 Pa, float3 Da, float a_end, float T, bool face_end,
-                                            float s, typename FieldAdj<FK>::Acc &acc) {
+                                            float s, typename FA::Acc &acc) {
     const FieldParams &F = P.field;
     w.i = nent - 1;
     w.e = traj_get(A, base, w.i);
@@ -684,8 +689,8 @@ __device__ __forceinline__ void sweep_begin(Sweep &w, const KParams &P, const Ad
     const float3 pk = f3(w.e.x, w.e.y, w.e.z);
     float n_k, H[6];
     float3 g_k;
-    typename FieldAdj<FK>::Cache kc;
-    FieldAdj<FK>::eval_h(F, pk, s, n_k, g_k, H, kc);
+    typename FA::Cache kc;
+    FA::eval_h(F, pk, s, n_k, g_k, H, kc);
     const float3 u = divs(md_end, n_k);
     const float At = dot3(u, Pa) + dot3(g_k, Da) + dot3(g_k, u) * a_end;
     if (face_end) {
@@ -697,14 +702,14 @@ __device__ __forceinline__ void sweep_begin(Sweep &w, const KParams &P, const Ad
     // second kick of the last step, and the end point's own use of n
     const float3 b = mul(Da, 0.5f * w.e.w);
     Pa = add(Pa, add(mul(g_k, a_end), hmul(H, b)));
-    FieldAdj<FK>::theta_c(F, pk, s, a_end, b, acc, A, kc);
+    FA::theta_c(F, pk, s, a_end, b, acc, A, kc);
     w.d = md_end; w.gk = g_k; w.Pa = Pa; w.Da = Da; w.T = T;
 }
 
 // Undo one step. 0: more to go; 1: the start point is reached (outputs in w); 2: malformed.
-template <int FK>
+template <int FK, class FA>
 __device__ __forceinline__ int sweep_point(Sweep &w, const KParams &P, const AdjParams &A, long long base, float s,
-                                           typename FieldAdj<FK>::Acc &acc) {
+                                           typename FA::Acc &acc) {
     const FieldParams &F = P.field;
     const float c = w.e.w, hh = 0.5f * c;
     int j = w.i - 1;
@@ -721,8 +726,8 @@ __device__ __forceinline__ int sweep_point(Sweep &w, const KParams &P, const Adj
     const float3 pp = f3(pe.x, pe.y, pe.z);
     float n1, H[6];
     float3 g1;
-    typename FieldAdj<FK>::Cache kc;
-    FieldAdj<FK>::eval_h(F, pp, s, n1, g1, H, kc);
+    typename FA::Cache kc;
+    FA::eval_h(F, pp, s, n1, g1, H, kc);
     const float3 dh = sub(w.d, mul(w.gk, hh));
     const float3 dprev = sub(dh, mul(g1, hh));
     const float q = c / n1;
@@ -752,7 +757,7 @@ __device__ __forceinline__ int sweep_point(Sweep &w, const KParams &P, const Adj
     const float3 b2 = mul(Da, 0.5f * pe.w);
     Pa = add(Pa, hmul(H, b2));
     b1 = add(b1, b2);
-    FieldAdj<FK>::theta_c(F, pp, s, a1, b1, acc, A, kc);
+    FA::theta_c(F, pp, s, a1, b1, acc, A, kc);
     w.Pa = Pa; w.Da = Da;
     w.i = j;
     w.e = pe;
@@ -1139,7 +1144,7 @@ __global__ void __launch_bounds__(128, 3) adjoint_replay_kernel(const __grid_con
 
         const unsigned live = __ballot_sync(kFull, mode != M_EXIT);
         if (live == 0) break;
-        const int thr = max(1, (__popc(live) + 2) >> 2);
+        const int thr = max(1, (__popc(live) * A.idle_replay + 16) >> 5);
         if (__any_sync(kFull, mode == M_MARCH)) {
             for (;;) {
                 if (mode == M_MARCH) {
@@ -1173,9 +1178,15 @@ enum AdjJob : int { JOB_CONN = 1, JOB_MOVE = 2, JOB_DIRECT = 3, JOB_SOURCE = 4 }
 
 
 
-template <int FK>
-__global__ void __launch_bounds__(128, 3) adjoint_sweep_kernel(const __grid_constant__ KParams P,
+// The sweep kernel per field kind; NW bounds the plane-wave count (a plane-wave field of at most two
+// waves runs the NW = 2 instance, whose accumulators take fewer registers); MINB resident blocks.
+template <int FK, int NW> struct FieldAdjSel { typedef FieldAdj<FK> T; };
+template <int NW> struct FieldAdjSel<FK_PLANEWAVE, NW> { typedef FieldAdjPW<NW> T; };
+
+template <int FK, int NW, int MINB>
+__global__ void __launch_bounds__(128, MINB) adjoint_sweep_kernel(const __grid_constant__ KParams P,
                                                             const __grid_constant__ AdjParams A, int round) {
+    typedef typename FieldAdjSel<FK, NW>::T FA;
     const FieldParams &F = P.field;
     Lane L;                                     // Philox draws of the HG rotation
     L.tab = P.field.btab;                       // Bessel table (global memory); NULL for other fields
@@ -1192,8 +1203,8 @@ __global__ void __launch_bounds__(128, 3) adjoint_sweep_kernel(const __grid_cons
     float s = 0.0f;
     float3 lp = f3(0.0f, 0.0f, 0.0f), ld = lp, Ddir = lp;
     long long sbase = 0;
-    typename FieldAdj<FK>::Acc acc;
-    FieldAdj<FK>::clear(acc);
+    typename FA::Acc acc;
+    FA::clear(acc);
     Sweep w;
     bool after = false;                         // a sweep just finished: its job's start handling is due
 
@@ -1209,9 +1220,9 @@ __global__ void __launch_bounds__(128, 3) adjoint_sweep_kernel(const __grid_cons
                     const float as = (g.md0[0] * w.Da.x + g.md0[1] * w.Da.y + g.md0[2] * w.Da.z) / w.n0;
                     lp = add(lp, add(w.Pa, mul(w.gk, as)));
                     ld = add(ld, Ddir);
-                    FieldAdj<FK>::theta(F, p0, s, w.a0 + as, w.b0, acc, A);
+                    FA::theta(F, p0, s, w.a0 + as, w.b0, acc, A);
                 } else if (job == JOB_MOVE) {
-                    FieldAdj<FK>::theta(F, p0, s, w.a0, w.b0, acc, A);
+                    FA::theta(F, p0, s, w.a0, w.b0, acc, A);
                     lp = w.Pa;
                     if (kv >= 2) {
                         // the move began with v' = |v| HG(v / |v|) at vertex kv - 1
@@ -1235,7 +1246,7 @@ __global__ void __launch_bounds__(128, 3) adjoint_sweep_kernel(const __grid_cons
                 } else {                            // JOB_DIRECT: starts from the source state
                     lp = add(lp, w.Pa);
                     ld = add(ld, w.Da);
-                    FieldAdj<FK>::theta(F, p0, s, w.a0, w.b0, acc, A);
+                    FA::theta(F, p0, s, w.a0, w.b0, acc, A);
                 }
                 // the next job
                 if (job == JOB_CONN) job = JOB_MOVE;
@@ -1254,8 +1265,8 @@ __global__ void __launch_bounds__(128, 3) adjoint_sweep_kernel(const __grid_cons
                 s = r.s;
                 V = A.pool + r.off;
                 segs = A.segs + 2LL * r.off;
-                FieldAdj<FK>::clear(acc);
-                FieldAdj<FK>::begin(acc, L, P, s);
+                FA::clear(acc);
+                FA::begin(acc, L, P, s);
                 lp = f3(0.0f, 0.0f, 0.0f); ld = lp;
                 kv = r.nv - 1;
                 job = kv >= 1 ? JOB_CONN : JOB_DIRECT;
@@ -1269,11 +1280,11 @@ __global__ void __launch_bounds__(128, 3) adjoint_sweep_kernel(const __grid_cons
                     const float3 p0 = f3(c.pos[0], c.pos[1], c.pos[2]);
                     float n0, H[6];
                     float3 g0;
-                    FieldAdj<FK>::eval_h(F, p0, s, n0, g0, H);
+                    FA::eval_h(F, p0, s, n0, g0, H);
                     const float as = (c.dir[0] * ld.x + c.dir[1] * ld.y + c.dir[2] * ld.z) / n0;
-                    FieldAdj<FK>::theta(F, p0, s, as, f3(0.0f, 0.0f, 0.0f), acc, A);
+                    FA::theta(F, p0, s, as, f3(0.0f, 0.0f, 0.0f), acc, A);
                 }
-                FieldAdj<FK>::flush(acc, F, A);
+                FA::flush(acc, F, A);
                 busy = false;
                 continue;
             }
@@ -1307,7 +1318,7 @@ __global__ void __launch_bounds__(128, 3) adjoint_sweep_kernel(const __grid_cons
             if (run && segs[c].len >= 2 && (job != JOB_MOVE || segs[c].ok)) {
                 const AdjSeg &g = segs[c];
                 sbase = g.off;
-                sweep_begin<FK>(w, P, A, sbase, g.len, f3(g.md[0], g.md[1], g.md[2]), Pa, Da, a_end, T, face_end, s, acc);
+                sweep_begin<FK, FA>(w, P, A, sbase, g.len, f3(g.md[0], g.md[1], g.md[2]), Pa, Da, a_end, T, face_end, s, acc);
                 mode = M_SWEEP;
                 break;
             }
@@ -1322,11 +1333,11 @@ __global__ void __launch_bounds__(128, 3) adjoint_sweep_kernel(const __grid_cons
 
         const unsigned live = __ballot_sync(kFull, mode != M_EXIT);
         if (live == 0) break;
-        const int thr = max(1, (__popc(live) + 2) >> 2);
+        const int thr = max(1, (__popc(live) * A.idle_sweep + 16) >> 5);
         if (__any_sync(kFull, mode == M_SWEEP)) {
             for (;;) {
                 if (mode == M_SWEEP) {
-                    const int rr = sweep_point<FK>(w, P, A, sbase, s, acc);
+                    const int rr = sweep_point<FK, FA>(w, P, A, sbase, s, acc);
                     ++pts;
                     if (rr == 1) { mode = M_DISC; after = true; }
                     else if (rr == 2) {

@@ -8,13 +8,17 @@
 
 namespace smp {
 
-AdjRoundFn adjoint_sweep_fn(int fk) {
+// Resident blocks per SM: 4 (128 registers) where the kernel fits without spilling much (Bessel,
+// plane waves of at most two waves: 20-25 % faster than 3), 3 for the spline and the eight-wave
+// instance, whose spills at 128 registers cost what the occupancy gains.
+AdjRoundFn adjoint_sweep_fn(int fk, int n_waves) {
     switch (fk) {
-        case FK_BESSEL0: return adjoint_sweep_kernel<FK_BESSEL0>;
-        case FK_BESSEL1: return adjoint_sweep_kernel<FK_BESSEL1>;
-        case FK_BESSEL2: return adjoint_sweep_kernel<FK_BESSEL2>;
-        case FK_PLANEWAVE: return adjoint_sweep_kernel<FK_PLANEWAVE>;
-        case FK_SPLINE: return adjoint_sweep_kernel<FK_SPLINE>;
+        case FK_BESSEL0: return adjoint_sweep_kernel<FK_BESSEL0, SMP_MAX_WAVES, 4>;
+        case FK_BESSEL1: return adjoint_sweep_kernel<FK_BESSEL1, SMP_MAX_WAVES, 4>;
+        case FK_BESSEL2: return adjoint_sweep_kernel<FK_BESSEL2, SMP_MAX_WAVES, 4>;
+        case FK_PLANEWAVE:
+            return n_waves <= 2 ? adjoint_sweep_kernel<FK_PLANEWAVE, 2, 4> : adjoint_sweep_kernel<FK_PLANEWAVE, SMP_MAX_WAVES, 3>;
+        case FK_SPLINE: return adjoint_sweep_kernel<FK_SPLINE, SMP_MAX_WAVES, 3>;
         default: return nullptr;
     }
 }

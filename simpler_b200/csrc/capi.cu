@@ -461,6 +461,7 @@ struct smp_plan {
     // adjoint buffers (smp_plan_adjoint), kept for the plan's life and grown on demand
     void *adj_buf = nullptr;
     size_t adj_bytes = 0;
+    long long adj_batch = 0, adj_traj_mb = 0;   // adjoint batch and trajectory buffer, fixed at the first adjoint
     std::vector<cudaEvent_t> march_ev;   // event pairs around march-kernel launches (a reused pool)
     size_t march_ev_used = 0;            // since the last clear
     long long n_launched = 0;            // kernels launched since the last clear
@@ -1684,7 +1685,7 @@ int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, in
     if (np < 0) return int(np);
     AdjFn fa = adjoint_trace_fn(plan->fk);
     AdjWaveFn fte = adjoint_trace_event_fn(plan->fk), ftf = adjoint_trace_finish_fn(plan->fk);
-    AdjRoundFn fr = adjoint_replay_fn(plan->fk), fs = adjoint_sweep_fn(plan->fk);
+    AdjRoundFn fr = adjoint_replay_fn(plan->fk), fs = adjoint_sweep_fn(plan->fk, plan->kp.field.n_waves);
     if (!fa || !fte || !ftf || !fr || !fs) return set_error(SMP_ERR_UNSUPPORTED, "no adjoint for field kind %d", plan->fk);
     if (plan->kp.rng != SMP_RNG_PHILOX) return set_error(SMP_ERR_UNSUPPORTED, "the adjoint replays Philox streams only");
     if (plan->kp.src_lens_active || plan->kp.cam_lens_active)
@@ -1706,10 +1707,21 @@ int smp_plan_adjoint(smp_plan *plan, int64_t first_photon, int64_t n_photons, in
     std::memset(&a, 0, sizeof(a));
     a.X = plan->kp.X; a.Y = plan->kp.Y; a.Z = plan->kp.Z;
     a.vcap = env_int("SMP_ADJ_VCAP", 256, 2, 1 << 20);
-    const long long batch = env_int("SMP_ADJ_BATCH", 1 << 21, 1024, 1 << 30);
+    a.idle_replay = env_int("SMP_ADJ_IDLE_REPLAY", 16, 1, 32);   // half of the live lanes
+    a.idle_sweep = env_int("SMP_ADJ_IDLE_SWEEP", 4, 1, 32);     // an eighth
+    if (!plan->adj_batch) {
+        // from the memory free before the first adjoint, so that later calls keep the same sizes
+        size_t fr = 0, tot = 0;
+        SMP_CUDA(cudaMemGetInfo(&fr, &tot));
+        const long long gib = 1LL << 30;
+        plan->adj_batch = env_int("SMP_ADJ_BATCH", (long long)fr >= 64 * gib ? 1 << 22 : 1 << 21, 1024, 1 << 30);
+        plan->adj_traj_mb = env_int("SMP_ADJ_TRAJ_MB", int(std::min<long long>(40960, std::max<long long>(1024, (long long)(fr / 4) >> 20))),
+                                    16, 1 << 20);
+    }
+    const long long batch = plan->adj_batch;
     const long long per_photon = env_int("SMP_ADJ_POOL_PER_PHOTON", 16, 1, 4096);
     a.pool_cap = batch * per_photon;
-    a.traj_cap = (long long)env_int("SMP_ADJ_TRAJ_MB", 8192, 16, 1 << 20) * (1LL << 20) / (long long)sizeof(float4);
+    a.traj_cap = plan->adj_traj_mb * (1LL << 20) / (long long)sizeof(float4);
     const size_t film = size_t(a.X) * a.Y * a.Z;
     const int ncnt = ADJ_COUNT + CNT_COUNT + 4;          // + pool_next, traj_next, pending, n_order
     auto up = [](size_t b) { return (b + 255) & ~size_t(255); };

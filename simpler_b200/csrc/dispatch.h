@@ -32,7 +32,7 @@ AdjFn adjoint_trace_fn(int fk);                  // the trace on the persistent 
 AdjWaveFn adjoint_trace_event_fn(int fk);        // the trace on the slot pool: event and tail kernels
 AdjWaveFn adjoint_trace_finish_fn(int fk);
 AdjRoundFn adjoint_replay_fn(int fk);
-AdjRoundFn adjoint_sweep_fn(int fk);
+AdjRoundFn adjoint_sweep_fn(int fk, int n_waves);    // n_waves: of a plane-wave field
 // the batch's photons in the order replays and sweeps take them (A.order, *A.n_order)
 cudaError_t adjoint_order(const AdjParams &A, long long n, int grid, cudaStream_t s);
 

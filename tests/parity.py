@@ -54,12 +54,22 @@ def compare_records(gpu, ref) -> dict:
 
 def summary(c: dict) -> str:
     n = len(c["ok"])
+    se = c["same_events"]
+
+    def mx(k):
+        return c[k][se].max() if se.any() else 0.0
+
+    def over(k, tol):
+        return int((se & (c[k] > tol)).sum())
+
     return (f"{c['ok_geom'].sum()}/{n} photons within the position, direction and path bounds, "
-            f"{c['ok'].sum()}/{n} also within the splat-value bound; events equal {c['same_events'].sum()}/{n}; "
-            f"max pos {c['pos_err'][c['same_events']].max() if c['same_events'].any() else 0:.3g} m, "
-            f"max dir {c['dir_err'][c['same_events']].max() if c['same_events'].any() else 0:.3g} rad, "
-            f"max path {c['path_err'][c['same_events']].max() if c['same_events'].any() else 0:.3g} m, "
-            f"max splat rel value {c['spl_val'].max():.3g}")
+            f"{c['ok'].sum()}/{n} also within the splat-value bound; events equal {se.sum()}/{n}; "
+            f"max pos {mx('pos_err'):.3g} m, max dir {mx('dir_err'):.3g} rad, max path {mx('path_err'):.3g} m, "
+            f"max splat pos {mx('spl_pos'):.3g} m, max splat path {mx('spl_path'):.3g} m, "
+            f"max splat rel value {c['spl_val'].max():.3g}; over the bounds: pos {over('pos_err', POS_TOL_M)}, "
+            f"dir {over('dir_err', DIR_TOL_RAD)}, path {over('path_err', PATH_TOL_M)}, splat pos "
+            f"{over('spl_pos', POS_TOL_M)}, splat path {over('spl_path', PATH_TOL_M)}, splat value "
+            f"{over('spl_val', VALUE_RTOL)}")
 
 
 def run_pair(setup, n, per_photon=256, weight=1_000_000, threads=0, real_bits=32):
@@ -75,20 +85,44 @@ def run_pair(setup, n, per_photon=256, weight=1_000_000, threads=0, real_bits=32
     return g, gimg, r, rimg
 
 
-def check(setup, n, min_ok=0.98, min_events=0.995, per_photon=256, img_tol=5e-4, real_bits=32, threads=0,
-          min_geom=0.995):
-    """Photon-by-photon parity of the GPU against the oracle: at least `min_events` of the photons
-    take the same discrete events, at least `min_geom` are within the position, direction and path
-    bounds and at least `min_ok` within every bound above; the films agree to `img_tol` in relative
-    L1. Prints and returns the comparison."""
-    g, gimg, r, rimg = run_pair(setup, n, per_photon, real_bits=real_bits, threads=threads)
-    assert not (r["end"] == 8).any(), "oracle ran out of injected uniforms"
+def accept(g, r, min_ok=0.98, min_events=0.995, min_geom=0.98, min_end=0.995, min_short=0.995) -> dict:
+    """compare_records(g, r) and the acceptance bounds of `check`; prints and returns the comparison."""
+    n = len(r)
     c = compare_records(g, r)
-    msg = summary(c)
+    end_ok = c["same_events"] & (c["pos_err"] <= POS_TOL_M) & (c["dir_err"] <= DIR_TOL_RAD) & (c["path_err"] <= PATH_TOL_M)
+    short = r["er_steps"] <= np.median(r["er_steps"])
+    c["end_ok"] = end_ok
+    c["short_ok_frac"] = float(c["ok_geom"][short].mean())
+    msg = (summary(c) + f"; ends within the bounds {end_ok.sum()}/{n}; photons with at most the median "
+           f"{int(np.median(r['er_steps']))} ER steps within the bounds {c['ok_geom'][short].sum()}/{short.sum()}")
     print(msg)
     assert c["same_events"].mean() >= min_events, msg
+    assert end_ok.mean() >= min_end, msg
+    assert c["short_ok_frac"] >= min_short, msg
     assert c["ok_geom"].mean() >= min_geom, msg
     assert c["ok"].mean() >= min_ok, msg
+    return c
+
+
+def check(setup, n, min_ok=0.98, min_events=0.995, per_photon=256, img_tol=5e-4, real_bits=32, threads=0,
+          min_geom=0.98, min_end=0.995, min_short=0.995):
+    """Photon-by-photon parity of the GPU against the oracle.
+
+    * at least `min_events` of the photons take the same discrete events;
+    * at least `min_end` end within the position, direction and path bounds;
+    * at least `min_geom` are within them at every splat too, and at least `min_ok` within every
+      bound including the splat values;
+    * at least `min_short` of the photons with no more ER steps than the median are within the
+      position, direction and path bounds everywhere. The photons outside those bounds are the
+      ones whose splats follow long internally reflected connections (tens of thousands of ER
+      steps), where the two float march orders (the GPU's reciprocal and fused multiply-adds, the
+      reference's h d / n) drift apart by up to micrometres; this bound keeps a defect on ordinary
+      paths from hiding among them.
+
+    The films agree to `img_tol` in relative L1. Prints and returns the comparison."""
+    g, gimg, r, rimg = run_pair(setup, n, per_photon, real_bits=real_bits, threads=threads)
+    assert not (r["end"] == 8).any(), "oracle ran out of injected uniforms"
+    c = accept(g, r, min_ok=min_ok, min_events=min_events, min_geom=min_geom, min_end=min_end, min_short=min_short)
     denom = np.abs(rimg).sum()
     if denom > 0:
         rel = np.abs(gimg - rimg).sum() / denom

@@ -136,7 +136,7 @@ def _direct_light_scale(s, G):
 
 
 def test_adjoint_stats_layout():
-    assert sb.check_layout()["smp_adjoint_stats"][0] == 96
+    assert sb.check_layout()["smp_adjoint_stats"][0] == 112
 
 
 # ---- GPU -----------------------------------------------------------------------------------------
@@ -211,6 +211,28 @@ def test_planewave_scattering_matched_fd():
         assert frac > 0.99
         fd /= dh
         assert abs(grad[i] - fd) <= tol * abs(fd), (i, grad[i], fd)
+
+
+@pytest.mark.gpu
+def test_planewave_wave_counts_agree():
+    """The sweep runs a two-wave instance for fields of at most two waves and an eight-wave one
+    otherwise: a third wave of amplitude 0 leaves every photon as it is, so the eight-wave
+    gradient of the first two waves equals the two-wave gradient (up to the order of the float
+    sums), and the third wave's amplitude derivative is that of a field it does not yet change."""
+    s2 = sb.config_planewave(max_depth=7)
+    k = 2.0 * np.pi * 1e6 / 1500.0
+    s3 = sb.config_planewave(max_depth=7, wave_amp=s2.wave_amp + (0.0,), wave_k=s2.wave_k + ((k, 0.0, 0.0),),
+                             wave_phase=s2.wave_phase + (0.5,))
+    G = sb.roi_weights(s2, 32)
+    n = 200_000
+    g2, st2 = sb.adjoint(s2, n, G)
+    g3, st3 = sb.adjoint(s3, n, G)
+    assert st2.replay_mismatch == 0 and st3.replay_mismatch == 0 and st2.dropped == 0 and st3.dropped == 0
+    assert st2.points == st3.points and st2.splats == st3.splats
+    first = [0, 1, 3, 4]                             # a_0, a_1, phase_0, phase_1 of the three-wave layout
+    np.testing.assert_allclose(g3[first], g2, rtol=1e-4, atol=1e-6 * np.abs(g2).max())
+    assert abs(g3[2]) > 1e-3 * np.abs(g2[:2]).max()  # d/da_2 at a_2 = 0
+    assert g3[5] == 0.0                              # d/dphase_2 carries a factor a_2 = 0
 
 
 @pytest.mark.gpu

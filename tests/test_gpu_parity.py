@@ -82,10 +82,7 @@ def test_parity_philox_many_photons_per_lane():
     g = sb.records_to_arrays(g)
     assert (g["photon"] == np.arange(n_gpu)).all()
     r, _ = ob.oracle_trace(s, 0, n_cmp, n_gpu, image=False)
-    c = parity.compare_records(g[:n_cmp], r)
-    assert c["same_events"].mean() >= 0.995, parity.summary(c)
-    assert c["ok_geom"].mean() >= 0.995, parity.summary(c)
-    assert c["ok"].mean() >= 0.98, parity.summary(c)
+    parity.accept(g[:n_cmp], r)
     # the tail of the range as well
     r2, _ = ob.oracle_trace(s, n_gpu - n_cmp, n_cmp, n_gpu, image=False)
     c2 = parity.compare_records(g[n_gpu - n_cmp:], r2)
