@@ -297,8 +297,9 @@ int smp_plan_render(smp_plan *plan, int64_t n_photons, double *image_out, smp_st
 
 /* Autotuner (no counterpart in the reference): times trial traces of n_sample photons (photons
    [0, n_sample) of this plan's render) over the slot pool's march-kernel block size (128, 256),
-   resident slots per march lane (2-8) and chunk (ER steps per slot per march launch, 64-192), keeps
-   the fastest for the plan and caches it per process under the device, field kind, precision, film,
+   resident slots per march lane (2-8) and chunk (ER steps per slot per march launch, 64-192; a sample
+   slower than about 400 ms per trial is scaled down), keeps the fastest (the two best timed twice)
+   for the plan and caches it per process under the device, field kind, precision, film,
    medium, field, scene and sample size, so a later plan of the same configuration takes it without
    trials. The trials render into the plan's film, which is cleared on return: tune before tracing.
    Plans that are not tuned keep their defaults and tune the chunk alone, online, while they trace. */

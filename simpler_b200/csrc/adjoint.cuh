@@ -911,10 +911,11 @@ adjoint_trace_event_kernel(const __grid_constant__ KParams P, const __grid_const
     const int lane = threadIdx.x & 31;
     const bool init = it < 0;
     const int cur = init ? 1 : (it & 1), nxt = cur ^ 1;
-    const unsigned n = init ? unsigned(W.n_slots) : W.cnt[2 + cur];
-    if (!init && blockIdx.x == 0 && threadIdx.x == 0) {
-        W.cnt[cur] = 0u;          // consumed by march launch `it`
-        W.cnt[2 + nxt] = 0u;      // filled by march launch `it + 1`
+    const unsigned q0 = init ? unsigned(W.n_slots) : queue_cnt(W, cur)[0];
+    const unsigned n = init ? q0 : q0 + queue_cnt(W, cur)[1];
+    if (!init && blockIdx.x == 0 && threadIdx.x < 2) {
+        list_cnt(W, cur)[threadIdx.x] = 0u;     // consumed by march launch `it`
+        queue_cnt(W, nxt)[threadIdx.x] = 0u;    // filled by march launch `it + 1`
     }
     LaneStats S;
     AdjTraceHook h;
@@ -927,8 +928,9 @@ adjoint_trace_event_kernel(const __grid_constant__ KParams P, const __grid_const
         const unsigned i = base + unsigned(lane);
         const bool valid = i < n;
         int st = ST_DONE, slot = 0;
+        bool cls1 = false;
         if (valid) {
-            slot = init ? int(i) : W.queue[cur][i];
+            slot = init ? int(i) : two_class_at(W.queue[cur], q0, W.n_slots, i);
             Lane L;
             L.inst = nullptr;
             if (init) {
@@ -969,10 +971,11 @@ adjoint_trace_event_kernel(const __grid_constant__ KParams P, const __grid_const
                 wf_store_lane(W, P, slot, L);
                 // + 1: the march's start marker
                 A.tstate[slot] = make_int4(h.nv, h.overflow | (h.direct_hit << 1), h.seg_entries + 1, L.steps);
+                cls1 = move_class(W, L.ctx);
             }
         }
         const unsigned mm = __ballot_sync(kFull, valid && st == ST_MARCH);
-        warp_append(W.list[nxt], W.cnt + nxt, mm, slot, lane);
+        warp_append2(W.list[nxt], list_cnt(W, nxt), W.n_slots, mm, cls1, slot, lane);
     }
     flush_stats(S, P, lane);
     if (h.nok) atomicAdd(A.cnt + ADJ_PHOTONS, h.nok);
@@ -986,7 +989,7 @@ __global__ void __launch_bounds__(128, 4)
 adjoint_trace_finish_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveParams W,
                             const __grid_constant__ AdjParams A, int it) {
     const int lane = threadIdx.x & 31, cur = it & 1;
-    const unsigned n = W.cnt[cur];
+    const unsigned n0 = list_cnt(W, cur)[0], n = n0 + list_cnt(W, cur)[1];
     const unsigned gid = blockIdx.x * blockDim.x + threadIdx.x, lanes = gridDim.x * blockDim.x;
     if (gid == 0 && n > lanes) atomicAdd(P.counters + CNT_LOST, (unsigned long long)(n - lanes));
     Lane L;
@@ -1003,7 +1006,7 @@ adjoint_trace_finish_kernel(const __grid_constant__ KParams P, const __grid_cons
     h.nv = 0; h.overflow = 0; h.direct_hit = 0; h.seg_entries = 0;
     int st = ST_FETCH;
     if (gid < n) {
-        const int slot = W.list[cur][gid];
+        const int slot = two_class_at(W.list[cur], n0, W.n_slots, gid);
         wf_load_lane(W, P, slot, L);
         L.tab = P.field.btab;
         trace_hook_load(h, P, A, slot, L);

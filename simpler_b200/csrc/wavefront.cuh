@@ -81,7 +81,13 @@ struct WaveParams {
     EventPart *ev;
     int *list[2];      // march lists, by iteration parity
     int *queue[2];     // event queues, by iteration parity
-    unsigned *cnt;     // cnt[0..1] march-list lengths, cnt[2..3] event-queue lengths
+    // Lists and queues hold two classes of march (when `split`): sensor marches (the direct march
+    // and connections, CTX_DIRECT / CTX_CONNECT) from the front of the array, moves from its back
+    // (entry k of class 1 at n_slots - 1 - k). A warp then marches, and afterwards runs the events
+    // of, marches of one kind: long marches to the sensor apart from short exponential moves, and
+    // splat + scatter apart from vertex + connection logic.
+    unsigned *cnt;     // march list of parity p, class c: cnt[2p + c]; event queue: cnt[4 + 2p + c]
+    int split;         // 1: two classes; 0 (spline bricks): class 0 only
     int n_slots;
     int chunk;         // ER steps per slot per march launch (grows when few slots are live)
     // Spline bricks (FK_SPLINE; nb == 0 without them): the march lists binned by the brick of
@@ -100,6 +106,17 @@ struct WaveParams {
                                // {4, kSplineBrick, kSplineBrickRows, kSplineBrickRows}
 };
 
+__device__ __forceinline__ unsigned *list_cnt(const WaveParams &W, int par) { return W.cnt + 2 * par; }
+__device__ __forceinline__ unsigned *queue_cnt(const WaveParams &W, int par) { return W.cnt + 4 + 2 * par; }
+// the march class of a lane about to march: 0 sensor march, 1 move
+__device__ __forceinline__ bool move_class(const WaveParams &W, int ctx) {
+    return W.split && (ctx == CTX_MOVE_FIRST || ctx == CTX_MOVE_VERTEX);
+}
+// entry i of a two-class list whose class 0 holds n0 entries
+__device__ __forceinline__ int two_class_at(const int *arr, unsigned n0, int n_slots, unsigned i) {
+    return i < n0 ? arr[i] : arr[n_slots - 1 - int(i - n0)];
+}
+
 // the brick (cells kSplineBrick b .. kSplineBrick b + kSplineBrick - 1 per axis) a march position lies
 // in, clamped to the grid
 __device__ __forceinline__ int spline_brick_of(const FieldParams &F, const WaveParams &W, float3 p) {
@@ -115,11 +132,11 @@ __device__ __forceinline__ int spline_brick_of(const FieldParams &F, const WaveP
 }
 
 // Appends `slot` of every lane in `mask` to the list of its brick (parity par) and counts them in
-// cnt[par]: one atomic per warp for the count and one per group of lanes of the same brick. All 32
+// the march-list count of parity par: one atomic per warp for the count and one per group of lanes of the same brick. All 32
 // lanes call it.
 __device__ __forceinline__ void brick_append(const WaveParams &W, int par, unsigned mask, int brick, int slot, int lane) {
     if (mask == 0u) return;
-    if (lane == __ffs(mask) - 1) atomicAdd(W.cnt + par, unsigned(__popc(mask)));
+    if (lane == __ffs(mask) - 1) atomicAdd(list_cnt(W, par), unsigned(__popc(mask)));
     if (mask & (1u << lane)) {
         const unsigned same = __match_any_sync(mask, brick);
         const int leader = __ffs(same) - 1;
@@ -202,6 +219,20 @@ __device__ __forceinline__ void warp_append(int *arr, unsigned *cnt, unsigned ma
     if (mask & (1u << lane)) arr[base + unsigned(__popc(mask & ((1u << lane) - 1u)))] = v;
 }
 
+// Appends `v` of every lane in `mask` to the two-class array arr[] with counts c[0], c[1]: lanes
+// with cls1 to class 1 (from the back), the others to class 0. All 32 lanes call it.
+__device__ __forceinline__ void warp_append2(int *arr, unsigned *c, int n_slots, unsigned mask, bool cls1, int v,
+                                             int lane) {
+    const unsigned m1 = __ballot_sync(kFull, cls1) & mask, m0 = mask & ~m1;
+    warp_append(arr, c, m0, v, lane);
+    if (m1 == 0u) return;
+    const int leader = __ffs(m1) - 1;
+    unsigned base = 0u;
+    if (lane == leader) base = atomicAdd(c + 1, unsigned(__popc(m1)));
+    base = __shfl_sync(kFull, base, leader);
+    if (m1 & (1u << lane)) arr[n_slots - 1 - int(base + unsigned(__popc(m1 & ((1u << lane) - 1u))))] = v;
+}
+
 // March launch `it` (BLOCK threads per block, a choice of the plan's tuner): slots on list[it & 1]
 // advance up to `chunk` ER steps each. When fewer slots
 // are live than the grid has lanes, the chunk grows in proportion (up to 64x) so the last photons
@@ -212,7 +243,7 @@ __global__ void __launch_bounds__(BLOCK, (FK == FK_SPLINE ? 4 : SMP_WF_MARCH_MIN
 wf_march_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveParams W, int it) {
     extern __shared__ __align__(16) float4 smem_tab[];
     const int lane = threadIdx.x & 31, cur = it & 1, nxt = cur ^ 1;
-    const unsigned n = W.cnt[cur];
+    const unsigned n0 = list_cnt(W, cur)[0], n = n0 + list_cnt(W, cur)[1];
     if (n == 0u) return;
     if (FK <= FK_BESSELN) {
         if (!stage_to_shared(smem_tab, P.field.btab, unsigned(P.field.bnodes) * 16u, P.counters + CNT_STAGE_TIMEOUT)) {
@@ -232,7 +263,7 @@ wf_march_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
         bool ended = false;
         int slot = 0;
         if (valid) {
-            slot = W.list[cur][i];
+            slot = two_class_at(W.list[cur], n0, W.n_slots, i);
             MarchState M;
             const float4 a = W.ma[slot], b = W.mb[slot], c = W.mc[slot], d = W.mdd[slot];
             const int4 e = W.mi[slot];
@@ -264,8 +295,8 @@ wf_march_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
         }
         const unsigned em = __ballot_sync(kFull, valid && ended);
         const unsigned cm = __ballot_sync(kFull, valid && !ended);
-        warp_append(W.queue[cur], W.cnt + 2 + cur, em, slot, lane);
-        warp_append(W.list[nxt], W.cnt + nxt, cm, slot, lane);
+        warp_append2(W.queue[cur], queue_cnt(W, cur), W.n_slots, em, i >= n0, slot, lane);
+        warp_append2(W.list[nxt], list_cnt(W, nxt), W.n_slots, cm, i >= n0, slot, lane);
     }
     unsigned long long wd = done;
 #pragma unroll
@@ -335,7 +366,7 @@ wf_march_spline_kernel(const __grid_constant__ KParams P, const __grid_constant_
     __shared__ unsigned s_pref[kMaxBricks + 1];
     __shared__ __align__(8) unsigned long long s_bar;
     const int lane = threadIdx.x & 31, cur = it & 1, nxt = cur ^ 1;
-    const unsigned n = W.cnt[cur];
+    const unsigned n = list_cnt(W, cur)[0];                 // one class: no split with bricks
     if (n == 0u) return;
     // the brick: quads 128-byte aligned, the header in the 16 bytes before them
     float4 *quads = reinterpret_cast<float4 *>((reinterpret_cast<uintptr_t>(smem_raw) + 16u + 127u) & ~uintptr_t(127));
@@ -412,7 +443,7 @@ wf_march_spline_kernel(const __grid_constant__ KParams P, const __grid_constant_
         }
         const unsigned em = __ballot_sync(kFull, valid && ended);
         const unsigned cm = __ballot_sync(kFull, valid && !ended);
-        warp_append(W.queue[cur], W.cnt + 2 + cur, em, slot, lane);
+        warp_append(W.queue[cur], queue_cnt(W, cur), em, slot, lane);
         brick_append(W, nxt, cm, key, slot, lane);
     }
     unsigned long long wd = done;
@@ -434,10 +465,11 @@ wf_event_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
     const int lane = threadIdx.x & 31;
     const bool init = it < 0;
     const int cur = init ? 1 : (it & 1), nxt = cur ^ 1;
-    const unsigned n = init ? unsigned(W.n_slots) : W.cnt[2 + cur];
-    if (!init && blockIdx.x == 0 && threadIdx.x == 0) {
-        W.cnt[cur] = 0u;          // consumed by march launch `it`
-        W.cnt[2 + nxt] = 0u;      // filled by march launch `it + 1`
+    const unsigned q0 = init ? unsigned(W.n_slots) : queue_cnt(W, cur)[0];
+    const unsigned n = init ? q0 : q0 + queue_cnt(W, cur)[1];
+    if (!init && blockIdx.x == 0 && threadIdx.x < 2) {
+        list_cnt(W, cur)[threadIdx.x] = 0u;     // consumed by march launch `it`
+        queue_cnt(W, nxt)[threadIdx.x] = 0u;    // filled by march launch `it + 1`
     }
     if (FK == FK_SPLINE && !init && blockIdx.x == 0)
         for (int b = threadIdx.x; b < W.nb; b += blockDim.x) W.bcnt[cur][b] = 0u;   // the brick lists too
@@ -447,8 +479,9 @@ wf_event_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
         const unsigned i = base + unsigned(lane);
         const bool valid = i < n;
         int st = ST_DONE, slot = 0, key = 0;
+        bool cls1 = false;
         if (valid) {
-            slot = init ? int(i) : W.queue[cur][i];
+            slot = init ? int(i) : two_class_at(W.queue[cur], q0, W.n_slots, i);
             Lane L;
             if (init) {
                 L.end = 0;
@@ -479,11 +512,12 @@ wf_event_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveP
             if (st == ST_MARCH) {
                 wf_store_lane(W, P, slot, L);
                 if (FK == FK_SPLINE && W.nb) key = spline_brick_of(P.field, W, L.mp);
+                cls1 = move_class(W, L.ctx);
             }
         }
         const unsigned mm = __ballot_sync(kFull, valid && st == ST_MARCH);
         if (FK == FK_SPLINE && W.nb) brick_append(W, nxt, mm, key, slot, lane);
-        else warp_append(W.list[nxt], W.cnt + nxt, mm, slot, lane);
+        else warp_append2(W.list[nxt], list_cnt(W, nxt), W.n_slots, mm, cls1, slot, lane);
     }
     flush_stats(S, P, lane);
 }
@@ -498,7 +532,7 @@ __global__ void __launch_bounds__(128, SMP_MIN_BLOCKS)
 wf_finish_kernel(const __grid_constant__ KParams P, const __grid_constant__ WaveParams W, int it) {
     extern __shared__ __align__(16) float4 smem_tab[];
     const int lane = threadIdx.x & 31, cur = it & 1;
-    const unsigned n = W.cnt[cur];
+    const unsigned n0 = list_cnt(W, cur)[0], n = n0 + list_cnt(W, cur)[1];
     const unsigned gid = blockIdx.x * blockDim.x + threadIdx.x, lanes = gridDim.x * blockDim.x;
     if (gid == 0 && n > lanes) atomicAdd(P.counters + CNT_LOST, (unsigned long long)(n - lanes));
     const float4 *tab = P.field.btab;
@@ -512,7 +546,7 @@ wf_finish_kernel(const __grid_constant__ KParams P, const __grid_constant__ Wave
     int st = ST_FETCH;
     L.inst = nullptr;
     if (gid < n) {
-        wf_load_lane(W, P, (FK == FK_SPLINE && W.nb) ? brick_slot(W, cur, gid) : W.list[cur][gid], L);
+        wf_load_lane(W, P, (FK == FK_SPLINE && W.nb) ? brick_slot(W, cur, gid) : two_class_at(W.list[cur], n0, W.n_slots, gid), L);
         st = ST_MARCH;
     }
     L.tab = (FK == FK_BATCH && L.inst) ? L.inst->field.btab : tab;

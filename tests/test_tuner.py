@@ -17,7 +17,7 @@ def test_tune_picks_a_candidate_caches_it_and_keeps_the_film():
     p = sb.Plan(s)
     t = p.tune(200_000)
     assert t.march_block in (128, 256) and t.slots_per_lane in (2, 4, 6, 8) and t.chunk in (64, 96, 128, 192)
-    assert t.trials == 17 and t.ms > 0 and t.paths_per_s > 0
+    assert t.trials == 19 and t.ms > 0 and t.paths_per_s > 0      # 16 + 1 at 256 threads + the two best again
     film, st = p.render(n)
     p.close()
     assert (st.march_block, st.slots_per_lane, st.chunk, st.tuned) == (t.march_block, t.slots_per_lane, t.chunk, 1)
