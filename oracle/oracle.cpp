@@ -537,7 +537,7 @@ template <typename R, typename A> struct Tracer {
     bool abort_cap = false, abort_nan = false;
     smp_photon_record *rec = nullptr;
     int n_splats = 0;
-    std::vector<A> *img = nullptr;   // thread-local film
+    A *img = nullptr;                // thread-local film (X*Y*Z)
 
     bool aborted() const { return abort_cap || abort_nan || u->exhausted; }
 
@@ -658,7 +658,7 @@ template <typename R, typename A> struct Tracer {
 
     void add_pixel(int x, int y, int z, A val) {              // scene.h:305-312, image.h:320-324
         if (img && x >= 0 && x < sc->X && y >= 0 && y < sc->Y && z >= 0 && z < sc->Z)
-            (*img)[size_t(z) * sc->X * sc->Y + size_t(y) * sc->X + x] += val;
+            img[size_t(z) * sc->X * sc->Y + size_t(y) * sc->X + x] += val;
     }
 
     // Scene::addEnergyToImage, scene.cpp:782-829
@@ -893,7 +893,7 @@ template <typename R, typename A>
 static int render_impl(const smp_scene_desc *sd, const smp_medium_desc *md, const smp_field_desc *fdesc,
                        const smp_render_opts *opts, int threads, int64_t first, int64_t n,
                        int64_t weight_photons, const float *uniforms, const int64_t *offsets,
-                       smp_photon_record *records, double *image_out) {
+                       smp_photon_record *records, double *image_out, A *thread_films = nullptr) {
     Scene<R> sc;
     sc.init(*sd);
     Field<R> fd;
@@ -904,7 +904,8 @@ static int render_impl(const smp_scene_desc *sd, const smp_medium_desc *md, cons
     R weight = sc.Li * sc.fresnel_trans / R(weight_photons);   // photon.h:76-80
     const size_t npix = size_t(sc.X) * sc.Y * sc.Z;
     int nt = threads > 0 ? threads : omp_get_max_threads();
-    std::vector<std::vector<A>> imgs(nt, std::vector<A>(image_out ? npix : 0, A(0)));
+    // per-thread films merged at the end (renderImage, photon.cpp:290-291, 337), or the caller's
+    std::vector<std::vector<A>> imgs(nt, std::vector<A>(image_out && !thread_films ? npix : 0, A(0)));
     int64_t cap = opts->step_cap > 0 ? opts->step_cap : int64_t(10000000);
 #pragma omp parallel num_threads(nt)
     {
@@ -930,7 +931,7 @@ static int render_impl(const smp_scene_desc *sd, const smp_medium_desc *md, cons
         tr.precision0 = fdesc->precision;
         tr.step_cap = cap;
         tr.weight = weight;
-        tr.img = image_out ? &imgs[tid] : nullptr;
+        tr.img = thread_films ? thread_films + size_t(tid) * npix : (image_out ? imgs[tid].data() : nullptr);
         Uniforms un;
 #pragma omp for schedule(dynamic, 64)
         for (int64_t k = 0; k < n; ++k) {
@@ -955,7 +956,7 @@ static int render_impl(const smp_scene_desc *sd, const smp_medium_desc *md, cons
             tr.photon(*fdesc);
         }
     }
-    if (image_out) {
+    if (image_out && !thread_films) {
         for (size_t j = 0; j < npix; ++j) {
             A v = 0;
             for (int t = 0; t < nt; ++t) v += imgs[t][j];
@@ -1026,6 +1027,26 @@ int orc_render(const smp_scene_desc *scene, const smp_medium_desc *medium, const
                                                uniforms, offsets, records, image_out);
     return orc::render_impl<float, float>(scene, medium, field, opts, threads, first, n, weight_photons,
                                           uniforms, offsets, records, image_out);
+}
+
+// The same trace with the film accumulated into caller-owned per-thread films: `threads` films of
+// X*Y*Z elements (double for real_bits 64 or SMP_PREC_MIXED, float otherwise), zeroed and merged by
+// the caller, so that a long render timed in steps keeps its thread films across the steps as the
+// reference's renderImage keeps its per-thread images across its photon loop. Philox or SFMT
+// streams (no injected uniforms, no records).
+int orc_render_films(const smp_scene_desc *scene, const smp_medium_desc *medium, const smp_field_desc *field,
+                     const smp_render_opts *opts, int real_bits, int threads, int64_t first, int64_t n,
+                     int64_t weight_photons, void *thread_films) {
+    if (!scene || !medium || !field || !opts || n < 0 || weight_photons <= 0 || threads <= 0 || !thread_films)
+        return SMP_ERR_BAD_ARG;
+    if (real_bits == 64)
+        return orc::render_impl<double, double>(scene, medium, field, opts, threads, first, n, weight_photons, nullptr,
+                                                nullptr, nullptr, nullptr, static_cast<double *>(thread_films));
+    if (opts->precision == SMP_PREC_MIXED)
+        return orc::render_impl<float, double>(scene, medium, field, opts, threads, first, n, weight_photons, nullptr,
+                                               nullptr, nullptr, nullptr, static_cast<double *>(thread_films));
+    return orc::render_impl<float, float>(scene, medium, field, opts, threads, first, n, weight_photons, nullptr,
+                                          nullptr, nullptr, nullptr, static_cast<float *>(thread_films));
 }
 
 // ---- single primitives (float, the reference's build), for pinning against its compiled code -------
