@@ -219,6 +219,23 @@ class ThreadFilms:
         return img, time.perf_counter() - t0
 
 
+def fp32_peak_from_clock(device: int) -> dict:
+    """The FP32 peak from the chip's figures, beside the live-measured one: SMs x 128 FP32 lanes x
+    2 FLOP (FMA) x the maximum SM clock (nvidia-smi clocks.max.sm)."""
+    import torch
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    mhz = None
+    try:
+        out = subprocess.run(["nvidia-smi", "-i", str(device), "--query-gpu=clocks.max.sm", "--format=csv,noheader,nounits"],
+                             capture_output=True, text=True, timeout=20).stdout.strip()
+        mhz = float(out.splitlines()[0])
+    except Exception:
+        mhz = None
+    if not mhz:
+        return {"tflops": None, "how": "clocks.max.sm unavailable"}
+    return {"tflops": sms * 128 * 2 * mhz * 1e6 / 1e12, "how": f"{sms} SMs x 128 FP32 lanes x 2 x {mhz:.0f} MHz"}
+
+
 def cpu_trace(n: int, first: int, films: ThreadFilms) -> float:
     """Trace n photons of the workload with the CPU restatement on films.threads host threads, each
     accumulating its splats into its own film; returns seconds (wall)."""
@@ -427,6 +444,10 @@ def run_ours(args):
                 "flop_per_er_step": fps, "er_steps_per_launch": march_steps / n_march,
                 "march_kernel_share_of_step_time": march_ms / ms,
                 "peak_source": "FP32 FMA throughput measured live on this GPU (smp_fp32_peak)"}
+        clk_peak = fp32_peak_from_clock(local)
+        roof["peak_clock_derived"] = clk_peak["tflops"]
+        roof["peak_clock_derived_how"] = clk_peak["how"]
+        roof["frac_of_clock_derived"] = achieved / clk_peak["tflops"] if clk_peak["tflops"] else None
         e2e = run_e2e(args, setup, min(args.steps, 3), per_step)
         out = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
