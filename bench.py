@@ -53,6 +53,9 @@ def parse():
                          "of the central 32x32 px ROI throughput")
     ap.add_argument("--sweep-scale", type=float, default=1.0,
                     help="sweep: multiply every instance's photon budget")
+    ap.add_argument("--step-budget", type=float, default=2e-3,
+                    help="sweep: relative image RMSE the step-size autotuner may spend per instance, against "
+                         "the instance's film at its own 0.01 mm step on the same photons")
     return ap.parse_args()
 
 
@@ -544,23 +547,66 @@ def run_e2e(args, setup, steps: int, per_step: int) -> dict:
             "call": "smp_render (one-shot plan, host film) per step, wall clock"}
 
 
+def sweep_image_check(setup, insts, steps, n: int, threads: int) -> list:
+    """The sweep's image check (the oracle as the checker): for the instances given, photons 0..n-1 on
+    their own Philox streams rendered by the batched form at its tuned step, by the batched form at
+    the nominal 0.01 mm step and by the plain kernel (FP32, nominal step), each against the FP64
+    restatement on the CPU at the nominal step; relative RMSE sqrt(sum (film - ref)^2 / sum ref^2)."""
+    import dataclasses
+    lib = _oracle_lib(fast=False)
+    out = []
+    for i, h in steps:
+        inst = dict(insts[i], n_photons=n)
+        over = {k: v for k, v in inst.items() if k != "n_photons"}
+        s = dataclasses.replace(setup, **over)
+        tuned, _ = sb.render_batch(setup, [dict(inst, er_stepsize=float(h))])
+        nominal, _ = sb.render_batch(setup, [inst])
+        plain, _ = sb.render(dataclasses.replace(s, kernel=L.KERNEL_PLAIN), n)
+        sc, md, fd, op = s.descs()
+        ref = np.zeros(s.film_shape(), dtype=np.float64)
+        rc = lib.orc_render(C.byref(sc), C.byref(md), C.byref(fd), C.byref(op), 64, threads, 0, n, n, None, None,
+                            None, C.c_void_p(ref.ctypes.data))
+        assert rc == 0
+
+        def rel(a):
+            return float(np.sqrt(((a - ref) ** 2).sum() / (ref ** 2).sum()))
+        out.append({"instance": i, "mode": inst["mode"], "f_u": inst["f_u"], "n_max": inst["n_max"],
+                    "step_m": float(h), "step_multiple": round(float(h) / setup.er_stepsize),
+                    "batched_tuned_step": rel(tuned[0]), "batched_nominal_step": rel(nominal[0]),
+                    "plain_fp32_nominal_step": rel(plain)})
+    return out
+
+
 def run_sweep(args):
     """The batched sweep (256 cylindrical-transducer instances over the plain small scene, budgets
     log-uniform 1e5-1e7, seed 2) rendered in one slot pool with smp_render_batch, against the same
-    instances rendered one smp_render call each (the reference's per-configuration loop). Both
-    host-timed end to end (films read back to host memory); one JSON line."""
+    instances rendered one smp_render call each (the reference's per-configuration loop) and with the
+    plain kernel. The batched form takes each instance's ER step from the step-size autotuner
+    (smp_batch_tune_steps, within --step-budget of the instance's film at its own step); the same
+    sweep at the nominal step is timed beside it. All host-timed end to end (films read back to host
+    memory); one JSON line."""
     import torch
     torch.cuda.set_device(0)
     setup, insts = sb.config_batch_sweep(n_inst=256, seed=2, scale=args.sweep_scale)
     total = sum(i["n_photons"] for i in insts)
-    # warm-up: module load, first allocations, and the tuner's trials (2e6 photons of this scene),
-    # whose schedule the timed sweep takes from the process-wide cache
+    # warm-up: module load, first allocations, and the schedule tuner's trials (2e6 photons of this
+    # scene), whose schedule the timed sweeps take from the process-wide cache (keyed by the scene and
+    # the first instance's field and step, so once for the nominal and once for the tuned steps)
     sb.render_batch(setup, insts[:16])
+    w_steps, _, _ = sb.tune_batch_steps(setup, insts[:16], args.step_budget, n_sample=20000)
+    sb.render_batch(setup, [dict(inst, er_stepsize=float(h)) for inst, h in zip(insts[:16], w_steps)])
     clocks = ClockSampler(0)
     clocks.start()
     t0 = time.perf_counter()
     films, st = sb.render_batch(setup, insts)          # tunes first (cached after the warm-up's call)
     t_batch = time.perf_counter() - t0
+    # the batched form: the autotuner's step per instance (its trial renders timed as part of it)
+    t0 = time.perf_counter()
+    steps, rmse, rounds = sb.tune_batch_steps(setup, insts, args.step_budget, n_sample=20000)
+    t_tune = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    films_t, st_t = sb.render_batch(setup, [dict(inst, er_stepsize=float(h)) for inst, h in zip(insts, steps)])
+    t_tuned = time.perf_counter() - t0
     import dataclasses
     t0 = time.perf_counter()
     serial_sum = 0.0
@@ -569,7 +615,7 @@ def run_sweep(args):
         img, _ = sb.render(dataclasses.replace(setup, **over), inst["n_photons"])
         serial_sum += float(img.sum())
     t_serial = time.perf_counter() - t0
-    # the plain kernel (one thread per photon, FP32) over every 8th instance, one render each
+    # the plain kernel (one thread per photon, FP32, nominal step) over every 8th instance, one render each
     t0 = time.perf_counter()
     plain_photons = 0
     for i, inst in enumerate(insts[::8]):
@@ -578,25 +624,45 @@ def run_sweep(args):
         plain_photons += inst["n_photons"]
     t_plain = time.perf_counter() - t0
     clk = clocks.stop()
+    mults = steps / setup.er_stepsize
+    plain_rate = plain_photons / t_plain
+    # image check against the FP64 oracle: the instance with the smallest step multiple among the
+    # hardest fields (largest n_max x f), the one with the largest multiple, and instance 0
+    hard = max(range(len(insts)), key=lambda i: insts[i]["n_max"] * insts[i]["f_u"])
+    big = int(np.argmax(mults))
+    check = sweep_image_check(setup, insts, [(i, steps[i]) for i in sorted({hard, big, 0})], 10000,
+                              os.cpu_count() or 1)
+    hist = {str(m): int((np.rint(mults) == m).sum()) for m in (1, 2, 3, 4, 6, 8, 12, 16, 24, 32)}
     out = {
-        "metric": METRIC, "value": total / t_batch, "unit": METRIC, "n_gpus": 1, "steps": 1, "warmup": 1,
-        "ms_per_step": t_batch * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "fp32", "data": "synthetic",
+        "metric": METRIC, "value": total / (t_tuned + t_tune), "unit": METRIC, "n_gpus": 1, "steps": 1,
+        "warmup": 1, "ms_per_step": (t_tuned + t_tune) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
         "config": {"workload": "batched sweep: 256 Bessel instances (n_max U[0,2e-3], f U[0.5,2] MHz, mode 0-2, "
                                "duty U[1,100]%, budgets log-uniform 1e5-1e7 x scale), medium and film of the "
-                               "plain small configuration, seed 2", "photons": total, "scale": args.sweep_scale,
-                   "film": list(setup.film_shape())},
+                               "plain small configuration, seed 2; ER step per instance from the step-size "
+                               "autotuner (its trial renders inside the timed region)", "photons": total,
+                   "scale": args.sweep_scale, "film": list(setup.film_shape()), "step_budget": args.step_budget},
+        "step_tuner": {"seconds": t_tune, "rounds": rounds, "sample_photons_per_instance": 20000,
+                       "multiples_histogram": hist, "mean_multiple_by_photons":
+                           float(sum(m * i["n_photons"] for m, i in zip(mults, insts)) / total),
+                       "max_measured_rmse": float(rmse.max())},
+        "tuned_render_seconds": t_tuned, "er_steps_per_s": st_t.er_steps / t_tuned, "er_steps": st_t.er_steps,
+        "nominal_step": {"value": total / t_batch, "unit": METRIC, "seconds": t_batch, "er_steps": st.er_steps,
+                         "speedup_vs_plain": (total / t_batch) / plain_rate,
+                         "call": "smp_render_batch with every instance at 0.01 mm"},
         "serial": {"value": total / t_serial, "unit": METRIC, "seconds": t_serial,
-                   "call": "one smp_render per instance, host film"},
-        "batch_seconds": t_batch, "speedup_vs_serial": t_serial / t_batch,
-        "plain": {"value": plain_photons / t_plain, "unit": METRIC, "seconds": t_plain, "photons": plain_photons,
-                  "call": "one smp_render per instance with the plain kernel (one thread per photon, fp32), every "
-                          "8th instance (32 of 256)"},
-        "speedup_vs_plain": (total / t_batch) / (plain_photons / t_plain),
+                   "call": "one smp_render per instance, host film, nominal step"},
+        "speedup_vs_serial": t_serial / (t_tuned + t_tune),
+        "plain": {"value": plain_rate, "unit": METRIC, "seconds": t_plain, "photons": plain_photons,
+                  "call": "one smp_render per instance with the plain kernel (one thread per photon, fp32, "
+                          "0.01 mm step), every 8th instance (32 of 256)"},
+        "speedup_vs_plain": (total / (t_tuned + t_tune)) / plain_rate,
+        "image_rmse_vs_fp64": {"photons": 10000, "reference": "FP64 CPU restatement at the nominal 0.01 mm step, "
+                                                              "same Philox photons", "instances": check},
         "film_sum_relative_difference": abs(float(films.sum()) - serial_sum) / max(serial_sum, 1e-300),
-        "er_steps_per_s": st.er_steps / t_batch, "gpu_launches": st.launches, "clocks": clk,
-        "schedule": {"march_block": st.march_block, "slots_per_lane": st.slots_per_lane, "chunk": st.chunk,
-                     "tuned": bool(st.tuned), "cuda_graph": True},
+        "gpu_launches": st_t.launches, "clocks": clk,
+        "schedule": {"march_block": st_t.march_block, "slots_per_lane": st_t.slots_per_lane, "chunk": st_t.chunk,
+                     "tuned": bool(st_t.tuned), "cuda_graph": True},
     }
     print(json.dumps(out), flush=True)
 

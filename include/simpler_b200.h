@@ -22,6 +22,7 @@
  *   smp_texture_cdf                <- area_textured_source texture CDF      renderer/src/area_textured_source.cpp:41-45
  *   smp_render_batch               <- the serial per-configuration loops    renderer/pybindFiles/tests/FUS_configurations.ipynb
  *                                     (one renderImage per configuration)   (cells at lines 591-603, 713-725)
+ *   smp_batch_tune_steps           <- no counterpart: the reference's ER step is a fixed setting
  *   smp_render_adjoint /           <- no counterpart: the reference has forward-mode tangents of
  *   smp_plan_adjoint                  single leapfrog steps only (er_derivativestep scene.cpp:351-359,
  *                                     bessel_HessianRIF :259-320, Spline::hessian spline.h:359-413),
@@ -340,6 +341,24 @@ int smp_spline_prefilter(const float *samples, const int32_t n[3], float *coeff_
 int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *instances,
                      int32_t n_inst, const smp_render_opts *opts,
                      double *images_out, smp_stats *stats_out);
+
+/* Step-size autotuner for a batched sweep (no counterpart in the reference, whose ER step is a fixed
+   setting). For each instance it renders photons [0, min(n_photons, n_sample)) at the instance's own
+   field.er_stepsize (its reference film) and at multiples of that step (2, 3, 4, 6, 8, 12, 16, 24 or
+   32, none above an eighth of the instance's ultrasound wavelength speed_u / f_u) on the same Philox
+   photons, and keeps the largest multiple whose film stays within rmse_budget relative RMSE
+   (sqrt(sum (film - ref)^2 / sum ref^2)) of the reference film. It tries the largest allowed
+   multiple first and, where that misses, bisects between the multiples known to pass and to miss
+   (the error grows with the step); each round is one batched render of the instances still
+   searching. An instance with no photons or an empty reference film keeps its own step.
+   steps_out[i] receives instance i's chosen er_stepsize; rmse_out[i] (may be NULL) the relative RMSE
+   measured at that step (0 where the instance kept its own); rounds_out (may be NULL) the number of
+   batched renders. The budget is against this library's own render at the nominal step: the image
+   error against an exact solution adds the nominal step's own error. Set
+   instances[i].field.er_stepsize = steps_out[i] and call smp_render_batch. At most 65535 instances. */
+int smp_batch_tune_steps(const smp_scene_desc *scene, const smp_instance_desc *instances,
+                         int32_t n_inst, const smp_render_opts *opts, int64_t n_sample,
+                         double rmse_budget, double *steps_out, double *rmse_out, int32_t *rounds_out);
 
 /* Rendering without allocation -- no counterpart in the reference. For callers that cannot call
    cudaMalloc (device memory owned by the host application's allocator or budget, code that must not

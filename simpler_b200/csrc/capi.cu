@@ -335,14 +335,17 @@ static float float_below(double x) {
     return f;
 }
 // traceTillBlock's step sizes: h0 and each refinement's current_stepsize / 10 in float
+static void step_table(double er_stepsize, float *tab) {
+    tab[0] = float(er_stepsize);
+    for (int i = 1; i <= SMP_MAX_REFINE; ++i) {
+        volatile float q = tab[i - 1] / 10.0f;           // one IEEE float division per level
+        tab[i] = q;
+    }
+}
 static void set_step_sizes(KParams &k, const smp_field_desc &f) {
     k.h0 = float(f.er_stepsize);
     k.precision = std::max(0, std::min(int(f.precision), SMP_MAX_REFINE));
-    k.cur_tab[0] = k.h0;
-    for (int i = 1; i <= SMP_MAX_REFINE; ++i) {
-        volatile float q = k.cur_tab[i - 1] / 10.0f;     // one IEEE float division per level
-        k.cur_tab[i] = q;
-    }
+    step_table(f.er_stepsize, k.cur_tab);
 }
 
 static void set_box_thresholds(KParams &k) {
@@ -1489,11 +1492,19 @@ int smp_fp32_peak(int device, double *tflops_out) {
 
 // The batched sweep: every instance's photons are one index range of a single photon stream, so
 // the slot pool mixes instances as it refills and the whole sweep has one tail. Each instance's
-// field, medium, weight, seed and film travel with its photons (Inst records); the scene and the
-// film shape are shared. Photon j of instance i draws the Philox stream (seed_i, j), so each
-// instance's film is the one a single-instance render with that seed produces.
-int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *instances, int32_t n_inst,
-                     const smp_render_opts *opts, double *images_out, smp_stats *stats_out) {
+// field, ER step, medium, weight, seed and film travel with its photons (Inst records); the scene,
+// the film shape and the number of refinement levels are shared. Photon j of instance i draws the
+// Philox stream (seed_i, j), so each instance's film is the one a single-instance render with that
+// seed produces.
+//
+// batch_run renders the sweep into n_inst consecutive device films (float, or double in the mixed
+// form; *film_bytes each), which it allocates and hands to the caller (*d_films_out, to cudaFree).
+// schedule_tune: run the slot pool's autotuner first (trials on the sweep's first photons, cached
+// per process).
+static int batch_run(const smp_scene_desc *scene, const smp_instance_desc *instances, int32_t n_inst,
+                     const smp_render_opts *opts, bool schedule_tune, void **d_films_out, size_t *film_bytes,
+                     smp_stats *stats_out) {
+    *d_films_out = nullptr;
     if (!scene || !instances || !opts || n_inst <= 0) return set_error(SMP_ERR_BAD_ARG, "bad batch arguments");
     if (opts->rng != SMP_RNG_PHILOX) return set_error(SMP_ERR_UNSUPPORTED, "a batched sweep draws from Philox");
     std::vector<int> fks(n_inst);
@@ -1506,12 +1517,16 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
         if (fks[i] > FK_BESSEL2)
             return set_error(SMP_ERR_UNSUPPORTED, "instance %d: a batched sweep renders Bessel fields of order 0-2", i);
         if (instances[i].n_photons < 0) return set_error(SMP_ERR_BAD_ARG, "instance %d: negative photon budget", i);
+        if (instances[i].field.precision != instances[0].field.precision)
+            return set_error(SMP_ERR_BAD_ARG, "instance %d: a batched sweep shares one number of refinement levels "
+                             "(%d, instance 0 has %d)", i, instances[i].field.precision, instances[0].field.precision);
         total += instances[i].n_photons;
     }
     smp_plan *p = nullptr;
     int rc = smp_plan_create(scene, &instances[0].medium, &instances[0].field, opts, &p);
     if (rc) return rc;
     const size_t px = p->film_elems, bpp = p->kp.fp64 ? 8 : 4;
+    *film_bytes = px * bpp;
     // host side of the per-instance records and tables
     std::vector<Inst> hi(n_inst);
     std::vector<long long> first(size_t(n_inst) + 1, 0);
@@ -1549,6 +1564,8 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
         I.weight = d.n_photons > 0 ? photon_weight(*scene, d.n_photons) : 0.0f;
         I.large_dist = sensor_march_budget(*opts, I.sigma_t);
         I.seed = d.seed;
+        I.h0 = float(d.field.er_stepsize);                      // each instance marches with its own step
+        step_table(d.field.er_stepsize, I.cur_tab);
         first[i + 1] = first[i] + d.n_photons;
     }
     Inst *d_insts = nullptr;
@@ -1581,7 +1598,7 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
         // the schedule from the tuner (trials on the sweep's first photons, cached per process),
         // and each batch of march/event launches replayed as one CUDA graph once it is fixed
         const char *tune_env = std::getenv("SMP_TUNE");
-        if (!rc && total > 0 && p->kernel == SMP_KERNEL_POOL && !(tune_env && std::atoi(tune_env) == 0)) {
+        if (!rc && schedule_tune && total > 0 && p->kernel == SMP_KERNEL_POOL && !(tune_env && std::atoi(tune_env) == 0)) {
             smp_tuning tt;
             rc = smp_plan_tune(p, std::min<long long>(total, 2000000LL), &tt);
             if (!rc) {
@@ -1595,16 +1612,6 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
         // the weight argument is unused: each instance carries its own Li T / N
         if (!rc && total > 0) rc = launch(p, 0, total, 1, nullptr, nullptr, nullptr, nullptr);
         int rs = rc ? rc : collect_stats(p);
-        if (!rc && images_out) {
-            if (p->kp.fp64) {
-                e = cudaMemcpy(images_out, d_films, px * 8 * size_t(n_inst), cudaMemcpyDeviceToHost);
-            } else {
-                std::vector<float> h(px * size_t(n_inst));           // FP32 films, widened on the host
-                e = cudaMemcpy(h.data(), d_films, h.size() * 4, cudaMemcpyDeviceToHost);
-                for (size_t j = 0; j < h.size(); ++j) images_out[j] = double(h[j]);
-            }
-            if (e != cudaSuccess) rc = set_error(SMP_ERR_CUDA, "batch films: %s", cudaGetErrorString(e));
-        }
         if (stats_out) *stats_out = p->stats;
         if (!rc) rc = rs;
     }
@@ -1612,10 +1619,156 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
     cudaFree(d_insts);
     cudaFree(d_first);
     cudaFree(d_tabs);
-    cudaFree(d_films);
+    if (rc) cudaFree(d_films);
+    else *d_films_out = d_films;
     smp_plan_destroy(p);
     g_last_error = err;
     return rc;
+}
+
+int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *instances, int32_t n_inst,
+                     const smp_render_opts *opts, double *images_out, smp_stats *stats_out) {
+    void *d_films = nullptr;
+    size_t fb = 0;
+    int rc = batch_run(scene, instances, n_inst, opts, true, &d_films, &fb, stats_out);
+    if (rc) return rc;
+    if (images_out) {
+        cudaError_t e;
+        if (opts->precision == SMP_PREC_MIXED) {
+            e = cudaMemcpy(images_out, d_films, fb * size_t(n_inst), cudaMemcpyDeviceToHost);
+        } else {
+            std::vector<float> h(fb / 4 * size_t(n_inst));           // FP32 films, widened on the host
+            e = cudaMemcpy(h.data(), d_films, h.size() * 4, cudaMemcpyDeviceToHost);
+            for (size_t j = 0; j < h.size(); ++j) images_out[j] = double(h[j]);
+        }
+        if (e != cudaSuccess) rc = set_error(SMP_ERR_CUDA, "batch films: %s", cudaGetErrorString(e));
+    }
+    cudaFree(d_films);
+    return rc;
+}
+
+// Per instance i (blockIdx.y): sum (a - r)^2 and sum r^2 over its film of px pixels (float, or
+// double when fp64), accumulated in double into acc[2i], acc[2i + 1].
+__global__ void film_diff_kernel(const void *a, const void *r, size_t px, int fp64, double *acc) {
+    __shared__ double sd[32], sr[32];
+    const size_t base = size_t(blockIdx.y) * px;
+    double d2 = 0.0, r2 = 0.0;
+    for (size_t j = size_t(blockIdx.x) * blockDim.x + threadIdx.x; j < px; j += size_t(gridDim.x) * blockDim.x) {
+        const double av = fp64 ? static_cast<const double *>(a)[base + j] : double(static_cast<const float *>(a)[base + j]);
+        const double rv = fp64 ? static_cast<const double *>(r)[base + j] : double(static_cast<const float *>(r)[base + j]);
+        d2 += (av - rv) * (av - rv);
+        r2 += rv * rv;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        d2 += __shfl_down_sync(0xffffffffu, d2, o);
+        r2 += __shfl_down_sync(0xffffffffu, r2, o);
+    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { sd[w] = d2; sr[w] = r2; }
+    __syncthreads();
+    if (w == 0) {
+        d2 = lane < int(blockDim.x >> 5) ? sd[lane] : 0.0;
+        r2 = lane < int(blockDim.x >> 5) ? sr[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            d2 += __shfl_down_sync(0xffffffffu, d2, o);
+            r2 += __shfl_down_sync(0xffffffffu, r2, o);
+        }
+        if (lane == 0) {
+            atomicAdd(acc + 2 * blockIdx.y, d2);
+            atomicAdd(acc + 2 * blockIdx.y + 1, r2);
+        }
+    }
+}
+
+// Step-size autotuner of a batched sweep. Photons [0, min(n_photons_i, n_sample)) of every
+// instance are rendered at the instance's own er_stepsize (its reference film), and then at
+// multiples of it from kStepMults, at most an eighth of the instance's ultrasound wavelength: first
+// the largest allowed one, and, when that misses the budget, by bisection between the largest
+// multiple known to pass and the smallest known to miss (the error grows with the step). Every
+// round is one batched render of the instances still searching; an instance keeps the largest
+// multiple whose film stayed within rmse_budget relative RMSE of its reference film on the same
+// photons, or its own step when its reference film is empty.
+int smp_batch_tune_steps(const smp_scene_desc *scene, const smp_instance_desc *instances, int32_t n_inst,
+                         const smp_render_opts *opts, int64_t n_sample, double rmse_budget, double *steps_out,
+                         double *rmse_out, int32_t *rounds_out) {
+    if (!scene || !instances || !opts || n_inst <= 0 || !steps_out) return set_error(SMP_ERR_BAD_ARG, "bad batch arguments");
+    if (n_inst > 65535) return set_error(SMP_ERR_BAD_ARG, "the step tuner takes at most 65535 instances");
+    if (n_sample <= 0) return set_error(SMP_ERR_BAD_ARG, "n_sample must be positive");
+    if (!(rmse_budget > 0.0)) return set_error(SMP_ERR_BAD_ARG, "rmse_budget must be positive");
+    static const int kStepMults[] = {2, 3, 4, 6, 8, 12, 16, 24, 32};
+    const int n_mult = int(sizeof(kStepMults) / sizeof(kStepMults[0]));
+    std::vector<smp_instance_desc> trial(instances, instances + n_inst);
+    // per instance: the allowed multiples are kStepMults[0 .. lim); index pass_i passes (-1: the
+    // instance's own step), index miss_i misses (lim: none known), try_i is this round's
+    std::vector<int> pass(n_inst, -1), miss(n_inst, 0), tr(n_inst, -1);
+    std::vector<double> rmse(n_inst, 0.0);
+    for (int i = 0; i < n_inst; ++i) {
+        const smp_field_desc &f = instances[i].field;
+        const double lambda = f.speed_u / f.f_u;
+        int lim = 0;
+        while (lim < n_mult && f.er_stepsize * kStepMults[lim] <= lambda / 8.0) ++lim;
+        miss[i] = instances[i].n_photons > 0 ? lim : 0;           // nothing to search without photons
+        trial[i].n_photons = std::min<int64_t>(instances[i].n_photons, n_sample);
+    }
+    int rc = check_device(opts->device);
+    if (rc) return rc;
+    void *d_ref = nullptr, *d_try = nullptr;
+    double *d_acc = nullptr;
+    size_t fb = 0;
+    int rounds = 0;
+    rc = batch_run(scene, trial.data(), n_inst, opts, false, &d_ref, &fb, nullptr);
+    ++rounds;
+    const int fp64 = opts->precision == SMP_PREC_MIXED;
+    const size_t px = fb / (fp64 ? 8 : 4);
+    std::vector<double> acc(2 * size_t(n_inst));
+    if (!rc) {
+        cudaError_t e = cudaMalloc(&d_acc, acc.size() * sizeof(double));
+        if (e != cudaSuccess) rc = set_error(SMP_ERR_OOM, "tuner buffers: %s", cudaGetErrorString(e));
+    }
+    for (bool first = true; !rc; first = false) {
+        bool any = false;
+        for (int i = 0; i < n_inst; ++i) {
+            tr[i] = -1;
+            if (miss[i] - pass[i] > 1) tr[i] = first ? miss[i] - 1 : (pass[i] + miss[i]) / 2;
+            trial[i].field.er_stepsize = instances[i].field.er_stepsize * (tr[i] >= 0 ? kStepMults[tr[i]] : 1);
+            trial[i].n_photons = tr[i] >= 0 ? std::min<int64_t>(instances[i].n_photons, n_sample) : 0;
+            any = any || tr[i] >= 0;
+        }
+        if (!any) break;
+        rc = batch_run(scene, trial.data(), n_inst, opts, false, &d_try, &fb, nullptr);
+        ++rounds;
+        if (rc) break;
+        cudaError_t e = cudaMemset(d_acc, 0, acc.size() * sizeof(double));
+        if (e == cudaSuccess) {
+            film_diff_kernel<<<dim3(64, unsigned(n_inst)), 256>>>(d_try, d_ref, px, fp64, d_acc);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpy(acc.data(), d_acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost);
+        cudaFree(d_try);
+        d_try = nullptr;
+        if (e != cudaSuccess) { rc = set_error(SMP_ERR_CUDA, "tuner films: %s", cudaGetErrorString(e)); break; }
+        for (int i = 0; i < n_inst; ++i) {
+            if (tr[i] < 0) continue;
+            if (!(acc[2 * i + 1] > 0.0)) { miss[i] = pass[i] + 1; continue; }   // empty reference film: keep its step
+            const double r = std::sqrt(acc[2 * i] / acc[2 * i + 1]);
+            if (r <= rmse_budget) { pass[i] = tr[i]; rmse[i] = r; }
+            else miss[i] = tr[i];
+        }
+    }
+    std::string err = g_last_error;
+    cudaFree(d_ref);
+    cudaFree(d_try);
+    cudaFree(d_acc);
+    g_last_error = err;
+    if (rc) return rc;
+    for (int i = 0; i < n_inst; ++i) {
+        steps_out[i] = instances[i].field.er_stepsize * (pass[i] >= 0 ? kStepMults[pass[i]] : 1);
+        if (rmse_out) rmse_out[i] = pass[i] >= 0 ? rmse[i] : 0.0;
+    }
+    if (rounds_out) *rounds_out = rounds;
+    return SMP_OK;
 }
 
 // ---- adjoint ------------------------------------------------------------------------------------

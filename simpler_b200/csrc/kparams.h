@@ -56,8 +56,11 @@ struct FieldParams {
     float grad_bound;       // bound on |grad n|_1 anywhere (0: unknown)
 };
 
-// One instance of a batched sweep: its field, medium, photon weight, film and seed. The scene
-// (box, source, camera, film shape) is shared by all instances.
+#define SMP_MAX_REFINE 39
+
+// One instance of a batched sweep: its field, ER step, medium, photon weight, film and seed. The
+// scene (box, source, camera, film shape) and the number of refinement levels are shared by all
+// instances.
 struct Inst {
     FieldParams field;
     float sigma_t, albedo, mfp, g;
@@ -65,9 +68,9 @@ struct Inst {
     float large_dist;       // movePhotonTillSensor budget for this sigma_t
     void *film;             // this instance's film (X*Y*Z, float or double)
     unsigned long long seed;
+    float h0;               // this instance's ER step
+    float cur_tab[SMP_MAX_REFINE + 1];   // its refinement steps, as KParams::cur_tab
 };
-
-#define SMP_MAX_REFINE 39
 
 struct KParams {
     // medium box (block.cpp)

@@ -358,16 +358,25 @@ __device__ __forceinline__ bool gen_ray(Lane &L, const KParams &P, float3 &pos, 
 }
 
 // ---- the traceTillBlock step ----------------------------------------------------------------
+// the photon's ER step and refinement steps: its instance's in a batched sweep, else the plan's
+template <int FK, class S>
+__device__ __forceinline__ float step_h0(const S &L, const KParams &P) { return FK == FK_BATCH ? L.inst->h0 : P.h0; }
+template <int FK, class S>
+__device__ __forceinline__ const float *step_tab(const S &L, const KParams &P) {
+    return FK == FK_BATCH ? L.inst->cur_tab : P.cur_tab;
+}
+
 template <int FK>
 __device__ __forceinline__ void begin_march(Lane &L, const KParams &P, float dlimit, bool eval) {
     if (eval) Field<FK>::eval(field_of<FK>(L, P), L.tab, L.mp, L.s, L.mn, L.mg);
+    const float h0 = step_h0<FK>(L, P);
     L.dist_acc = 0.0f;
     L.dlimit = dlimit;
-    L.cur = P.h0;
-    L.hh = 0.5f * P.h0;
-    L.cur_d = double(P.h0);
+    L.cur = h0;
+    L.hh = 0.5f * h0;
+    L.cur_d = double(h0);
     L.prec = P.precision;
-    L.stop = int(min((long long)L.steps + (long long)steps_for(dlimit, P.h0), (long long)P.step_cap));
+    L.stop = int(min((long long)L.steps + (long long)steps_for(dlimit, h0), (long long)P.step_cap));
     L.mtotf = float(L.mtot);
 }
 // a march with no steps ends at once (traceTillBlock's maxsteps <= 0)
@@ -419,7 +428,7 @@ __device__ __forceinline__ bool march_step(S &L, const KParams &P) {
         L.mp = p; L.md = d2; L.mn = n2; L.mg = g2;
         return true;
     }
-    L.cur = P.cur_tab[P.precision - L.prec];      // restore (mp, md unchanged) and refine: cur / 10
+    L.cur = step_tab<FK>(L, P)[P.precision - L.prec];   // restore (mp, md unchanged) and refine: cur / 10
     L.hh = 0.5f * L.cur;
     L.cur_d = double(L.cur);
     L.stop = min(L.steps + 10, P.step_cap);       // maxsteps = 11 from i = 0: ten more steps

@@ -110,33 +110,54 @@ class Plan:
             pass
 
 
+def _instance_descs(setup: Setup, instances: list):
+    import dataclasses
+    n = len(instances)
+    arr = (L.InstanceDesc * n)()
+    for i, inst in enumerate(instances):
+        over = {k: v for k, v in inst.items() if k not in ("n_photons", "seed")}
+        s = dataclasses.replace(setup, **over)
+        arr[i].field = s.field_desc()
+        arr[i].medium = s.medium_desc()
+        arr[i].n_photons = int(inst["n_photons"])
+        arr[i].seed = int(inst.get("seed", 0))
+    return arr
+
+
 def render_batch(setup: Setup, instances: list) -> tuple[np.ndarray, L.Stats]:
     """A sweep of many field / medium configurations over one scene, in one slot pool.
 
     `instances` is a list of dicts: any Setup field or medium attribute to override
-    (mode, n_max, n_clip, f_u, speed_u, phi_min, phi_max, sigma_t, albedo, g, ...) plus
-    `n_photons` and `seed`. Returns the films as an (n_inst, z, y, x) float64 array and the
+    (mode, n_max, n_clip, f_u, speed_u, phi_min, phi_max, sigma_t, albedo, g, er_stepsize, ...)
+    plus `n_photons` and `seed`. Returns the films as an (n_inst, z, y, x) float64 array and the
     statistics of the whole sweep. Photon j of instance i draws the stream (seed_i, j), so each
     film equals a single render of that configuration with that seed."""
-    import dataclasses
     lib = L.load()
     n = len(instances)
-    arr = (L.InstanceDesc * n)()
-    keep = []
-    for i, inst in enumerate(instances):
-        over = {k: v for k, v in inst.items() if k not in ("n_photons", "seed")}
-        s = dataclasses.replace(setup, **over)
-        fd = s.field_desc()
-        keep.append(s)
-        arr[i].field = fd
-        arr[i].medium = s.medium_desc()
-        arr[i].n_photons = int(inst["n_photons"])
-        arr[i].seed = int(inst.get("seed", 0))
+    arr = _instance_descs(setup, instances)
     sc, _, _, op = setup.descs()
     films = np.zeros((n,) + setup.film_shape(), dtype=np.float64)
     st = L.Stats()
     L.check(lib.smp_render_batch(C.byref(sc), arr, n, C.byref(op), _ptr(films), C.byref(st)))
     return films, st
+
+
+def tune_batch_steps(setup: Setup, instances: list, rmse_budget: float, n_sample: int = 20000):
+    """The step-size autotuner of a batched sweep (smp_batch_tune_steps): per instance, the largest
+    multiple (2 .. 32, at most an eighth of the ultrasound wavelength) of its ER step whose film on
+    its first n_sample photons stays within `rmse_budget` relative RMSE of the film at its own step,
+    on the same photons (largest allowed multiple first, then bisection). Returns (steps, rmse,
+    rounds); pass {"er_stepsize": steps[i]} into instance i for render_batch."""
+    lib = L.load()
+    n = len(instances)
+    arr = _instance_descs(setup, instances)
+    sc, _, _, op = setup.descs()
+    steps = np.zeros(n)
+    rmse = np.zeros(n)
+    rounds = C.c_int32(0)
+    L.check(lib.smp_batch_tune_steps(C.byref(sc), arr, n, C.byref(op), int(n_sample), float(rmse_budget),
+                                     _ptr(steps), _ptr(rmse), C.byref(rounds)))
+    return steps, rmse, int(rounds.value)
 
 
 def trace_photons(setup: Setup, first: int, n: int, weight_photons: int,
