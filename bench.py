@@ -443,7 +443,9 @@ def run_ours(args):
         roof = {"bound": "fp32", "kernel": f"wf_march_kernel<{kname}, {form}>",
                 "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                 "frac": achieved / peak.value,
-                "traffic": _profile_traffic() if args.workload == "precision" else None,
+                "traffic": _profile_traffic(tuning.slots_per_lane) if args.workload == "precision" else None,
+                "traffic_source": "profiles/wf_march_kernel_precision_traffic.txt: one captured steady-state "
+                                  "launch, scaled to this run's slots per lane",
                 "flop_per_er_step": fps, "er_steps_per_launch": march_steps / n_march,
                 "march_kernel_share_of_step_time": march_ms / ms,
                 "peak_source": "FP32 FMA throughput measured live on this GPU (smp_fp32_peak)"}
@@ -510,18 +512,23 @@ def run_plain(args, setup, per_step: int, device: int, first_step: int, steps: i
             "er_steps_per_s": (st.er_steps - st0.er_steps) / (ms / 1e3)}
 
 
-def _profile_traffic():
-    """DRAM bytes of one steady-state march-kernel launch (every slot of the pool live, the bench's
-    slot count and chunk), from the committed ncu capture."""
+def _profile_traffic(slots_per_lane: int):
+    """DRAM bytes of one steady-state march-kernel launch (every slot of the pool live) from the
+    committed ncu capture, scaled from the capture's slots per lane to this run's: a launch moves
+    each live slot's march state, so its traffic follows the live slots."""
     path = os.path.join(ROOT, "profiles", "wf_march_kernel_precision_traffic.txt")
+    vals = {}
     try:
         with open(path) as f:
             for line in f:
-                if line.startswith("dram_bytes_per_launch"):
-                    return float(line.split("=")[1])
+                if "=" in line and not line.startswith("#"):
+                    k, v = line.split("=")
+                    vals[k.strip()] = float(v)
     except OSError:
-        pass
-    return None
+        return None
+    if "dram_bytes_per_launch" not in vals:
+        return None
+    return vals["dram_bytes_per_launch"] * slots_per_lane / vals.get("slots_per_lane", slots_per_lane)
 
 
 def run_e2e(args, setup, steps: int, per_step: int) -> dict:

@@ -16,8 +16,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kparams.h"
@@ -1637,9 +1639,21 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
         if (opts->precision == SMP_PREC_MIXED) {
             e = cudaMemcpy(images_out, d_films, fb * size_t(n_inst), cudaMemcpyDeviceToHost);
         } else {
-            std::vector<float> h(fb / 4 * size_t(n_inst));           // FP32 films, widened on the host
-            e = cudaMemcpy(h.data(), d_films, h.size() * 4, cudaMemcpyDeviceToHost);
-            for (size_t j = 0; j < h.size(); ++j) images_out[j] = double(h[j]);
+            // FP32 films, widened on the host by several threads (the copy's buffer is left
+            // uninitialised: the copy writes all of it)
+            const size_t cnt = fb / 4 * size_t(n_inst);
+            std::unique_ptr<float[]> h(new float[cnt]);
+            e = cudaMemcpy(h.get(), d_films, cnt * 4, cudaMemcpyDeviceToHost);
+            if (e == cudaSuccess) {
+                const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+                const size_t per = (cnt + hw - 1) / hw;
+                std::vector<std::thread> ts;
+                for (unsigned t = 0; t < hw; ++t) {
+                    const size_t a = std::min(cnt, t * per), b = std::min(cnt, a + per);
+                    ts.emplace_back([&h, images_out, a, b] { for (size_t j = a; j < b; ++j) images_out[j] = double(h[j]); });
+                }
+                for (auto &t : ts) t.join();
+            }
         }
         if (e != cudaSuccess) rc = set_error(SMP_ERR_CUDA, "batch films: %s", cudaGetErrorString(e));
     }
