@@ -355,7 +355,9 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
    measured at that step (0 where the instance kept its own); rounds_out (may be NULL) the number of
    batched renders. The budget is against this library's own render at the nominal step: the image
    error against an exact solution adds the nominal step's own error. Set
-   instances[i].field.er_stepsize = steps_out[i] and call smp_render_batch. At most 65535 instances. */
+   instances[i].field.er_stepsize = steps_out[i] and call smp_render_batch. The search holds a
+   reference and a trial film per instance, so instances are tuned in groups whose films fit in 40 %
+   of the free device memory (SMP_ERR_OOM when not even one instance's two films fit). */
 int smp_batch_tune_steps(const smp_scene_desc *scene, const smp_instance_desc *instances,
                          int32_t n_inst, const smp_render_opts *opts, int64_t n_sample,
                          double rmse_budget, double *steps_out, double *rmse_out, int32_t *rounds_out);

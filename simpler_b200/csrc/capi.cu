@@ -1703,67 +1703,65 @@ __global__ void film_diff_kernel(const void *a, const void *r, size_t px, int fp
 // multiple known to pass and the smallest known to miss (the error grows with the step). Every
 // round is one batched render of the instances still searching; an instance keeps the largest
 // multiple whose film stayed within rmse_budget relative RMSE of its reference film on the same
-// photons, or its own step when its reference film is empty.
-int smp_batch_tune_steps(const smp_scene_desc *scene, const smp_instance_desc *instances, int32_t n_inst,
-                         const smp_render_opts *opts, int64_t n_sample, double rmse_budget, double *steps_out,
-                         double *rmse_out, int32_t *rounds_out) {
-    if (!scene || !instances || !opts || n_inst <= 0 || !steps_out) return set_error(SMP_ERR_BAD_ARG, "bad batch arguments");
-    if (n_inst > 65535) return set_error(SMP_ERR_BAD_ARG, "the step tuner takes at most 65535 instances");
-    if (n_sample <= 0) return set_error(SMP_ERR_BAD_ARG, "n_sample must be positive");
-    if (!(rmse_budget > 0.0)) return set_error(SMP_ERR_BAD_ARG, "rmse_budget must be positive");
-    static const int kStepMults[] = {2, 3, 4, 6, 8, 12, 16, 24, 32};
-    const int n_mult = int(sizeof(kStepMults) / sizeof(kStepMults[0]));
-    std::vector<smp_instance_desc> trial(instances, instances + n_inst);
-    // per instance: the allowed multiples are kStepMults[0 .. lim); index pass_i passes (-1: the
-    // instance's own step), index miss_i misses (lim: none known), try_i is this round's
-    std::vector<int> pass(n_inst, -1), miss(n_inst, 0), tr(n_inst, -1);
-    std::vector<double> rmse(n_inst, 0.0);
-    for (int i = 0; i < n_inst; ++i) {
-        const smp_field_desc &f = instances[i].field;
+// photons, or its own step when its reference film is empty. The search holds two films per
+// instance (reference and trial), so instances are tuned in groups whose films fit in 40 % of the
+// free device memory.
+namespace {
+const int kStepMults[] = {2, 3, 4, 6, 8, 12, 16, 24, 32};
+const int kNumStepMults = int(sizeof(kStepMults) / sizeof(kStepMults[0]));
+
+// the search over instances [0, n) of `inst`; pass/rmse per instance out; *rounds accumulates
+int tune_steps_group(const smp_scene_desc *scene, const smp_instance_desc *inst, int n, const smp_render_opts *opts,
+                     int64_t n_sample, double rmse_budget, int *pass, double *rmse, int *rounds) {
+    std::vector<smp_instance_desc> trial(inst, inst + n);
+    // per instance: the allowed multiples are kStepMults[0 .. lim); index pass[i] passes (-1: the
+    // instance's own step), index miss[i] misses (lim: none known), tr[i] is this round's
+    std::vector<int> miss(n, 0), tr(n, -1);
+    for (int i = 0; i < n; ++i) {
+        const smp_field_desc &f = inst[i].field;
         const double lambda = f.speed_u / f.f_u;
         int lim = 0;
-        while (lim < n_mult && f.er_stepsize * kStepMults[lim] <= lambda / 8.0) ++lim;
-        miss[i] = instances[i].n_photons > 0 ? lim : 0;           // nothing to search without photons
-        trial[i].n_photons = std::min<int64_t>(instances[i].n_photons, n_sample);
+        while (lim < kNumStepMults && f.er_stepsize * kStepMults[lim] <= lambda / 8.0) ++lim;
+        pass[i] = -1;
+        rmse[i] = 0.0;
+        miss[i] = inst[i].n_photons > 0 ? lim : 0;                 // nothing to search without photons
+        trial[i].n_photons = std::min<int64_t>(inst[i].n_photons, n_sample);
     }
-    int rc = check_device(opts->device);
-    if (rc) return rc;
     void *d_ref = nullptr, *d_try = nullptr;
     double *d_acc = nullptr;
     size_t fb = 0;
-    int rounds = 0;
-    rc = batch_run(scene, trial.data(), n_inst, opts, false, &d_ref, &fb, nullptr);
-    ++rounds;
+    int rc = batch_run(scene, trial.data(), n, opts, false, &d_ref, &fb, nullptr);
+    ++*rounds;
     const int fp64 = opts->precision == SMP_PREC_MIXED;
     const size_t px = fb / (fp64 ? 8 : 4);
-    std::vector<double> acc(2 * size_t(n_inst));
+    std::vector<double> acc(2 * size_t(n));
     if (!rc) {
         cudaError_t e = cudaMalloc(&d_acc, acc.size() * sizeof(double));
         if (e != cudaSuccess) rc = set_error(SMP_ERR_OOM, "tuner buffers: %s", cudaGetErrorString(e));
     }
     for (bool first = true; !rc; first = false) {
         bool any = false;
-        for (int i = 0; i < n_inst; ++i) {
+        for (int i = 0; i < n; ++i) {
             tr[i] = -1;
             if (miss[i] - pass[i] > 1) tr[i] = first ? miss[i] - 1 : (pass[i] + miss[i]) / 2;
-            trial[i].field.er_stepsize = instances[i].field.er_stepsize * (tr[i] >= 0 ? kStepMults[tr[i]] : 1);
-            trial[i].n_photons = tr[i] >= 0 ? std::min<int64_t>(instances[i].n_photons, n_sample) : 0;
+            trial[i].field.er_stepsize = inst[i].field.er_stepsize * (tr[i] >= 0 ? kStepMults[tr[i]] : 1);
+            trial[i].n_photons = tr[i] >= 0 ? std::min<int64_t>(inst[i].n_photons, n_sample) : 0;
             any = any || tr[i] >= 0;
         }
         if (!any) break;
-        rc = batch_run(scene, trial.data(), n_inst, opts, false, &d_try, &fb, nullptr);
-        ++rounds;
+        rc = batch_run(scene, trial.data(), n, opts, false, &d_try, &fb, nullptr);
+        ++*rounds;
         if (rc) break;
         cudaError_t e = cudaMemset(d_acc, 0, acc.size() * sizeof(double));
         if (e == cudaSuccess) {
-            film_diff_kernel<<<dim3(64, unsigned(n_inst)), 256>>>(d_try, d_ref, px, fp64, d_acc);
+            film_diff_kernel<<<dim3(64, unsigned(n)), 256>>>(d_try, d_ref, px, fp64, d_acc);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaMemcpy(acc.data(), d_acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost);
         cudaFree(d_try);
         d_try = nullptr;
         if (e != cudaSuccess) { rc = set_error(SMP_ERR_CUDA, "tuner films: %s", cudaGetErrorString(e)); break; }
-        for (int i = 0; i < n_inst; ++i) {
+        for (int i = 0; i < n; ++i) {
             if (tr[i] < 0) continue;
             if (!(acc[2 * i + 1] > 0.0)) { miss[i] = pass[i] + 1; continue; }   // empty reference film: keep its step
             const double r = std::sqrt(acc[2 * i] / acc[2 * i + 1]);
@@ -1776,6 +1774,35 @@ int smp_batch_tune_steps(const smp_scene_desc *scene, const smp_instance_desc *i
     cudaFree(d_try);
     cudaFree(d_acc);
     g_last_error = err;
+    return rc;
+}
+}  // namespace
+
+int smp_batch_tune_steps(const smp_scene_desc *scene, const smp_instance_desc *instances, int32_t n_inst,
+                         const smp_render_opts *opts, int64_t n_sample, double rmse_budget, double *steps_out,
+                         double *rmse_out, int32_t *rounds_out) {
+    if (!scene || !instances || !opts || n_inst <= 0 || !steps_out) return set_error(SMP_ERR_BAD_ARG, "bad batch arguments");
+    if (n_sample <= 0) return set_error(SMP_ERR_BAD_ARG, "n_sample must be positive");
+    if (!(rmse_budget > 0.0)) return set_error(SMP_ERR_BAD_ARG, "rmse_budget must be positive");
+    int rc = check_device(opts->device);
+    if (rc) return rc;
+    // instances per group: two films each within 40 % of the free memory (at most 65535, the
+    // difference kernel's grid height)
+    size_t free_b = 0, total_b = 0;
+    SMP_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t film = size_t(scene->x_res) * size_t(scene->y_res) * size_t(scene->z_res) *
+                        (opts->precision == SMP_PREC_MIXED ? 8 : 4);
+    const size_t fit = film ? size_t(double(free_b) * 0.4) / (2 * film) : size_t(n_inst);
+    if (fit == 0) return set_error(SMP_ERR_OOM, "the step tuner needs two films of %zu bytes; %zu bytes are free", film, free_b);
+    const int group = int(std::min<size_t>({size_t(n_inst), fit, size_t(65535)}));
+    std::vector<int> pass(n_inst, -1);
+    std::vector<double> rmse(n_inst, 0.0);
+    int rounds = 0;
+    for (int g0 = 0; g0 < n_inst && !rc; g0 += group) {
+        const int gn = std::min(group, n_inst - g0);
+        rc = tune_steps_group(scene, instances + g0, gn, opts, n_sample, rmse_budget, pass.data() + g0,
+                              rmse.data() + g0, &rounds);
+    }
     if (rc) return rc;
     for (int i = 0; i < n_inst; ++i) {
         steps_out[i] = instances[i].field.er_stepsize * (pass[i] >= 0 ? kStepMults[pass[i]] : 1);

@@ -127,3 +127,12 @@ def test_tune_batch_steps_within_budget_and_against_fp64_oracle():
         e_tuned, e_nominal = _rel(tuned[i], ref), _rel(nominal[i], ref)
         assert e_tuned <= 1e-2, (i, e_tuned, e_nominal)
         assert e_tuned <= e_nominal + budget, (i, e_tuned, e_nominal)
+
+
+def test_tune_batch_steps_rejects_bad_arguments():
+    """The step tuner's argument checks run before any device work."""
+    setup, insts = sb.config_batch_sweep(n_inst=2)
+    with pytest.raises(sb.SmpError, match="n_sample"):
+        sb.tune_batch_steps(setup, insts, 2e-3, n_sample=0)
+    with pytest.raises(sb.SmpError, match="rmse_budget"):
+        sb.tune_batch_steps(setup, insts, 0.0)
