@@ -350,7 +350,10 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
    (sqrt(sum (film - ref)^2 / sum ref^2)) of the reference film. It tries the largest allowed
    multiple first and, where that misses, bisects between the multiples known to pass and to miss
    (the error grows with the step); each round is one batched render of the instances still
-   searching. An instance with no photons or an empty reference film keeps its own step.
+   searching. An instance with no photons or an empty reference film keeps its own step. Unless
+   opts->sensor_march_max is set, the trial renders stop a sensor march at 30 mean free paths of the
+   thinnest medium, which cuts the reference and trial films alike by less than e^-30 of a photon's
+   weight and shortens the rounds' tails.
    steps_out[i] receives instance i's chosen er_stepsize; rmse_out[i] (may be NULL) the relative RMSE
    measured at that step (0 where the instance kept its own); rounds_out (may be NULL) the number of
    batched renders. The budget is against this library's own render at the nominal step: the image

@@ -1714,6 +1714,17 @@ const int kNumStepMults = int(sizeof(kStepMults) / sizeof(kStepMults[0]));
 int tune_steps_group(const smp_scene_desc *scene, const smp_instance_desc *inst, int n, const smp_render_opts *opts,
                      int64_t n_sample, double rmse_budget, int *pass, double *rmse, int *rounds) {
     std::vector<smp_instance_desc> trial(inst, inst + n);
+    // The trial renders stop a sensor march at 30 mean free paths of the thinnest medium (unless the
+    // caller set a budget): the reference and trial films are cut alike, a cut photon's remaining
+    // contribution is below e^-30 of its weight, and the photons trapped by total internal
+    // reflection, which set every round's tail, stop sooner than at the default 110.
+    smp_render_opts topts = *opts;
+    if (!(topts.sensor_march_max > 0.0)) {
+        double st_min = HUGE_VAL;
+        for (int i = 0; i < n; ++i) st_min = std::min(st_min, inst[i].medium.sigma_t);
+        if (st_min > 1e-3) topts.sensor_march_max = 30.0 / st_min;
+    }
+    opts = &topts;
     // per instance: the allowed multiples are kStepMults[0 .. lim); index pass[i] passes (-1: the
     // instance's own step), index miss[i] misses (lim: none known), tr[i] is this round's
     std::vector<int> miss(n, 0), tr(n, -1);
