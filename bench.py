@@ -11,7 +11,12 @@ pool of the two-kernel march is refilled until the step's photons run out, then 
 
 Under torchrun each rank traces its own photon range (counter-based streams keyed by the global
 photon index, so the render is the same for any GPU count) and the film is reduced to rank 0 over
-NCCL every step. Prints one JSON line (rank 0).
+NCCL every step. Prints one JSON line (rank 0). On one GPU the line also carries `plain` (the plain
+one-thread-per-photon kernel on the same workload), `image_rmse_vs_fp64` (the films against the FP64
+oracle on the same photons) and `batched_form`: the north star's batched form, the 256-instance
+sweep with ER steps from the step-size autotuner, against the plain kernel on the same instances,
+with its own image check against the FP64 oracle (`--workload sweep` prints it as its own line,
+with the nominal-step sweep and the one-render-per-instance loop beside it).
 """
 from __future__ import annotations
 
@@ -474,6 +479,9 @@ def run_ours(args):
         out["speedup_vs_plain"] = value / world / plain["value"]
         if world == 1 and args.workload in ("precision", "plain"):
             out["image_rmse_vs_fp64"] = image_check(setup, 20_000 if args.workload == "precision" else 100_000)
+        if world == 1 and args.workload == "precision":
+            # the north star's batched form against the plain kernel, beside the headline
+            out["batched_form"] = batched_form(args, False)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -584,93 +592,116 @@ def sweep_image_check(setup, insts, steps, n: int, threads: int) -> list:
     return out
 
 
-def run_sweep(args):
-    """The batched sweep (256 cylindrical-transducer instances over the plain small scene, budgets
-    log-uniform 1e5-1e7, seed 2) rendered in one slot pool with smp_render_batch, against the same
-    instances rendered one smp_render call each (the reference's per-configuration loop) and with the
-    plain kernel. The batched form takes each instance's ER step from the step-size autotuner
-    (smp_batch_tune_steps, within --step-budget of the instance's film at its own step); the same
-    sweep at the nominal step is timed beside it. All host-timed end to end (films read back to host
-    memory); one JSON line."""
-    import torch
-    torch.cuda.set_device(0)
+SWEEP_DESC = ("batched sweep: 256 Bessel instances (n_max U[0,2e-3], f U[0.5,2] MHz, mode 0-2, duty U[1,100]%, "
+              "budgets log-uniform 1e5-1e7 x scale), medium and film of the plain small configuration, seed 2")
+
+
+def batched_form(args, with_reference_legs: bool) -> dict:
+    """The batched form against the plain kernel (the north star's target): the 256-instance sweep
+    with each instance's ER step from the step-size autotuner (smp_batch_tune_steps within
+    --step-budget of the instance's film at its own step; the tuner inside the timed region),
+    rendered in one slot pool by smp_render_batch; the plain kernel (one thread per photon, FP32,
+    0.01 mm) over every 8th instance, one render each; and the image check of three instances
+    against the FP64 oracle at 0.01 mm. With with_reference_legs also the sweep at the nominal step
+    and the one-smp_render-per-instance loop. All host-timed end to end (films read back)."""
+    import dataclasses
     setup, insts = sb.config_batch_sweep(n_inst=256, seed=2, scale=args.sweep_scale)
     total = sum(i["n_photons"] for i in insts)
     # warm-up: module load, first allocations, and the schedule tuner's trials (2e6 photons of this
     # scene), whose schedule the timed sweeps take from the process-wide cache (keyed by the scene and
     # the first instance's field and step, so once for the nominal and once for the tuned steps)
-    sb.render_batch(setup, insts[:16])
     w_steps, _, _ = sb.tune_batch_steps(setup, insts[:16], args.step_budget, n_sample=20000)
     sb.render_batch(setup, [dict(inst, er_stepsize=float(h)) for inst, h in zip(insts[:16], w_steps)])
+    if with_reference_legs:
+        sb.render_batch(setup, insts[:16])
     clocks = ClockSampler(0)
     clocks.start()
-    t0 = time.perf_counter()
-    films, st = sb.render_batch(setup, insts)          # tunes first (cached after the warm-up's call)
-    t_batch = time.perf_counter() - t0
-    # the batched form: the autotuner's step per instance (its trial renders timed as part of it)
     t0 = time.perf_counter()
     steps, rmse, rounds = sb.tune_batch_steps(setup, insts, args.step_budget, n_sample=20000)
     t_tune = time.perf_counter() - t0
     t0 = time.perf_counter()
     films_t, st_t = sb.render_batch(setup, [dict(inst, er_stepsize=float(h)) for inst, h in zip(insts, steps)])
     t_tuned = time.perf_counter() - t0
-    import dataclasses
-    t0 = time.perf_counter()
-    serial_sum = 0.0
-    for i, inst in enumerate(insts):
-        over = {k: v for k, v in inst.items() if k != "n_photons"}
-        img, _ = sb.render(dataclasses.replace(setup, **over), inst["n_photons"])
-        serial_sum += float(img.sum())
-    t_serial = time.perf_counter() - t0
+    extra = {}
+    if with_reference_legs:
+        t0 = time.perf_counter()
+        films, st = sb.render_batch(setup, insts)
+        t_batch = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        serial_sum = 0.0
+        for i, inst in enumerate(insts):
+            over = {k: v for k, v in inst.items() if k != "n_photons"}
+            img, _ = sb.render(dataclasses.replace(setup, **over), inst["n_photons"])
+            serial_sum += float(img.sum())
+        t_serial = time.perf_counter() - t0
+        extra = {"nominal_step": {"value": total / t_batch, "unit": METRIC, "seconds": t_batch, "er_steps": st.er_steps,
+                                  "call": "smp_render_batch with every instance at 0.01 mm"},
+                 "serial": {"value": total / t_serial, "unit": METRIC, "seconds": t_serial,
+                            "call": "one smp_render per instance, host film, nominal step"},
+                 "speedup_vs_serial": t_serial / (t_tuned + t_tune),
+                 "film_sum_relative_difference": abs(float(films.sum()) - serial_sum) / max(serial_sum, 1e-300)}
     # the plain kernel (one thread per photon, FP32, nominal step) over every 8th instance, one render each
     t0 = time.perf_counter()
     plain_photons = 0
+    plain_dev_ms = 0.0
     for i, inst in enumerate(insts[::8]):
         over = {k: v for k, v in inst.items() if k != "n_photons"}
-        sb.render(dataclasses.replace(setup, kernel=L.KERNEL_PLAIN, **over), inst["n_photons"])
+        _, pst = sb.render(dataclasses.replace(setup, kernel=L.KERNEL_PLAIN, **over), inst["n_photons"])
         plain_photons += inst["n_photons"]
+        plain_dev_ms += pst.kernel_ms
     t_plain = time.perf_counter() - t0
     clk = clocks.stop()
     mults = steps / setup.er_stepsize
     plain_rate = plain_photons / t_plain
-    # image check against the FP64 oracle: the instance with the smallest step multiple among the
-    # hardest fields (largest n_max x f), the one with the largest multiple, and instance 0
+    value = total / (t_tuned + t_tune)
+    if with_reference_legs:
+        extra["nominal_step"]["speedup_vs_plain"] = extra["nominal_step"]["value"] / plain_rate
+    # image check against the FP64 oracle: the hardest field (largest n_max x f), the instance with
+    # the largest multiple, and instance 0
     hard = max(range(len(insts)), key=lambda i: insts[i]["n_max"] * insts[i]["f_u"])
     big = int(np.argmax(mults))
     check = sweep_image_check(setup, insts, [(i, steps[i]) for i in sorted({hard, big, 0})], 10000,
                               os.cpu_count() or 1)
     hist = {str(m): int((np.rint(mults) == m).sum()) for m in (1, 2, 3, 4, 6, 8, 12, 16, 24, 32)}
     out = {
-        "metric": METRIC, "value": total / (t_tuned + t_tune), "unit": METRIC, "n_gpus": 1, "steps": 1,
-        "warmup": 1, "ms_per_step": (t_tuned + t_tune) * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-        "config": {"workload": "batched sweep: 256 Bessel instances (n_max U[0,2e-3], f U[0.5,2] MHz, mode 0-2, "
-                               "duty U[1,100]%, budgets log-uniform 1e5-1e7 x scale), medium and film of the "
-                               "plain small configuration, seed 2; ER step per instance from the step-size "
-                               "autotuner (its trial renders inside the timed region)", "photons": total,
-                   "scale": args.sweep_scale, "film": list(setup.film_shape()), "step_budget": args.step_budget},
+        "value": value, "unit": METRIC, "seconds": t_tuned + t_tune,
+        "config": {"workload": SWEEP_DESC + "; ER step per instance from the step-size autotuner (its trial renders "
+                                           "inside the timed region)", "photons": total, "scale": args.sweep_scale,
+                   "film": list(setup.film_shape()), "step_budget": args.step_budget},
         "step_tuner": {"seconds": t_tune, "rounds": rounds, "sample_photons_per_instance": 20000,
                        "multiples_histogram": hist, "mean_multiple_by_photons":
                            float(sum(m * i["n_photons"] for m, i in zip(mults, insts)) / total),
                        "max_measured_rmse": float(rmse.max())},
         "tuned_render_seconds": t_tuned, "er_steps_per_s": st_t.er_steps / t_tuned, "er_steps": st_t.er_steps,
-        "nominal_step": {"value": total / t_batch, "unit": METRIC, "seconds": t_batch, "er_steps": st.er_steps,
-                         "speedup_vs_plain": (total / t_batch) / plain_rate,
-                         "call": "smp_render_batch with every instance at 0.01 mm"},
-        "serial": {"value": total / t_serial, "unit": METRIC, "seconds": t_serial,
-                   "call": "one smp_render per instance, host film, nominal step"},
-        "speedup_vs_serial": t_serial / (t_tuned + t_tune),
         "plain": {"value": plain_rate, "unit": METRIC, "seconds": t_plain, "photons": plain_photons,
                   "call": "one smp_render per instance with the plain kernel (one thread per photon, fp32, "
                           "0.01 mm step), every 8th instance (32 of 256)"},
-        "speedup_vs_plain": (total / (t_tuned + t_tune)) / plain_rate,
+        "speedup_vs_plain": value / plain_rate,
+        # the same comparison on device time alone (the render's traces against the plain kernel's
+        # launches; the step tuner's renders are host-timed only and left out here)
+        "device": {"tuned_render_seconds": st_t.kernel_ms / 1e3, "plain_seconds": plain_dev_ms / 1e3,
+                   "value": total / (st_t.kernel_ms / 1e3), "plain_value": plain_photons / (plain_dev_ms / 1e3),
+                   "speedup_vs_plain": (total / st_t.kernel_ms) / (plain_photons / plain_dev_ms)},
         "image_rmse_vs_fp64": {"photons": 10000, "reference": "FP64 CPU restatement at the nominal 0.01 mm step, "
                                                               "same Philox photons", "instances": check},
-        "film_sum_relative_difference": abs(float(films.sum()) - serial_sum) / max(serial_sum, 1e-300),
         "gpu_launches": st_t.launches, "clocks": clk,
         "schedule": {"march_block": st_t.march_block, "slots_per_lane": st_t.slots_per_lane, "chunk": st_t.chunk,
                      "tuned": bool(st_t.tuned), "cuda_graph": True},
     }
+    out.update(extra)
+    return out
+
+
+def run_sweep(args):
+    """The batched sweep as its own JSON line (batched_form with the nominal-step and
+    one-render-per-instance legs)."""
+    import torch
+    torch.cuda.set_device(0)
+    b = batched_form(args, True)
+    out = {"metric": METRIC, "value": b.pop("value"), "unit": METRIC, "n_gpus": 1, "steps": 1, "warmup": 1,
+           "ms_per_step": b.pop("seconds") * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "fp32", "data": "synthetic"}
+    out.update(b)
     print(json.dumps(out), flush=True)
 
 

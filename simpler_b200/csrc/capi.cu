@@ -1242,7 +1242,18 @@ int tune_trial(smp_plan *p, int64_t n, int64_t weight, double *ms) {
 }
 }  // namespace
 
+// The tuner. n_grow > n_sample (a batched sweep, whose whole render is cheap per photon): the trial
+// size is chosen from two warm-up traces instead, which separate a trace's fixed cost (the fill,
+// and the tail: one photon trapped by total internal reflection marching alone, tens of ms) from its
+// cost per photon, so that every trial holds about 250 ms of work per photon -- up to n_grow
+// photons -- and the tails do not decide between schedules. The cache key keeps n_sample.
+static int plan_tune(smp_plan *plan, int64_t n_sample, int64_t n_grow, smp_tuning *out);
+
 extern "C" int smp_plan_tune(smp_plan *plan, int64_t n_sample, smp_tuning *out) {
+    return plan_tune(plan, n_sample, n_sample, out);
+}
+
+static int plan_tune(smp_plan *plan, int64_t n_sample, int64_t n_grow, smp_tuning *out) {
     if (!plan || n_sample <= 0) return set_error(SMP_ERR_BAD_ARG, "bad plan / sample size");
     if (plan->kernel != SMP_KERNEL_POOL)
         return set_error(SMP_ERR_UNSUPPORTED, "the tuner chooses the slot pool's parameters (kernel SMP_KERNEL_POOL)");
@@ -1276,10 +1287,20 @@ extern "C" int smp_plan_tune(smp_plan *plan, int64_t n_sample, smp_tuning *out) 
     const int64_t n_warm = std::min<int64_t>(n_sample, 200000);
     int rc = tune_trial(plan, n_warm, weight, &ms);
     if (rc) return rc;
-    // keep each trial near 400 ms, long enough that the full pool's steady state and not the fill
-    // and drain decides: a sample that takes longer is scaled down (not below 1e5 photons)
-    const double est = ms * double(n_sample) / double(n_warm);
-    if (est > 400.0) n_sample = std::max<int64_t>(std::min<int64_t>(n_sample, 100000), int64_t(double(n_sample) * 400.0 / est));
+    if (n_grow > n_sample) {
+        // cost per photon from a second warm-up of 8x the photons: ms = fixed + per_photon * n
+        const int64_t n2 = std::min<int64_t>(n_grow, 8 * n_warm);
+        double ms2 = 0.0;
+        rc = tune_trial(plan, n2, weight, &ms2);
+        if (rc) return rc;
+        const double per = n2 > n_warm ? std::max(ms2 - ms, 1e-3) / double(n2 - n_warm) : ms2 / double(n2);
+        n_sample = std::min<int64_t>(n_grow, std::max<int64_t>(n_warm, int64_t(250.0 / per)));
+    } else {
+        // keep each trial near 400 ms, long enough that the full pool's steady state and not the fill
+        // and drain decides: a sample that takes longer is scaled down (not below 1e5 photons)
+        const double est = ms * double(n_sample) / double(n_warm);
+        if (est > 400.0) n_sample = std::max<int64_t>(std::min<int64_t>(n_sample, 100000), int64_t(double(n_sample) * 400.0 / est));
+    }
     smp_tuning second = best;
     auto consider = [&](const smp_tuning &c, double m) {
         if (m < best.ms) { second = best; best = c; best.ms = m; }
@@ -1602,7 +1623,7 @@ static int batch_run(const smp_scene_desc *scene, const smp_instance_desc *insta
         const char *tune_env = std::getenv("SMP_TUNE");
         if (!rc && schedule_tune && total > 0 && p->kernel == SMP_KERNEL_POOL && !(tune_env && std::atoi(tune_env) == 0)) {
             smp_tuning tt;
-            rc = smp_plan_tune(p, std::min<long long>(total, 2000000LL), &tt);
+            rc = plan_tune(p, std::min<long long>(total, 2000000LL), total, &tt);
             if (!rc) {
                 e = cudaMemset(d_films, 0, px * bpp * size_t(n_inst));      // the trials' photons
                 if (e != cudaSuccess) rc = set_error(SMP_ERR_CUDA, "batch films: %s", cudaGetErrorString(e));
