@@ -350,6 +350,19 @@ static void set_step_sizes(KParams &k, const smp_field_desc &f) {
     step_table(f.er_stepsize, k.cur_tab);
 }
 
+// Runs f(begin, end) over [0, n) on up to 16 host threads.
+template <class F>
+static void host_parallel(size_t n, F f) {
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t per = (n + hw - 1) / hw;
+    std::vector<std::thread> ts;
+    for (unsigned t = 0; t < hw; ++t) {
+        const size_t a = std::min(n, t * per), b = std::min(n, a + per);
+        if (a < b) ts.emplace_back([&f, a, b] { f(a, b); });
+    }
+    for (auto &t : ts) t.join();
+}
+
 static void set_box_thresholds(KParams &k) {
     const double eps = double(1.19209290e-07f);
     for (int i = 0; i < 3; ++i) {
@@ -1520,165 +1533,191 @@ int smp_fp32_peak(int device, double *tflops_out) {
 // Philox stream (seed_i, j), so each instance's film is the one a single-instance render with that
 // seed produces.
 //
-// batch_run renders the sweep into n_inst consecutive device films (float, or double in the mixed
-// form; *film_bytes each), which it allocates and hands to the caller (*d_films_out, to cudaFree).
-// schedule_tune: run the slot pool's autotuner first (trials on the sweep's first photons, cached
-// per process).
-static int batch_run(const smp_scene_desc *scene, const smp_instance_desc *instances, int32_t n_inst,
-                     const smp_render_opts *opts, bool schedule_tune, void **d_films_out, size_t *film_bytes,
-                     smp_stats *stats_out) {
-    *d_films_out = nullptr;
+// A sweep's device state (BatchRun): its plan (field kind FK_BATCH), the instance records, the
+// prefix sums of the photon budgets, the Bessel tables and n_inst consecutive films (float, or
+// double in the mixed form; film_bytes each). batch_open builds it; batch_set writes the instance
+// records and budgets (again for a sweep of the same fields with other steps or budgets, as the
+// step tuner's rounds are); batch_trace clears the films and renders.
+namespace {
+struct BatchRun {
+    smp_plan *p = nullptr;
+    Inst *d_insts = nullptr;
+    long long *d_first = nullptr;
+    float4 *d_tabs = nullptr;
+    void *d_films = nullptr;
+    size_t film_bytes = 0;
+    int n_inst = 0;
+    long long total = 0;
+    std::vector<int> fks;
+    size_t tab_off[3] = {0, 0, 0};
+    int tab_int[3] = {0, 0, 0};
+    smp_scene_desc scene;
+    smp_render_opts opts;
+    BatchRun() = default;
+    BatchRun(const BatchRun &) = delete;
+    BatchRun &operator=(const BatchRun &) = delete;
+    ~BatchRun() {
+        const std::string err = g_last_error;
+        cudaFree(d_insts);
+        cudaFree(d_first);
+        cudaFree(d_tabs);
+        cudaFree(d_films);
+        if (p) smp_plan_destroy(p);
+        g_last_error = err;
+    }
+};
+}  // namespace
+
+static int batch_set(BatchRun &b, const smp_instance_desc *instances);
+
+static int batch_open(const smp_scene_desc *scene, const smp_instance_desc *instances, int32_t n_inst,
+                      const smp_render_opts *opts, BatchRun &b) {
     if (!scene || !instances || !opts || n_inst <= 0) return set_error(SMP_ERR_BAD_ARG, "bad batch arguments");
     if (opts->rng != SMP_RNG_PHILOX) return set_error(SMP_ERR_UNSUPPORTED, "a batched sweep draws from Philox");
-    std::vector<int> fks(n_inst);
-    long long total = 0;
+    b.fks.assign(n_inst, 0);
     for (int i = 0; i < n_inst; ++i) {
         int rc = check_descs(scene, &instances[i].medium, &instances[i].field, opts);
         if (rc) return rc;
-        rc = field_kind(instances[i].field, &fks[i]);
+        rc = field_kind(instances[i].field, &b.fks[i]);
         if (rc) return rc;
-        if (fks[i] > FK_BESSEL2)
+        if (b.fks[i] > FK_BESSEL2)
             return set_error(SMP_ERR_UNSUPPORTED, "instance %d: a batched sweep renders Bessel fields of order 0-2", i);
         if (instances[i].n_photons < 0) return set_error(SMP_ERR_BAD_ARG, "instance %d: negative photon budget", i);
         if (instances[i].field.precision != instances[0].field.precision)
             return set_error(SMP_ERR_BAD_ARG, "instance %d: a batched sweep shares one number of refinement levels "
                              "(%d, instance 0 has %d)", i, instances[i].field.precision, instances[0].field.precision);
-        total += instances[i].n_photons;
     }
-    smp_plan *p = nullptr;
-    int rc = smp_plan_create(scene, &instances[0].medium, &instances[0].field, opts, &p);
+    b.n_inst = n_inst;
+    b.scene = *scene;
+    b.opts = *opts;
+    int rc = smp_plan_create(scene, &instances[0].medium, &instances[0].field, opts, &b.p);
     if (rc) return rc;
+    smp_plan *p = b.p;
     const size_t px = p->film_elems, bpp = p->kp.fp64 ? 8 : 4;
-    *film_bytes = px * bpp;
-    // host side of the per-instance records and tables
-    std::vector<Inst> hi(n_inst);
-    std::vector<long long> first(size_t(n_inst) + 1, 0);
+    b.film_bytes = px * bpp;
     // the tables depend on the order and the largest k r only: one per order, as long as the
     // largest k r any instance of that order meets
     double xmax[3] = {0.0, 0.0, 0.0};
     for (int i = 0; i < n_inst; ++i) {
         FieldParams F;
-        fill_field_params(instances[i].field, fks[i], F);
-        xmax[fks[i]] = std::max(xmax[fks[i]], box_max_kr(*scene, F.k_r));
+        fill_field_params(instances[i].field, b.fks[i], F);
+        xmax[b.fks[i]] = std::max(xmax[b.fks[i]], box_max_kr(*scene, F.k_r));
     }
     std::vector<float4> tabs;
-    size_t tab_off[3] = {0, 0, 0};
-    int tab_int[3] = {0, 0, 0};
     for (int m = 0; m < 3; ++m) {
         if (xmax[m] <= 0.0) continue;
         std::vector<float4> t;
         bessel_table(m, xmax[m], t);
-        tab_off[m] = tabs.size();
-        tab_int[m] = int(t.size() / 2);
+        b.tab_off[m] = tabs.size();
+        b.tab_int[m] = int(t.size() / 2);
         tabs.insert(tabs.end(), t.begin(), t.end());
     }
-    for (int i = 0; i < n_inst; ++i) {
+    cudaError_t e = cudaMalloc(&b.d_insts, sizeof(Inst) * size_t(n_inst));
+    if (e == cudaSuccess) e = cudaMalloc(&b.d_first, sizeof(long long) * size_t(n_inst + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&b.d_tabs, sizeof(float4) * tabs.size());
+    if (e == cudaSuccess) e = cudaMalloc(&b.d_films, b.film_bytes * size_t(n_inst));
+    if (e == cudaSuccess) e = cudaMemcpy(b.d_tabs, tabs.data(), sizeof(float4) * tabs.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess)
+        return set_error(e == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "batch buffers: %s", cudaGetErrorString(e));
+    p->kp.insts = b.d_insts;
+    p->kp.inst_first = b.d_first;
+    p->kp.n_inst = n_inst;
+    p->fk = FK_BATCH;
+    p->smem_bytes = 0;
+    rc = grid_for(FK_BATCH, p->device, p->opts.blocks_per_sm, 0, &p->grid);
+    if (rc) return rc;
+    const char *graph_env = std::getenv("SMP_WF_GRAPH");
+    p->use_graph = !(graph_env && std::atoi(graph_env) == 0);
+    return batch_set(b, instances);
+}
+
+// Instance records and budgets of a sweep whose fields (orders, largest k r) are those it was opened
+// with; steps, media, seeds and budgets may differ.
+static int batch_set(BatchRun &b, const smp_instance_desc *instances) {
+    std::vector<Inst> hi(b.n_inst);
+    std::vector<long long> first(size_t(b.n_inst) + 1, 0);
+    const size_t px = b.p->film_elems, bpp = b.p->kp.fp64 ? 8 : 4;
+    for (int i = 0; i < b.n_inst; ++i) {
         const smp_instance_desc &d = instances[i];
         Inst &I = hi[i];
         std::memset(&I, 0, sizeof(I));
-        fill_field_params(d.field, fks[i], I.field);
-        I.field.bnodes = 2 * tab_int[fks[i]];
-        I.field.bint = tab_int[fks[i]];
+        const int fk = b.fks[i];
+        fill_field_params(d.field, fk, I.field);
+        I.field.bnodes = 2 * b.tab_int[fk];
+        I.field.bint = b.tab_int[fk];
+        I.field.btab = b.d_tabs + b.tab_off[fk];
+        I.film = static_cast<char *>(b.d_films) + px * bpp * size_t(i);
         I.sigma_t = float(d.medium.sigma_t);                      // medium.h:24-38
         I.albedo = float(d.medium.albedo);
         I.mfp = 1.0f / float(d.medium.sigma_t);
         if (I.sigma_t <= 1.19209290e-07f) { I.sigma_t = 0.0f; I.mfp = 1.0f; I.albedo = 0.0f; }
         I.g = float(d.medium.g);
-        I.weight = d.n_photons > 0 ? photon_weight(*scene, d.n_photons) : 0.0f;
-        I.large_dist = sensor_march_budget(*opts, I.sigma_t);
+        I.weight = d.n_photons > 0 ? photon_weight(b.scene, d.n_photons) : 0.0f;
+        I.large_dist = sensor_march_budget(b.opts, I.sigma_t);
         I.seed = d.seed;
         I.h0 = float(d.field.er_stepsize);                      // each instance marches with its own step
         step_table(d.field.er_stepsize, I.cur_tab);
         first[i + 1] = first[i] + d.n_photons;
     }
-    Inst *d_insts = nullptr;
-    long long *d_first = nullptr;
-    float4 *d_tabs = nullptr;
-    void *d_films = nullptr;
-    cudaError_t e = cudaMalloc(&d_insts, sizeof(Inst) * size_t(n_inst));
-    if (e == cudaSuccess) e = cudaMalloc(&d_first, sizeof(long long) * size_t(n_inst + 1));
-    if (e == cudaSuccess) e = cudaMalloc(&d_tabs, sizeof(float4) * tabs.size());
-    if (e == cudaSuccess) e = cudaMalloc(&d_films, px * bpp * size_t(n_inst));
-    if (e == cudaSuccess) e = cudaMemset(d_films, 0, px * bpp * size_t(n_inst));
-    if (e == cudaSuccess) {
-        for (int i = 0; i < n_inst; ++i) {
-            hi[i].field.btab = d_tabs + tab_off[fks[i]];
-            hi[i].film = static_cast<char *>(d_films) + px * bpp * size_t(i);
-        }
-        e = cudaMemcpy(d_insts, hi.data(), sizeof(Inst) * size_t(n_inst), cudaMemcpyHostToDevice);
+    b.total = first[b.n_inst];
+    cudaError_t e = cudaMemcpy(b.d_insts, hi.data(), sizeof(Inst) * size_t(b.n_inst), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b.d_first, first.data(), sizeof(long long) * size_t(b.n_inst + 1), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return set_error(SMP_ERR_CUDA, "batch records: %s", cudaGetErrorString(e));
+    return SMP_OK;
+}
+
+// Clears the films and renders every instance's budget. schedule_tune: run the slot pool's autotuner
+// first (trials on the sweep's own photons, cached per process).
+static int batch_trace(BatchRun &b, bool schedule_tune, smp_stats *stats_out) {
+    smp_plan *p = b.p;
+    int rc = SMP_OK;
+    const char *tune_env = std::getenv("SMP_TUNE");
+    if (schedule_tune && b.total > 0 && p->kernel == SMP_KERNEL_POOL && !(tune_env && std::atoi(tune_env) == 0)) {
+        smp_tuning tt;
+        rc = plan_tune(p, std::min<long long>(b.total, 2000000LL), b.total, &tt);
+        if (rc) return rc;
     }
-    if (e == cudaSuccess) e = cudaMemcpy(d_first, first.data(), sizeof(long long) * size_t(n_inst + 1), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(d_tabs, tabs.data(), sizeof(float4) * tabs.size(), cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) {
-        rc = set_error(e == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "batch buffers: %s", cudaGetErrorString(e));
-    } else {
-        p->kp.insts = d_insts;
-        p->kp.inst_first = d_first;
-        p->kp.n_inst = n_inst;
-        p->fk = FK_BATCH;
-        p->smem_bytes = 0;
-        rc = grid_for(FK_BATCH, p->device, p->opts.blocks_per_sm, 0, &p->grid);
-        // the schedule from the tuner (trials on the sweep's first photons, cached per process),
-        // and each batch of march/event launches replayed as one CUDA graph once it is fixed
-        const char *tune_env = std::getenv("SMP_TUNE");
-        if (!rc && schedule_tune && total > 0 && p->kernel == SMP_KERNEL_POOL && !(tune_env && std::atoi(tune_env) == 0)) {
-            smp_tuning tt;
-            rc = plan_tune(p, std::min<long long>(total, 2000000LL), total, &tt);
-            if (!rc) {
-                e = cudaMemset(d_films, 0, px * bpp * size_t(n_inst));      // the trials' photons
-                if (e != cudaSuccess) rc = set_error(SMP_ERR_CUDA, "batch films: %s", cudaGetErrorString(e));
-            }
-        }
-        const char *graph_env = std::getenv("SMP_WF_GRAPH");
-        p->use_graph = !(graph_env && std::atoi(graph_env) == 0);
-        if (!rc) rc = smp_plan_clear(p, nullptr);
-        // the weight argument is unused: each instance carries its own Li T / N
-        if (!rc && total > 0) rc = launch(p, 0, total, 1, nullptr, nullptr, nullptr, nullptr);
-        int rs = rc ? rc : collect_stats(p);
-        if (stats_out) *stats_out = p->stats;
-        if (!rc) rc = rs;
-    }
-    std::string err = g_last_error;
-    cudaFree(d_insts);
-    cudaFree(d_first);
-    cudaFree(d_tabs);
-    if (rc) cudaFree(d_films);
-    else *d_films_out = d_films;
-    smp_plan_destroy(p);
-    g_last_error = err;
-    return rc;
+    cudaError_t e = cudaMemset(b.d_films, 0, b.film_bytes * size_t(b.n_inst));
+    if (e != cudaSuccess) return set_error(SMP_ERR_CUDA, "batch films: %s", cudaGetErrorString(e));
+    rc = smp_plan_clear(p, nullptr);
+    // the weight argument is unused: each instance carries its own Li T / N
+    if (!rc && b.total > 0) rc = launch(p, 0, b.total, 1, nullptr, nullptr, nullptr, nullptr);
+    const int rs = rc ? rc : collect_stats(p);
+    if (stats_out) *stats_out = p->stats;
+    return rc ? rc : rs;
 }
 
 int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *instances, int32_t n_inst,
                      const smp_render_opts *opts, double *images_out, smp_stats *stats_out) {
-    void *d_films = nullptr;
-    size_t fb = 0;
-    int rc = batch_run(scene, instances, n_inst, opts, true, &d_films, &fb, stats_out);
+    BatchRun b;
+    int rc = batch_open(scene, instances, n_inst, opts, b);
+    if (!rc) rc = batch_trace(b, true, stats_out);
     if (rc) return rc;
+    const size_t fb = b.film_bytes;
+    const void *d_films = b.d_films;
     if (images_out) {
+        // The films reach host memory that is usually fresh (a new array per call): its pages are
+        // first written on several threads, so that the copy, whose page faults one thread would
+        // take, finds them mapped.
         cudaError_t e;
         if (opts->precision == SMP_PREC_MIXED) {
-            e = cudaMemcpy(images_out, d_films, fb * size_t(n_inst), cudaMemcpyDeviceToHost);
+            const size_t cnt = fb / 8 * size_t(n_inst);
+            host_parallel(cnt, [images_out](size_t a, size_t b) { std::memset(images_out + a, 0, (b - a) * 8); });
+            e = cudaMemcpy(images_out, d_films, cnt * 8, cudaMemcpyDeviceToHost);
         } else {
-            // FP32 films, widened on the host by several threads (the copy's buffer is left
-            // uninitialised: the copy writes all of it)
+            // FP32 films through a staging buffer, widened on the host by several threads
             const size_t cnt = fb / 4 * size_t(n_inst);
             std::unique_ptr<float[]> h(new float[cnt]);
-            e = cudaMemcpy(h.get(), d_films, cnt * 4, cudaMemcpyDeviceToHost);
-            if (e == cudaSuccess) {
-                const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-                const size_t per = (cnt + hw - 1) / hw;
-                std::vector<std::thread> ts;
-                for (unsigned t = 0; t < hw; ++t) {
-                    const size_t a = std::min(cnt, t * per), b = std::min(cnt, a + per);
-                    ts.emplace_back([&h, images_out, a, b] { for (size_t j = a; j < b; ++j) images_out[j] = double(h[j]); });
-                }
-                for (auto &t : ts) t.join();
-            }
+            float *hp = h.get();
+            host_parallel(cnt, [hp](size_t a, size_t b) { std::memset(hp + a, 0, (b - a) * 4); });
+            e = cudaMemcpy(hp, d_films, cnt * 4, cudaMemcpyDeviceToHost);
+            if (e == cudaSuccess)
+                host_parallel(cnt, [hp, images_out](size_t a, size_t b) {
+                    for (size_t j = a; j < b; ++j) images_out[j] = double(hp[j]);
+                });
         }
         if (e != cudaSuccess) rc = set_error(SMP_ERR_CUDA, "batch films: %s", cudaGetErrorString(e));
     }
-    cudaFree(d_films);
     return rc;
 }
 
@@ -1759,17 +1798,23 @@ int tune_steps_group(const smp_scene_desc *scene, const smp_instance_desc *inst,
         miss[i] = inst[i].n_photons > 0 ? lim : 0;                 // nothing to search without photons
         trial[i].n_photons = std::min<int64_t>(inst[i].n_photons, n_sample);
     }
-    void *d_ref = nullptr, *d_try = nullptr;
-    double *d_acc = nullptr;
-    size_t fb = 0;
-    int rc = batch_run(scene, trial.data(), n, opts, false, &d_ref, &fb, nullptr);
+    // one sweep state for every round: the reference render, then each round's trial steps
+    BatchRun b;
+    int rc = batch_open(scene, trial.data(), n, opts, b);
+    if (!rc) rc = batch_trace(b, false, nullptr);
     ++*rounds;
+    void *d_ref = nullptr;
+    double *d_acc = nullptr;
+    const size_t fb = b.film_bytes;
     const int fp64 = opts->precision == SMP_PREC_MIXED;
     const size_t px = fb / (fp64 ? 8 : 4);
     std::vector<double> acc(2 * size_t(n));
     if (!rc) {
-        cudaError_t e = cudaMalloc(&d_acc, acc.size() * sizeof(double));
-        if (e != cudaSuccess) rc = set_error(SMP_ERR_OOM, "tuner buffers: %s", cudaGetErrorString(e));
+        cudaError_t e = cudaMalloc(&d_ref, fb * size_t(n));
+        if (e == cudaSuccess) e = cudaMalloc(&d_acc, acc.size() * sizeof(double));
+        if (e == cudaSuccess) e = cudaMemcpy(d_ref, b.d_films, fb * size_t(n), cudaMemcpyDeviceToDevice);
+        if (e != cudaSuccess)
+            rc = set_error(e == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "tuner buffers: %s", cudaGetErrorString(e));
     }
     for (bool first = true; !rc; first = false) {
         bool any = false;
@@ -1781,17 +1826,16 @@ int tune_steps_group(const smp_scene_desc *scene, const smp_instance_desc *inst,
             any = any || tr[i] >= 0;
         }
         if (!any) break;
-        rc = batch_run(scene, trial.data(), n, opts, false, &d_try, &fb, nullptr);
+        rc = batch_set(b, trial.data());
+        if (!rc) rc = batch_trace(b, false, nullptr);
         ++*rounds;
         if (rc) break;
         cudaError_t e = cudaMemset(d_acc, 0, acc.size() * sizeof(double));
         if (e == cudaSuccess) {
-            film_diff_kernel<<<dim3(64, unsigned(n)), 256>>>(d_try, d_ref, px, fp64, d_acc);
+            film_diff_kernel<<<dim3(64, unsigned(n)), 256>>>(b.d_films, d_ref, px, fp64, d_acc);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaMemcpy(acc.data(), d_acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost);
-        cudaFree(d_try);
-        d_try = nullptr;
         if (e != cudaSuccess) { rc = set_error(SMP_ERR_CUDA, "tuner films: %s", cudaGetErrorString(e)); break; }
         for (int i = 0; i < n; ++i) {
             if (tr[i] < 0) continue;
@@ -1803,7 +1847,6 @@ int tune_steps_group(const smp_scene_desc *scene, const smp_instance_desc *inst,
     }
     std::string err = g_last_error;
     cudaFree(d_ref);
-    cudaFree(d_try);
     cudaFree(d_acc);
     g_last_error = err;
     return rc;
