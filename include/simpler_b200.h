@@ -22,7 +22,8 @@
  *   smp_texture_cdf                <- area_textured_source texture CDF      renderer/src/area_textured_source.cpp:41-45
  *   smp_render_batch               <- the serial per-configuration loops    renderer/pybindFiles/tests/FUS_configurations.ipynb
  *                                     (one renderImage per configuration)   (cells at lines 591-603, 713-725)
- *   smp_batch_tune_steps           <- no counterpart: the reference's ER step is a fixed setting
+ *   smp_batch_tune_steps /         <- no counterpart: the reference's ER step is a fixed setting
+ *   smp_plan_tune_step
  *   smp_render_adjoint /           <- no counterpart: the reference has forward-mode tangents of
  *   smp_plan_adjoint                  single leapfrog steps only (er_derivativestep scene.cpp:351-359,
  *                                     bessel_HessianRIF :259-320, Spline::hessian spline.h:359-413),
@@ -313,6 +314,19 @@ typedef struct smp_tuning {
     double  paths_per_s;          /* its photon paths/s                                             */
 } smp_tuning;
 int smp_plan_tune(smp_plan *plan, int64_t n_sample, smp_tuning *out);
+
+/* Step-size autotuner for a plan (no counterpart in the reference, whose ER step is a fixed
+   setting): renders photons [0, n_sample) of the plan's render at the plan's own ER step (the
+   reference film) and at multiples of it (2, 3, 4, 6, 8, 12, 16, 24 or 32), on the same photons, and
+   sets the plan's step to the largest multiple whose film stays within rmse_budget relative RMSE
+   (sqrt(sum (film - ref)^2 / sum ref^2)) of the reference film -- the largest allowed multiple
+   first, then bisection, as smp_batch_tune_steps. The step stays at most an eighth of the field's
+   shortest wavelength (Bessel, plane waves, point sources at their highest harmonic) or a quarter
+   of a spline grid's finest spacing. Unless opts.sensor_march_max is set, the trial renders stop a
+   sensor march at 30 mean free paths (both films alike). *step_out receives the plan's new step,
+   rmse_out (may be NULL) the error measured at it (0 when the plan kept its step). The film is
+   cleared on return; smp_plan_set_field restores the field's own step. Not for batched sweeps. */
+int smp_plan_tune_step(smp_plan *plan, int64_t n_sample, double rmse_budget, double *step_out, double *rmse_out);
 
 /* Parity mode: traces n_photons with per-photon injected uniforms
    (photon i consumes uniforms[offsets[i] .. offsets[i+1]) ), or with the opts->rng stream when

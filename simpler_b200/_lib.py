@@ -165,7 +165,7 @@ EXPORTS = [
     "smp_plan_read_image", "smp_plan_film", "smp_plan_stats", "smp_plan_render", "smp_trace_photons",
     "smp_field_eval", "smp_texture_cdf", "smp_spline_prefilter", "smp_render_batch", "smp_fp32_peak",
     "smp_render_noalloc", "smp_adjoint_param_count", "smp_plan_adjoint", "smp_render_adjoint", "smp_plan_tune",
-    "smp_batch_tune_steps",
+    "smp_batch_tune_steps", "smp_plan_tune_step",
 ]
 
 _lib = None
@@ -208,6 +208,7 @@ def load() -> C.CDLL:
     lib.smp_texture_cdf.argtypes = [vp, C.c_int32, C.c_int32, vp]
     lib.smp_spline_prefilter.argtypes = [vp, vp, vp]
     lib.smp_render_batch.argtypes = [P(SceneDesc), P(InstanceDesc), C.c_int32, P(RenderOpts), vp, P(Stats)]
+    lib.smp_plan_tune_step.argtypes = [vp, C.c_int64, C.c_double, P(C.c_double), P(C.c_double)]
     lib.smp_batch_tune_steps.argtypes = [P(SceneDesc), P(InstanceDesc), C.c_int32, P(RenderOpts), C.c_int64,
                                          C.c_double, vp, vp, P(C.c_int32)]
     lib.smp_fp32_peak.argtypes = [C.c_int, P(C.c_double)]

@@ -1887,6 +1887,105 @@ int smp_batch_tune_steps(const smp_scene_desc *scene, const smp_instance_desc *i
     return SMP_OK;
 }
 
+// Step-size autotuner of a plan: the batched tuner's search (multiples from kStepMults, the largest
+// allowed first, then bisection) on photons [0, n_sample) of the plan's own render, against the
+// film at the plan's own step on the same photons. The cap on the step is the field's shortest
+// length scale: an eighth of the shortest wavelength of a Bessel, point-source (its highest
+// harmonic) or plane-wave field, a quarter of a spline grid's finest spacing.
+static double field_step_cap(const smp_plan *p) {
+    const FieldParams &F = p->kp.field;
+    const double two_pi = 6.283185307179586;
+    switch (p->fk) {
+        case FK_PLANEWAVE: {
+            double kmax = 0.0;
+            for (int i = 0; i < F.n_waves; ++i)
+                kmax = std::max(kmax, std::sqrt(double(F.wk[i][0]) * F.wk[i][0] + double(F.wk[i][1]) * F.wk[i][1] +
+                                                double(F.wk[i][2]) * F.wk[i][2]));
+            return kmax > 0.0 ? two_pi / kmax / 8.0 : HUGE_VAL;
+        }
+        case FK_SPLINE: {
+            double res = 0.0;
+            for (int a = 0; a < 3; ++a) res = std::max(res, double(F.xres[a]));
+            return res > 0.0 ? 0.25 / res : HUGE_VAL;
+        }
+        case FK_SOURCES:
+            return F.k_r > 0.0f ? two_pi / (double(F.k_r) * std::max(1, F.n_coeff)) / 8.0 : HUGE_VAL;
+        default:                                                   // Bessel, any order
+            return F.k_r > 0.0f ? two_pi / double(F.k_r) / 8.0 : HUGE_VAL;
+    }
+}
+
+static void plan_set_step(smp_plan *p, double h) {
+    p->kp.h0 = float(h);
+    step_table(h, p->kp.cur_tab);
+}
+
+extern "C" int smp_plan_tune_step(smp_plan *plan, int64_t n_sample, double rmse_budget, double *step_out,
+                                  double *rmse_out) {
+    if (!plan || !step_out) return set_error(SMP_ERR_BAD_ARG, "NULL argument");
+    if (n_sample <= 0) return set_error(SMP_ERR_BAD_ARG, "n_sample must be positive");
+    if (!(rmse_budget > 0.0)) return set_error(SMP_ERR_BAD_ARG, "rmse_budget must be positive");
+    if (plan->kp.n_inst) return set_error(SMP_ERR_UNSUPPORTED, "a batched sweep tunes its steps with smp_batch_tune_steps");
+    SMP_CUDA(cudaSetDevice(plan->device));
+    const double h0 = double(plan->kp.h0), cap = field_step_cap(plan);
+    int lim = 0;
+    while (lim < kNumStepMults && h0 * kStepMults[lim] <= cap) ++lim;
+    // The trial renders stop a sensor march at 30 mean free paths (as the batched tuner's do): the
+    // reference and trial films are cut alike and the rounds' tails are shorter.
+    const float large0 = plan->kp.large_dist;
+    if (plan->opts.sensor_march_max <= 0.0 && plan->kp.sigma_t > 1e-3f)
+        plan->kp.large_dist = std::min(large0, 30.0f / plan->kp.sigma_t);
+    const size_t fb = plan->film_elems * (plan->kp.fp64 ? 8 : 4);
+    void *d_ref = nullptr;
+    double *d_acc = nullptr;
+    cudaError_t e = cudaMalloc(&d_ref, fb);
+    if (e == cudaSuccess) e = cudaMalloc(&d_acc, 2 * sizeof(double));
+    int rc = e == cudaSuccess ? SMP_OK
+                              : set_error(e == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "tuner buffers: %s",
+                                          cudaGetErrorString(e));
+    // the reference film at the plan's own step
+    if (!rc) rc = smp_plan_clear(plan, nullptr);
+    if (!rc) rc = smp_plan_trace(plan, 0, n_sample, n_sample, nullptr);
+    if (!rc) {
+        e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaMemcpy(d_ref, plan->d_film, fb, cudaMemcpyDeviceToDevice);
+        if (e != cudaSuccess) rc = set_error(SMP_ERR_CUDA, "tuner films: %s", cudaGetErrorString(e));
+    }
+    int pass = -1, miss = lim;
+    double best_rmse = 0.0;
+    for (bool first = true; !rc && miss - pass > 1; first = false) {
+        const int t = first ? miss - 1 : (pass + miss) / 2;
+        plan_set_step(plan, h0 * kStepMults[t]);
+        rc = smp_plan_clear(plan, nullptr);
+        if (!rc) rc = smp_plan_trace(plan, 0, n_sample, n_sample, nullptr);
+        if (rc) break;
+        double acc[2] = {0.0, 0.0};
+        e = cudaMemset(d_acc, 0, sizeof(acc));
+        if (e == cudaSuccess) {
+            film_diff_kernel<<<dim3(148, 1), 256>>>(plan->d_film, d_ref, plan->film_elems, plan->kp.fp64, d_acc);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpy(acc, d_acc, sizeof(acc), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) { rc = set_error(SMP_ERR_CUDA, "tuner films: %s", cudaGetErrorString(e)); break; }
+        if (!(acc[1] > 0.0)) break;                            // empty reference film: keep the step
+        const double r = std::sqrt(acc[0] / acc[1]);
+        if (r <= rmse_budget) { pass = t; best_rmse = r; }
+        else miss = t;
+    }
+    std::string err = g_last_error;
+    cudaFree(d_ref);
+    cudaFree(d_acc);
+    g_last_error = err;
+    plan->kp.large_dist = large0;
+    plan_set_step(plan, pass >= 0 ? h0 * kStepMults[pass] : h0);
+    const int rc2 = smp_plan_clear(plan, nullptr);
+    if (rc) return rc;
+    if (rc2) return rc2;
+    *step_out = double(plan->kp.h0);
+    if (rmse_out) *rmse_out = pass >= 0 ? best_rmse : 0.0;
+    return SMP_OK;
+}
+
 // ---- adjoint ------------------------------------------------------------------------------------
 int64_t smp_adjoint_param_count(const smp_field_desc *f) {
     if (!f) return set_error(SMP_ERR_BAD_ARG, "NULL field");

@@ -93,6 +93,17 @@ class Plan:
         L.check(self.lib.smp_plan_tune(self.handle, int(n_sample), C.byref(t)))
         return t
 
+    def tune_step(self, n_sample: int, rmse_budget: float) -> tuple[float, float]:
+        """The step-size autotuner (smp_plan_tune_step): sets the plan's ER step to the largest
+        multiple (2 .. 32, capped by the field's shortest length scale) of its own whose film on
+        photons [0, n_sample) stays within `rmse_budget` relative RMSE of the film at its own step.
+        Returns (step in metres, measured RMSE). The film is cleared; set_field restores the
+        field's own step."""
+        step, rmse = C.c_double(), C.c_double()
+        L.check(self.lib.smp_plan_tune_step(self.handle, int(n_sample), float(rmse_budget), C.byref(step),
+                                            C.byref(rmse)))
+        return step.value, rmse.value
+
     def set_field(self, setup: Setup) -> None:
         fd = setup.field_desc()
         L.check(self.lib.smp_plan_set_field(self.handle, C.byref(fd)))
