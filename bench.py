@@ -482,6 +482,8 @@ def run_ours(args):
         if world == 1 and args.workload == "precision":
             # the north star's batched form against the plain kernel, beside the headline
             out["batched_form"] = batched_form(args, False)
+        if world == 1 and args.workload == "plain":
+            out["tuned_step"] = plan_tuned_step(args, setup, per_step)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -518,6 +520,36 @@ def run_plain(args, setup, per_step: int, device: int, first_step: int, steps: i
             "kernel": "plain_kernel: one thread per photon, one launch per step (cuda_renderer.cu:681-725 structure)",
             "precision": "fp32 march, fp32 path length, fp32 film atomics",
             "er_steps_per_s": (st.er_steps - st0.er_steps) / (ms / 1e3)}
+
+
+def plan_tuned_step(args, setup, per_step: int) -> dict:
+    """The same workload with the plan's ER step from the step-size autotuner (smp_plan_tune_step on
+    the render's first 2e4 photons, within --step-budget of the film at the workload's own step),
+    device-timed over --steps renders of per_step photons, and its image against the FP64 oracle at
+    the own step on 2e4 photons (the oracle as the checker)."""
+    plan = sb.Plan(setup)
+    plan.tune(min(per_step, 5_000_000))
+    t0 = time.perf_counter()
+    step, rmse = plan.tune_step(20000, args.step_budget)
+    t_tune = time.perf_counter() - t0
+    ms = 0.0
+    for i in range(args.steps):
+        plan.clear(0)
+        st0 = plan.stats()
+        plan.trace((args.warmup + i) * per_step, per_step, render_photons(args), 0)
+        ms += plan.stats().kernel_ms - st0.kernel_ms
+    n = 20000
+    film, _ = plan.render(n)
+    plan.close()
+    sc, md, fd, op = setup.descs()
+    lib = _oracle_lib(fast=False)
+    ref = np.zeros(setup.film_shape(), dtype=np.float64)
+    assert lib.orc_render(C.byref(sc), C.byref(md), C.byref(fd), C.byref(op), 64, os.cpu_count() or 1, 0, n, n,
+                          None, None, None, C.c_void_p(ref.ctypes.data)) == 0
+    return {"value": per_step * args.steps / (ms / 1e3), "unit": METRIC, "step_m": step,
+            "step_multiple": step / setup.er_stepsize, "tuner_seconds": t_tune, "tuner_rmse": rmse,
+            "image_rmse_vs_fp64": float(np.sqrt(((film - ref) ** 2).sum() / (ref ** 2).sum())),
+            "image_photons": n, "call": "Plan.tune_step then device-timed traces (smp_plan_trace)"}
 
 
 def _profile_traffic(slots_per_lane: int):
