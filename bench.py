@@ -689,10 +689,11 @@ def batched_form(args, with_reference_legs: bool) -> dict:
     if with_reference_legs:
         extra["nominal_step"]["speedup_vs_plain"] = extra["nominal_step"]["value"] / plain_rate
     # image check against the FP64 oracle: the hardest field (largest n_max x f), the instance with
-    # the largest multiple, and instance 0
+    # the largest multiple, the one with the largest error the tuner measured, and instance 0
     hard = max(range(len(insts)), key=lambda i: insts[i]["n_max"] * insts[i]["f_u"])
     big = int(np.argmax(mults))
-    check = sweep_image_check(setup, insts, [(i, steps[i]) for i in sorted({hard, big, 0})], 10000,
+    worst = int(np.argmax(rmse))                # the largest error the tuner measured
+    check = sweep_image_check(setup, insts, [(i, steps[i]) for i in sorted({hard, big, worst, 0})], 10000,
                               os.cpu_count() or 1)
     hist = {str(m): int((np.rint(mults) == m).sum()) for m in (1, 2, 3, 4, 6, 8, 12, 16, 24, 32)}
     out = {

@@ -316,16 +316,20 @@ typedef struct smp_tuning {
 int smp_plan_tune(smp_plan *plan, int64_t n_sample, smp_tuning *out);
 
 /* Step-size autotuner for a plan (no counterpart in the reference, whose ER step is a fixed
-   setting): renders photons [0, n_sample) of the plan's render at the plan's own ER step (the
+   setting): renders photons [0, n_sample) of the plan's render at its field's own ER step (the
    reference film) and at multiples of it (2, 3, 4, 6, 8, 12, 16, 24 or 32), on the same photons, and
    sets the plan's step to the largest multiple whose film stays within rmse_budget relative RMSE
    (sqrt(sum (film - ref)^2 / sum ref^2)) of the reference film -- the largest allowed multiple
-   first, then bisection, as smp_batch_tune_steps. The step stays at most an eighth of the field's
+   first, then bisection, as smp_batch_tune_steps. The search renders in the mixed form, as there: a
+   plan of the FP32 form searches on a mixed-form copy of itself, except a spline plan (its
+   coefficients are the caller's host memory), which searches in its own form, where the float path
+   length's rounding counts against the budget too. The step stays at most an eighth of the field's
    shortest wavelength (Bessel, plane waves, point sources at their highest harmonic) or a quarter
-   of a spline grid's finest spacing. Unless opts.sensor_march_max is set, the trial renders stop a
-   sensor march at 30 mean free paths (both films alike). *step_out receives the plan's new step,
-   rmse_out (may be NULL) the error measured at it (0 when the plan kept its step). The film is
-   cleared on return; smp_plan_set_field restores the field's own step. Not for batched sweeps. */
+   of a spline grid's finest spacing. Unless opts.sensor_march_max is set, the tuner's renders stop a
+   sensor march at 30 mean free paths (all films alike). *step_out receives the plan's new step,
+   rmse_out (may be NULL) the error measured at it. The film is cleared on return; a second call
+   starts again from the field's own step; smp_plan_set_field restores that step. Not for batched
+   sweeps. */
 int smp_plan_tune_step(smp_plan *plan, int64_t n_sample, double rmse_budget, double *step_out, double *rmse_out);
 
 /* Parity mode: traces n_photons with per-photon injected uniforms
@@ -358,23 +362,24 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
 
 /* Step-size autotuner for a batched sweep (no counterpart in the reference, whose ER step is a fixed
    setting). For each instance it renders photons [0, min(n_photons, n_sample)) at the instance's own
-   field.er_stepsize (its reference film) and at multiples of that step (2, 3, 4, 6, 8, 12, 16, 24 or
-   32, none above an eighth of the instance's ultrasound wavelength speed_u / f_u) on the same Philox
-   photons, and keeps the largest multiple whose film stays within rmse_budget relative RMSE
-   (sqrt(sum (film - ref)^2 / sum ref^2)) of the reference film. It tries the largest allowed
-   multiple first and, where that misses, bisects between the multiples known to pass and to miss
-   (the error grows with the step); each round is one batched render of the instances still
-   searching. An instance with no photons or an empty reference film keeps its own step. Unless
-   opts->sensor_march_max is set, the trial renders stop a sensor march at 30 mean free paths of the
-   thinnest medium, which cuts the reference and trial films alike by less than e^-30 of a photon's
-   weight and shortens the rounds' tails.
-   steps_out[i] receives instance i's chosen er_stepsize; rmse_out[i] (may be NULL) the relative RMSE
-   measured at that step (0 where the instance kept its own); rounds_out (may be NULL) the number of
-   batched renders. The budget is against this library's own render at the nominal step: the image
-   error against an exact solution adds the nominal step's own error. Set
-   instances[i].field.er_stepsize = steps_out[i] and call smp_render_batch. The search holds a
-   reference and a trial film per instance, so instances are tuned in groups whose films fit in 40 %
-   of the free device memory (SMP_ERR_OOM when not even one instance's two films fit). */
+   field.er_stepsize (the reference film) and at multiples of that step (2, 3, 4, 6, 8, 12, 16, 24 or
+   32, none above an eighth of the instance's ultrasound wavelength speed_u / f_u), on the same
+   Philox photons, and keeps the largest multiple whose film stays within rmse_budget relative RMSE
+   (sqrt(sum (film - ref)^2 / sum ref^2)) of the reference film. These renders are all in the mixed
+   form (FP64 path length and film), whatever opts->precision says: in the FP32 form the float path
+   length rounds differently at every step, the own one included, and moves photons across
+   path-length bins, which the step does not cause and the FP32 render keeps at any step. It tries
+   the largest allowed multiple first and, where that misses, bisects between the multiples known to
+   pass and to miss (the error grows with the step); each round is one batched render of the
+   instances still searching. An instance with no photons or an empty reference film keeps its own
+   step. Unless opts->sensor_march_max is set, the tuner's renders stop a sensor march at 30 mean free
+   paths of the thinnest medium, which cuts the compared films alike by less than e^-30 of a photon's
+   weight and shortens the rounds' tails. steps_out[i] receives instance i's chosen er_stepsize;
+   rmse_out[i] (may be NULL) the relative RMSE measured at that step (0 where the instance kept its
+   own); rounds_out (may be NULL) the number of batched renders. Set
+   instances[i].field.er_stepsize = steps_out[i] and call smp_render_batch. Instances are tuned in
+   groups that fit in 40 % of the free device memory at 16 bytes per film pixel each (SMP_ERR_OOM
+   when not even one fits). */
 int smp_batch_tune_steps(const smp_scene_desc *scene, const smp_instance_desc *instances,
                          int32_t n_inst, const smp_render_opts *opts, int64_t n_sample,
                          double rmse_budget, double *steps_out, double *rmse_out, int32_t *rounds_out);

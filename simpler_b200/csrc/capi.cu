@@ -1721,15 +1721,15 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
     return rc;
 }
 
-// Per instance i (blockIdx.y): sum (a - r)^2 and sum r^2 over its film of px pixels (float, or
-// double when fp64), accumulated in double into acc[2i], acc[2i + 1].
-__global__ void film_diff_kernel(const void *a, const void *r, size_t px, int fp64, double *acc) {
+// Per instance i (blockIdx.y): sum (a - r)^2 and sum r^2 over its film of px pixels (each film float,
+// or double when its flag is set), accumulated in double into acc[2i], acc[2i + 1].
+__global__ void film_diff_kernel(const void *a, int a64, const void *r, int r64, size_t px, double *acc) {
     __shared__ double sd[32], sr[32];
     const size_t base = size_t(blockIdx.y) * px;
     double d2 = 0.0, r2 = 0.0;
     for (size_t j = size_t(blockIdx.x) * blockDim.x + threadIdx.x; j < px; j += size_t(gridDim.x) * blockDim.x) {
-        const double av = fp64 ? static_cast<const double *>(a)[base + j] : double(static_cast<const float *>(a)[base + j]);
-        const double rv = fp64 ? static_cast<const double *>(r)[base + j] : double(static_cast<const float *>(r)[base + j]);
+        const double av = a64 ? static_cast<const double *>(a)[base + j] : double(static_cast<const float *>(a)[base + j]);
+        const double rv = r64 ? static_cast<const double *>(r)[base + j] : double(static_cast<const float *>(r)[base + j]);
         d2 += (av - rv) * (av - rv);
         r2 += rv * rv;
     }
@@ -1798,21 +1798,26 @@ int tune_steps_group(const smp_scene_desc *scene, const smp_instance_desc *inst,
         miss[i] = inst[i].n_photons > 0 ? lim : 0;                 // nothing to search without photons
         trial[i].n_photons = std::min<int64_t>(inst[i].n_photons, n_sample);
     }
-    // one sweep state for every round: the reference render, then each round's trial steps
+    // Every render of the search is in the mixed form (FP64 path length and film), whatever the
+    // sweep's own form. In the FP32 form the path length is accumulated in float and a different
+    // number of steps rounds it differently, which moves photons near a path-length bin edge to the
+    // next bin -- at any step, the own one included, and for a few large splats (connections in the
+    // Henyey-Greenstein peak) by more than the budget. In the mixed form the films differ by the
+    // step's own effect on the march, which is what the step decides; the FP32 render then carries
+    // the same kind of float rounding at the chosen step as at its own.
+    topts.precision = SMP_PREC_MIXED;
     BatchRun b;
     int rc = batch_open(scene, trial.data(), n, opts, b);
     if (!rc) rc = batch_trace(b, false, nullptr);
     ++*rounds;
     void *d_ref = nullptr;
     double *d_acc = nullptr;
-    const size_t fb = b.film_bytes;
-    const int fp64 = opts->precision == SMP_PREC_MIXED;
-    const size_t px = fb / (fp64 ? 8 : 4);
+    const size_t px = b.film_bytes / 8;
     std::vector<double> acc(2 * size_t(n));
     if (!rc) {
-        cudaError_t e = cudaMalloc(&d_ref, fb * size_t(n));
+        cudaError_t e = cudaMalloc(&d_ref, b.film_bytes * size_t(n));
         if (e == cudaSuccess) e = cudaMalloc(&d_acc, acc.size() * sizeof(double));
-        if (e == cudaSuccess) e = cudaMemcpy(d_ref, b.d_films, fb * size_t(n), cudaMemcpyDeviceToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(d_ref, b.d_films, b.film_bytes * size_t(n), cudaMemcpyDeviceToDevice);
         if (e != cudaSuccess)
             rc = set_error(e == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "tuner buffers: %s", cudaGetErrorString(e));
     }
@@ -1832,7 +1837,7 @@ int tune_steps_group(const smp_scene_desc *scene, const smp_instance_desc *inst,
         if (rc) break;
         cudaError_t e = cudaMemset(d_acc, 0, acc.size() * sizeof(double));
         if (e == cudaSuccess) {
-            film_diff_kernel<<<dim3(64, unsigned(n)), 256>>>(b.d_films, d_ref, px, fp64, d_acc);
+            film_diff_kernel<<<dim3(64, unsigned(n)), 256>>>(b.d_films, 1, d_ref, 1, px, d_acc);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaMemcpy(acc.data(), d_acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost);
@@ -1861,14 +1866,13 @@ int smp_batch_tune_steps(const smp_scene_desc *scene, const smp_instance_desc *i
     if (!(rmse_budget > 0.0)) return set_error(SMP_ERR_BAD_ARG, "rmse_budget must be positive");
     int rc = check_device(opts->device);
     if (rc) return rc;
-    // instances per group: two films each within 40 % of the free memory (at most 65535, the
-    // difference kernel's grid height)
+    // instances per group: within 40 % of the free memory, 16 bytes per pixel each (the FP64
+    // reference film and an FP64 trial film), at most 65535 (the difference kernel's grid height)
     size_t free_b = 0, total_b = 0;
     SMP_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t film = size_t(scene->x_res) * size_t(scene->y_res) * size_t(scene->z_res) *
-                        (opts->precision == SMP_PREC_MIXED ? 8 : 4);
-    const size_t fit = film ? size_t(double(free_b) * 0.4) / (2 * film) : size_t(n_inst);
-    if (fit == 0) return set_error(SMP_ERR_OOM, "the step tuner needs two films of %zu bytes; %zu bytes are free", film, free_b);
+    const size_t film = size_t(scene->x_res) * size_t(scene->y_res) * size_t(scene->z_res) * 16;
+    const size_t fit = film ? size_t(double(free_b) * 0.4) / film : size_t(n_inst);
+    if (fit == 0) return set_error(SMP_ERR_OOM, "the step tuner needs %zu bytes per instance; %zu bytes are free", film, free_b);
     const int group = int(std::min<size_t>({size_t(n_inst), fit, size_t(65535)}));
     std::vector<int> pass(n_inst, -1);
     std::vector<double> rmse(n_inst, 0.0);
@@ -1881,7 +1885,7 @@ int smp_batch_tune_steps(const smp_scene_desc *scene, const smp_instance_desc *i
     if (rc) return rc;
     for (int i = 0; i < n_inst; ++i) {
         steps_out[i] = instances[i].field.er_stepsize * (pass[i] >= 0 ? kStepMults[pass[i]] : 1);
-        if (rmse_out) rmse_out[i] = pass[i] >= 0 ? rmse[i] : 0.0;
+        if (rmse_out) rmse_out[i] = rmse[i];
     }
     if (rounds_out) *rounds_out = rounds;
     return SMP_OK;
@@ -1927,7 +1931,9 @@ extern "C" int smp_plan_tune_step(smp_plan *plan, int64_t n_sample, double rmse_
     if (!(rmse_budget > 0.0)) return set_error(SMP_ERR_BAD_ARG, "rmse_budget must be positive");
     if (plan->kp.n_inst) return set_error(SMP_ERR_UNSUPPORTED, "a batched sweep tunes its steps with smp_batch_tune_steps");
     SMP_CUDA(cudaSetDevice(plan->device));
-    const double h0 = double(plan->kp.h0), cap = field_step_cap(plan);
+    // multiples of the field's own step (a plan tuned before starts again from it)
+    const double h0 = double(float(plan->field.er_stepsize)), cap = field_step_cap(plan);
+    plan_set_step(plan, h0);
     int lim = 0;
     while (lim < kNumStepMults && h0 * kStepMults[lim] <= cap) ++lim;
     // The trial renders stop a sensor march at 30 mean free paths (as the batched tuner's do): the
@@ -1935,34 +1941,52 @@ extern "C" int smp_plan_tune_step(smp_plan *plan, int64_t n_sample, double rmse_
     const float large0 = plan->kp.large_dist;
     if (plan->opts.sensor_march_max <= 0.0 && plan->kp.sigma_t > 1e-3f)
         plan->kp.large_dist = std::min(large0, 30.0f / plan->kp.sigma_t);
-    const size_t fb = plan->film_elems * (plan->kp.fp64 ? 8 : 4);
+    // The search renders in the mixed form (FP64 path length and film), as smp_batch_tune_steps'
+    // does: a plan of the FP32 form whose field is held by value searches on a mixed-form twin and
+    // takes the chosen step back. (A spline's coefficients are the caller's host memory, so an FP32
+    // spline plan searches in its own form, where the float path length's rounding, different at
+    // every step, counts against the budget too.)
+    const bool twin = plan->kp.fp64 == 0 && plan->field.type != SMP_FIELD_SPLINE;
+    smp_plan *q = plan;                                        // the plan the search renders with
+    int rc = SMP_OK;
+    if (twin) {
+        smp_render_opts ro = plan->opts;
+        ro.precision = SMP_PREC_MIXED;
+        if (ro.sensor_march_max <= 0.0 && plan->kp.sigma_t > 1e-3f) ro.sensor_march_max = 30.0 / double(plan->kp.sigma_t);
+        q = nullptr;
+        rc = smp_plan_create(&plan->scene, &plan->medium, &plan->field, &ro, &q);
+    }
+    const size_t px = plan->film_elems;
+    const int q64 = q ? q->kp.fp64 : 0;
+    const size_t fb = px * (q64 ? 8 : 4);
     void *d_ref = nullptr;
     double *d_acc = nullptr;
-    cudaError_t e = cudaMalloc(&d_ref, fb);
-    if (e == cudaSuccess) e = cudaMalloc(&d_acc, 2 * sizeof(double));
-    int rc = e == cudaSuccess ? SMP_OK
-                              : set_error(e == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "tuner buffers: %s",
-                                          cudaGetErrorString(e));
-    // the reference film at the plan's own step
-    if (!rc) rc = smp_plan_clear(plan, nullptr);
-    if (!rc) rc = smp_plan_trace(plan, 0, n_sample, n_sample, nullptr);
+    cudaError_t e = cudaSuccess;
+    if (!rc) {
+        e = cudaMalloc(&d_acc, 2 * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&d_ref, fb);
+        if (e != cudaSuccess) rc = set_error(SMP_ERR_OOM, "tuner buffers: %s", cudaGetErrorString(e));
+    }
+    // the reference film: the own step
+    if (!rc) rc = smp_plan_clear(q, nullptr);
+    if (!rc) rc = smp_plan_trace(q, 0, n_sample, n_sample, nullptr);
     if (!rc) {
         e = cudaDeviceSynchronize();
-        if (e == cudaSuccess) e = cudaMemcpy(d_ref, plan->d_film, fb, cudaMemcpyDeviceToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(d_ref, q->d_film, fb, cudaMemcpyDeviceToDevice);
         if (e != cudaSuccess) rc = set_error(SMP_ERR_CUDA, "tuner films: %s", cudaGetErrorString(e));
     }
     int pass = -1, miss = lim;
     double best_rmse = 0.0;
     for (bool first = true; !rc && miss - pass > 1; first = false) {
         const int t = first ? miss - 1 : (pass + miss) / 2;
-        plan_set_step(plan, h0 * kStepMults[t]);
-        rc = smp_plan_clear(plan, nullptr);
-        if (!rc) rc = smp_plan_trace(plan, 0, n_sample, n_sample, nullptr);
+        plan_set_step(q, h0 * kStepMults[t]);
+        rc = smp_plan_clear(q, nullptr);
+        if (!rc) rc = smp_plan_trace(q, 0, n_sample, n_sample, nullptr);
         if (rc) break;
         double acc[2] = {0.0, 0.0};
         e = cudaMemset(d_acc, 0, sizeof(acc));
         if (e == cudaSuccess) {
-            film_diff_kernel<<<dim3(148, 1), 256>>>(plan->d_film, d_ref, plan->film_elems, plan->kp.fp64, d_acc);
+            film_diff_kernel<<<dim3(148, 1), 256>>>(q->d_film, q64, d_ref, q64, px, d_acc);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaMemcpy(acc, d_acc, sizeof(acc), cudaMemcpyDeviceToHost);
@@ -1971,6 +1995,13 @@ extern "C" int smp_plan_tune_step(smp_plan *plan, int64_t n_sample, double rmse_
         const double r = std::sqrt(acc[0] / acc[1]);
         if (r <= rmse_budget) { pass = t; best_rmse = r; }
         else miss = t;
+    }
+    if (twin && q) {
+        const std::string err = g_last_error;
+        smp_plan_destroy(q);
+        g_last_error = err;
+        e = cudaSetDevice(plan->device);
+        if (!rc && e != cudaSuccess) rc = set_error(SMP_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
     }
     std::string err = g_last_error;
     cudaFree(d_ref);
@@ -1982,7 +2013,7 @@ extern "C" int smp_plan_tune_step(smp_plan *plan, int64_t n_sample, double rmse_
     if (rc) return rc;
     if (rc2) return rc2;
     *step_out = double(plan->kp.h0);
-    if (rmse_out) *rmse_out = pass >= 0 ? best_rmse : 0.0;
+    if (rmse_out) *rmse_out = best_rmse;
     return SMP_OK;
 }
 

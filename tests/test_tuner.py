@@ -76,6 +76,20 @@ def test_plan_tune_step_within_budget_and_against_fp64_oracle():
     again, _ = p.render(n)
     assert np.abs(again - nominal).sum() <= 1e-12 * np.abs(nominal).sum()     # the own step again
     p.close()
+    # the FP32 form: the search runs on a mixed-form copy of the plan, so the float path length's
+    # own rounding does not hold the step at its own value
+    f = sb.config_plain_small()
+    assert f.precision_mode == L.PREC_FP32
+    r = sb.Plan(f)
+    nominal32, _ = r.render(n)
+    step, rmse = r.tune_step(n, budget)
+    m = step / f.er_stepsize
+    assert abs(m - round(m)) < 1e-4 and round(m) in (4, 6, 8, 12, 16), m
+    assert 0.0 < rmse <= budget
+    tuned32, _ = r.render(n)
+    r.close()
+    e_tuned, e_nominal = _rel(tuned32, ref), _rel(nominal32, ref)
+    assert e_tuned <= 1e-2 and e_tuned <= max(budget, e_nominal) + budget, (e_tuned, e_nominal)
     w = sb.config_planewave()
     q = sb.Plan(w)
     step, rmse = q.tune_step(10000, budget)
