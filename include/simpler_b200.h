@@ -371,8 +371,11 @@ int smp_render_batch(const smp_scene_desc *scene, const smp_instance_desc *insta
    path-length bins, which the step does not cause and the FP32 render keeps at any step. It tries
    the largest allowed multiple first and, where that misses, bisects between the multiples known to
    pass and to miss (the error grows with the step); each round is one batched render of the
-   instances still searching. An instance with no photons or an empty reference film keeps its own
-   step. Unless opts->sensor_march_max is set, the tuner's renders stop a sensor march at 30 mean free
+   instances still searching. An instance that misses at every multiple and has more than n_sample
+   photons searches once more with 10 n_sample photons (a small film led by a few large splats moves
+   by about the same amount at any step change, which more photons average out). An instance with
+   no photons or an empty reference film keeps its own step. Unless opts->sensor_march_max is set,
+   the tuner's renders stop a sensor march at 30 mean free
    paths of the thinnest medium, which cuts the compared films alike by less than e^-30 of a photon's
    weight and shortens the rounds' tails. steps_out[i] receives instance i's chosen er_stepsize;
    rmse_out[i] (may be NULL) the relative RMSE measured at that step (0 where the instance kept its

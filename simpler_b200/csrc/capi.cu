@@ -1883,6 +1883,28 @@ int smp_batch_tune_steps(const smp_scene_desc *scene, const smp_instance_desc *i
                               rmse.data() + g0, &rounds);
     }
     if (rc) return rc;
+    // A film of n_sample photons can be led by a few large splats (connections in the
+    // Henyey-Greenstein peak), and any change of step moves some of them: then every multiple misses
+    // by about the same amount, which the step does not cause and more photons average out. The
+    // instances that kept their own step although they have more photons search once more with ten
+    // times the sample.
+    std::vector<int> again;
+    for (int i = 0; i < n_inst; ++i)
+        if (pass[i] < 0 && instances[i].n_photons > n_sample) again.push_back(i);
+    if (!again.empty()) {
+        std::vector<smp_instance_desc> sub(again.size());
+        for (size_t j = 0; j < again.size(); ++j) sub[j] = instances[again[j]];
+        std::vector<int> pass2(sub.size(), -1);
+        std::vector<double> rmse2(sub.size(), 0.0);
+        const int64_t n2 = n_sample * 10;
+        for (int g0 = 0; g0 < int(sub.size()) && !rc; g0 += group) {
+            const int gn = std::min(group, int(sub.size()) - g0);
+            rc = tune_steps_group(scene, sub.data() + g0, gn, opts, n2, rmse_budget, pass2.data() + g0,
+                                  rmse2.data() + g0, &rounds);
+        }
+        if (rc) return rc;
+        for (size_t j = 0; j < again.size(); ++j) { pass[again[j]] = pass2[j]; rmse[again[j]] = rmse2[j]; }
+    }
     for (int i = 0; i < n_inst; ++i) {
         steps_out[i] = instances[i].field.er_stepsize * (pass[i] >= 0 ? kStepMults[pass[i]] : 1);
         if (rmse_out) rmse_out[i] = rmse[i];
