@@ -1889,8 +1889,11 @@ int smp_batch_tune_steps(const smp_scene_desc *scene, const smp_instance_desc *i
     // instances that kept their own step although they have more photons search once more with ten
     // times the sample.
     std::vector<int> again;
-    for (int i = 0; i < n_inst; ++i)
-        if (pass[i] < 0 && instances[i].n_photons > n_sample) again.push_back(i);
+    for (int i = 0; i < n_inst; ++i) {
+        const smp_field_desc &f = instances[i].field;
+        const bool allowed = f.er_stepsize * kStepMults[0] <= f.speed_u / f.f_u / 8.0;   // any multiple at all
+        if (pass[i] < 0 && allowed && instances[i].n_photons > n_sample) again.push_back(i);
+    }
     if (!again.empty()) {
         std::vector<smp_instance_desc> sub(again.size());
         for (size_t j = 0; j < again.size(); ++j) sub[j] = instances[again[j]];
