@@ -65,6 +65,29 @@ static void texture_cdf(const double *tex, int n, std::vector<float> &cdf) {
     }
 }
 
+// Guide table of a texture CDF (KParams::cdf_guide): 2^bits buckets in u, at least 256 and about one
+// per CDF entry (at most 2^20); entry b is the lower bound of b / 2^bits (exact in float), the last
+// is the end. Returns 0 (no guide) when the CDF is not non-decreasing (a negative texel, or the last
+// entry set to 1 below its predecessor's rounding): a binary search over unsorted entries depends on
+// the order of its probes, and a narrowed search could then differ from the full one.
+static int cdf_guide(const std::vector<float> &cdf, std::vector<int> &guide) {
+    const int n1 = int(cdf.size());
+    for (int i = 1; i < n1; ++i)
+        if (!(cdf[i] >= cdf[i - 1])) return 0;
+    int bits = 8;
+    while ((1 << bits) < n1 - 1 && bits < 20) ++bits;
+    const int G = 1 << bits;
+    guide.assign(size_t(G) + 2, 0);
+    int i = 0;
+    for (int b = 0; b <= G; ++b) {
+        const float t = float(b) / float(G);
+        while (i < n1 && cdf[i] < t) ++i;
+        guide[b] = i;
+    }
+    guide[size_t(G) + 1] = n1;
+    return bits;
+}
+
 // Spline<3>::build1d (renderer/include/spline.h:686-714): causal + anticausal recursive filter,
 // pole z1 = sqrt(3) - 2, mirror boundary.
 static void prefilter_1d(const float *data, long off, long stride, int size, float *out) {
@@ -751,11 +774,17 @@ int smp_plan_create(const smp_scene_desc *scene, const smp_medium_desc *medium, 
     k.rng = opts->rng;
     k.seed = opts->seed;
 
-    // texture CDF
+    // texture CDF, and its guide table in the same allocation
     std::vector<float> cdf;
     texture_cdf(scene->texture, k.n_tex, cdf);
-    cudaError_t e = cudaMalloc(&p->d_cdf, cdf.size() * sizeof(float));
+    std::vector<int> guide;
+    const int gbits = cdf_guide(cdf, guide);
+    const size_t cdf_bytes = (cdf.size() * sizeof(float) + 15) & ~size_t(15);
+    cudaError_t e = cudaMalloc(&p->d_cdf, cdf_bytes + guide.size() * sizeof(int));
     if (e == cudaSuccess) e = cudaMemcpy(p->d_cdf, cdf.data(), cdf.size() * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && gbits)
+        e = cudaMemcpy(reinterpret_cast<char *>(p->d_cdf) + cdf_bytes, guide.data(), guide.size() * sizeof(int),
+                       cudaMemcpyHostToDevice);
     p->film_elems = size_t(k.X) * k.Y * k.Z;
     if (e == cudaSuccess) e = cudaMalloc(&p->d_film, p->film_elems * (k.fp64 ? 8 : 4));
     if (e == cudaSuccess) e = cudaMalloc(&p->d_counters, CNT_COUNT * sizeof(unsigned long long));
@@ -766,6 +795,8 @@ int smp_plan_create(const smp_scene_desc *scene, const smp_medium_desc *medium, 
         return set_error(e == cudaErrorMemoryAllocation ? SMP_ERR_OOM : SMP_ERR_CUDA, "plan allocation: %s", cudaGetErrorString(e));
     }
     k.cdf = p->d_cdf;
+    k.cdf_guide = gbits ? reinterpret_cast<const int *>(reinterpret_cast<const char *>(p->d_cdf) + cdf_bytes) : nullptr;
+    k.guide_bits = gbits;
     k.film = p->d_film;
     k.counters = p->d_counters;
     rc = plan_setup_field(p, *field);

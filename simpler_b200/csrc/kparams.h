@@ -83,6 +83,11 @@ struct KParams {
     float ct;
     int tex_x, n_tex;
     const float *cdf;       // n_tex + 1 entries
+    // Guide table of the CDF (NULL: none): for bucket b of 2^guide_bits in u, cdf_guide[b] is the
+    // lower bound of b / 2^guide_bits in the CDF (b = 0 .. 2^guide_bits), cdf_guide[2^guide_bits + 1]
+    // = n_tex + 1; the lower bound of any u in the bucket lies in [cdf_guide[b], cdf_guide[b + 1]].
+    const int *cdf_guide;
+    int guide_bits;
     int src_lens_active;
     float src_lens_origin[3], src_lens_sqap, src_lens_focal;
     // camera

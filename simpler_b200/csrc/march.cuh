@@ -325,6 +325,14 @@ __device__ __forceinline__ bool roulette(Lane &L, const KParams &P) {
 __device__ __forceinline__ bool gen_ray(Lane &L, const KParams &P, float3 &pos, float3 &dir, double &total) {
     float u = draw(L, P);
     int lo = 0, hi = P.n_tex + 1;                 // lower_bound over n_tex + 1 cdf entries
+    if (P.cdf_guide) {
+        // u's bucket of the guide table narrows the search to a few entries; the CDF is monotone
+        // (the host builds no guide otherwise), so the lower bound found is the same
+        const int G = 1 << P.guide_bits;
+        const int b = min(int(u * float(G)), G);
+        lo = __ldg(P.cdf_guide + b);
+        hi = __ldg(P.cdf_guide + b + 1);
+    }
     while (lo < hi) {
         int mid = (lo + hi) >> 1;
         if (__ldg(P.cdf + mid) < u) lo = mid + 1; else hi = mid;
