@@ -95,10 +95,11 @@ class Plan:
 
     def tune_step(self, n_sample: int, rmse_budget: float) -> tuple[float, float]:
         """The step-size autotuner (smp_plan_tune_step): sets the plan's ER step to the largest
-        multiple (2 .. 32, capped by the field's shortest length scale) of its own whose film on
-        photons [0, n_sample) stays within `rmse_budget` relative RMSE of the film at its own step.
-        Returns (step in metres, measured RMSE). The film is cleared; set_field restores the
-        field's own step."""
+        multiple (2 .. 32, capped by the field's shortest length scale) of the field's own step whose
+        film on photons [0, n_sample) stays within `rmse_budget` relative RMSE of the film at the own
+        step (searched in the mixed form; an FP32 plan uses a mixed-form copy of itself, except a
+        spline plan). Returns (step in metres, measured RMSE). The film is cleared; set_field
+        restores the field's own step."""
         step, rmse = C.c_double(), C.c_double()
         L.check(self.lib.smp_plan_tune_step(self.handle, int(n_sample), float(rmse_budget), C.byref(step),
                                             C.byref(rmse)))
@@ -157,8 +158,10 @@ def tune_batch_steps(setup: Setup, instances: list, rmse_budget: float, n_sample
     """The step-size autotuner of a batched sweep (smp_batch_tune_steps): per instance, the largest
     multiple (2 .. 32, at most an eighth of the ultrasound wavelength) of its ER step whose film on
     its first n_sample photons stays within `rmse_budget` relative RMSE of the film at its own step,
-    on the same photons (largest allowed multiple first, then bisection). Returns (steps, rmse,
-    rounds); pass {"er_stepsize": steps[i]} into instance i for render_batch."""
+    on the same photons (largest allowed multiple first, then bisection; the search renders in the
+    mixed form, and an instance that misses at every multiple searches again with 10 n_sample
+    photons). Returns (steps, rmse, rounds); pass {"er_stepsize": steps[i]} into instance i for
+    render_batch."""
     lib = L.load()
     n = len(instances)
     arr = _instance_descs(setup, instances)
